@@ -1,0 +1,226 @@
+"""TEST INFRASTRUCTURE ONLY -- Python bindings of the CPU oracle.
+
+Loads ``oracle/libkspir_oracle.so`` (the plain-C restatement of the KsPIR
+online answer, reference tests/test-pir.cpp:110-116) and, when it was built,
+``oracle/_ref/libkspir_ref.so`` (the reference's own sources compiled against
+the HEXL restatement).  Only ``tests/``, ``__graft_entry__.smoke()`` and the
+CPU-baseline leg of ``bench.py`` import this module; the product path never
+does.
+
+Also holds the seeded synthetic-input generator shared by the tests and the
+benchmark (splitmix64-seeded numpy PCG64 streams; every word canonical).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+import threading
+
+import numpy as np
+
+N = 4096
+Q1 = 268369921
+Q2 = 249561089
+CRTMOD = Q1 * Q2
+BSMOD = 16760833
+P = 65537
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_ORACLE_SO = os.path.join(_HERE, "libkspir_oracle.so")
+_REF_SO = os.path.join(_HERE, "_ref", "libkspir_ref.so")
+_lock = threading.Lock()
+_lib = None
+_ref = None
+
+_u64p = ctypes.POINTER(ctypes.c_uint64)
+_i32p = ctypes.POINTER(ctypes.c_int32)
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def build_oracle() -> str:
+    """Compiles the C restatement with the committed Makefile if needed."""
+    src = os.path.join(_HERE, "kspir_oracle.c")
+    if not os.path.exists(_ORACLE_SO) or os.path.getmtime(_ORACLE_SO) < os.path.getmtime(src):
+        subprocess.run(["make", "-s", "-C", _HERE, "oracle"], check=True)
+    return _ORACLE_SO
+
+
+def lib():
+    global _lib
+    with _lock:
+        if _lib is None:
+            build_oracle()
+            L = ctypes.CDLL(_ORACLE_SO)
+            vp = ctypes.c_void_p
+            L.ko_answer.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, vp, vp, vp, vp, vp, vp, vp, vp]
+            L.ko_matrix_vector_mul.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, vp, vp, vp, vp, vp]
+            L.ko_external_product.argtypes = [vp, vp, vp]
+            L.ko_packing.argtypes = [vp, ctypes.c_int, vp, vp]
+            L.ko_scan.argtypes = [vp, vp, ctypes.c_int, vp]
+            L.ko_ntt_forward.argtypes = [vp, ctypes.c_uint64]
+            L.ko_ntt_inverse.argtypes = [vp, ctypes.c_uint64]
+            L.ko_ntt_root.argtypes = [ctypes.c_uint64]
+            L.ko_ntt_root.restype = ctypes.c_uint64
+            L.ko_decompose_bsgs.argtypes = [vp, vp, ctypes.c_int, ctypes.c_uint64, ctypes.c_uint64, vp, vp]
+            L.ko_decompose.argtypes = [vp, ctypes.c_int, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, vp]
+            L.ko_decompose_rlwe.argtypes = [vp, vp, ctypes.c_int, ctypes.c_uint64, ctypes.c_uint64,
+                                            ctypes.c_uint64, vp]
+            L.ko_crt_compose.argtypes = [ctypes.c_uint64, ctypes.c_uint64]
+            L.ko_crt_compose.restype = ctypes.c_uint64
+            L.ko_barrett_coeff.argtypes = [ctypes.c_uint64, ctypes.c_int]
+            L.ko_barrett_coeff.restype = ctypes.c_uint64
+            L.ko_permutation_matrix.argtypes = [vp, ctypes.c_int]
+            L.ko_pow_mod_index.argtypes = [ctypes.c_int, ctypes.c_int]
+            _lib = L
+    return _lib
+
+
+def ref_available() -> bool:
+    return os.path.exists(_REF_SO)
+
+
+def ref():
+    """The reference compiled from its own sources (built here by ``make -C oracle ref``)."""
+    global _ref
+    with _lock:
+        if _ref is None:
+            if not os.path.exists(_REF_SO):
+                raise FileNotFoundError(_REF_SO)
+            L = ctypes.CDLL(_REF_SO)
+            vp = ctypes.c_void_p
+            L.ref_pir_setup.argtypes = [ctypes.c_uint32, ctypes.c_int, ctypes.c_int]
+            L.ref_pir_target.argtypes = [vp, vp]
+            L.ref_pir_get_inputs.argtypes = [vp] * 7
+            L.ref_pir_decrypt.argtypes = [vp, vp]
+            L.ref_answer.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]
+            L.ref_matrix_vector_mul.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, vp, vp, vp, vp]
+            L.ref_external_product.argtypes = [vp, vp, vp]
+            L.ref_packing.argtypes = [vp, ctypes.c_int, vp, vp]
+            L.ref_scan.argtypes = [vp, vp, ctypes.c_int, vp]
+            L.ref_crt_compose.argtypes = [ctypes.c_uint64, ctypes.c_uint64]
+            L.ref_crt_compose.restype = ctypes.c_uint64
+            L.ref_permutation_matrix.argtypes = [vp, ctypes.c_int]
+            L.ref_ntt.argtypes = [vp, ctypes.c_uint64, ctypes.c_int]
+            L.ref_decompose_bsgs.argtypes = [vp, vp, vp, vp]
+            L.ref_decompose.argtypes = [vp, ctypes.c_int, ctypes.c_uint64, ctypes.c_uint64, vp]
+            L.ref_decompose_rlwe.argtypes = [vp, vp, ctypes.c_int, ctypes.c_uint64, ctypes.c_uint64, vp]
+            _ref = L
+    return _ref
+
+
+# ---------------------------------------------------------------------------
+# sizes and seeded synthetic inputs
+
+def sizes(r: int, N1: int) -> dict:
+    N2 = N // 2 // N1
+    levels = int(r).bit_length() - 1
+    return dict(N2=N2, db=r * N * N // 2, query=4 * N, baby=(N1 // 2) * 6 * 2 * N,
+                giant=(N2 - 1) * 2 * 2 * N, packing=levels * 4 * 2 * N, rgsw=4 * 2 * N,
+                perms=N1 * N, result=r * 2 * N, response=2 * N)
+
+
+def _uniform(rng, n, q):
+    return rng.integers(0, q, size=n, dtype=np.uint64)
+
+
+def gen_db(seed: int, r: int, N1: int) -> np.ndarray:
+    """A preprocessed database in the reference's packed CRT layout
+    (crt.cpp:859-885): word = (v mod q1) | (v mod q2) << 32 with v uniform mod crtMod."""
+    rng = np.random.default_rng(np.random.SeedSequence([seed, 0xDB]))
+    n = r * N * N // 2
+    out = np.empty(n, dtype=np.uint64)
+    step = 1 << 24
+    for s in range(0, n, step):
+        m = min(step, n - s)
+        lo = rng.integers(0, Q1, size=m, dtype=np.uint64)
+        hi = rng.integers(0, Q2, size=m, dtype=np.uint64)
+        out[s:s + m] = lo | (hi << np.uint64(32))
+    return out
+
+
+def gen_client(seed: int, r: int, N1: int) -> dict:
+    """Query, keys and RGSW with uniformly random canonical words (layouts of kspir_oracle.h)."""
+    sz = sizes(r, N1)
+    rng = np.random.default_rng(np.random.SeedSequence([seed, 0xC1]))
+    q = np.concatenate([_uniform(rng, 2 * N, CRTMOD), _uniform(rng, 2 * N, BSMOD)])
+    baby = np.empty((N1 // 2, 6, 2 * N), dtype=np.uint64)
+    baby[:, :3] = _uniform(rng, (N1 // 2) * 3 * 2 * N, CRTMOD).reshape(N1 // 2, 3, 2 * N)
+    baby[:, 3:] = _uniform(rng, (N1 // 2) * 3 * 2 * N, BSMOD).reshape(N1 // 2, 3, 2 * N)
+    giant = _uniform(rng, sz["giant"], CRTMOD)
+    packing = _uniform(rng, sz["packing"], CRTMOD)
+    rgsw = _uniform(rng, sz["rgsw"], CRTMOD)
+    return dict(query=q, baby=baby.reshape(-1), giant=giant, packing=packing, rgsw=rgsw,
+                perms=permutation_matrix(N1))
+
+
+# ---------------------------------------------------------------------------
+# C restatement wrappers
+
+def permutation_matrix(N1: int) -> np.ndarray:
+    out = np.empty(N1 * N, dtype=np.int32)
+    lib().ko_permutation_matrix(_p(out), N1)
+    return out
+
+
+def answer(db, r, N1, c, with_stages=False):
+    resp = np.zeros(2 * N, dtype=np.uint64)
+    bsgs = np.zeros(r * 2 * N, dtype=np.uint64) if with_stages else None
+    ext = np.zeros(r * 2 * N, dtype=np.uint64) if with_stages else None
+    rc = lib().ko_answer(_p(db), r, N1, _p(c["query"]), _p(c["baby"]), _p(c["giant"]),
+                         _p(c["packing"]), _p(c["rgsw"]), _p(c["perms"]), _p(resp), _p(bsgs), _p(ext))
+    if rc:
+        raise RuntimeError(f"ko_answer rc={rc}")
+    return (resp, bsgs, ext) if with_stages else resp
+
+
+def matrix_vector_mul(db, r, N1, c, want_cipherbuf=False):
+    q = c["query"].copy()
+    res = np.zeros(r * 2 * N, dtype=np.uint64)
+    cb = np.zeros(N * 2 * N1, dtype=np.uint64) if want_cipherbuf else None
+    rc = lib().ko_matrix_vector_mul(_p(db), r, N1, _p(q), _p(c["baby"]), _p(c["giant"]),
+                                    _p(c["perms"]), _p(res), _p(cb))
+    if rc:
+        raise RuntimeError(f"ko_matrix_vector_mul rc={rc}")
+    return (res, q, cb) if want_cipherbuf else (res, q)
+
+
+def external_product(first_dim, rgsw, ext=None):
+    fd = first_dim.copy()
+    e = np.zeros(2 * N, dtype=np.uint64) if ext is None else ext.copy()
+    lib().ko_external_product(_p(e), _p(fd), _p(rgsw))
+    return e, fd
+
+
+def packing(rlwes, r, keys):
+    rl = rlwes.copy()
+    resp = np.zeros(2 * N, dtype=np.uint64)
+    rc = lib().ko_packing(_p(rl), r, _p(keys), _p(resp))
+    if rc:
+        raise RuntimeError(f"ko_packing rc={rc}")
+    return resp
+
+
+def scan(db_sub, cipherbuf, N1):
+    out = np.zeros((N // 2 // N1) * 2 * N, dtype=np.uint64)
+    lib().ko_scan(_p(db_sub), _p(cipherbuf), N1, _p(out))
+    return out
+
+
+def ntt(a, modulus, inverse=False):
+    x = np.ascontiguousarray(a, dtype=np.uint64).copy()
+    fn = lib().ko_ntt_inverse if inverse else lib().ko_ntt_forward
+    if fn(_p(x), modulus):
+        raise ValueError("unsupported modulus")
+    return x
+
+
+def crt_compose(x: int, y: int) -> int:
+    return lib().ko_crt_compose(x, y)
+
+
+def barrett_coeff(v: int, n: int) -> int:
+    return lib().ko_barrett_coeff(v, n)
