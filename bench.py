@@ -1,0 +1,366 @@
+#!/usr/bin/env python3
+"""Benchmark of the KsPIR online answer on B200.
+
+Workload (one "step"): one client's online answer over the 256 MB database of
+tests/test-pir.cpp -- 32768 records x 8 KB = r = 16 sub-databases of
+4096 x 2048 16-bit entries, preprocessed to 1 GiB of packed CRT words --
+with N = 4096, N1 = 128, N2 = 16 (reference tests/test-pir.cpp:14-29).
+Synthetic, seeded inputs of that shape (kspir_b200.synth).
+
+Reported (one JSON line on rank 0):
+  value      whole-job queries/s, inputs resident in HBM, device-timed with
+             CUDA events on the launching stream (max over ranks)
+  e2e        queries/s through the public C ABI (kspir_answer) with the
+             query in pinned host memory and the response read back, per step
+  roofline   the dominant kernel (the database scan): algorithmic bytes per
+             launch (r * N * N/2 * 8 = 1 GiB) / its mean CUDA-event duration
+  cpu_baseline  the reference's CPU answer (oracle/_ref, or the C port)
+             on the host cores, on a bounded sample
+
+--impl reference times the reference's own CPU implementation instead
+(rank 0 only), on the same metric.
+Multi-GPU (torchrun): each rank is an independent replica answering its own
+queries (no data-path collective); scaling "weak".
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "answer ms/query & batched queries/s at 256 MB DB (bit-exact); GB/s vs HBM peak"
+N = 4096
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="kspir", choices=["kspir", "reference"])
+    ap.add_argument("--r", type=int, default=16)
+    ap.add_argument("--N1", type=int, default=128)
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU-baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload_config(args):
+    return {"workload": f"single-query online answer, 256 MB DB (32768 x 8 KB records), "
+                        f"r={args.r} N1={args.N1} N2={N // 2 // args.N1} N={N}",
+            "r": args.r, "N1": args.N1, "N2": N // 2 // args.N1,
+            "db_bytes_preprocessed": args.r * N * N // 2 * 8,
+            "l2": "inputs larger than L2: the 1 GiB preprocessed database is streamed every step",
+            "parallelism": "replicas"}
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region (NVML reads only)
+
+class ClockSampler:
+    def __init__(self, index: int, period: float = 0.05):
+        self.samples = []
+        self.max_mhz = None
+        self.reasons = set()
+        self._stop = threading.Event()
+        self._ok = False
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+            self._ok = True
+        except Exception:
+            self.nv = None
+        self.period = period
+        self._t = None
+
+    def _run(self):
+        nv = self.nv
+        names = {
+            "hw_slowdown": getattr(nv, "nvmlClocksThrottleReasonHwSlowdown", 0x8),
+            "sw_thermal_slowdown": getattr(nv, "nvmlClocksThrottleReasonSwThermalSlowdown", 0x20),
+            "hw_thermal_slowdown": getattr(nv, "nvmlClocksThrottleReasonHwThermalSlowdown", 0x40),
+            "sw_power_cap": getattr(nv, "nvmlClocksThrottleReasonSwPowerCap", 0x4),
+        }
+        while not self._stop.is_set():
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
+                mask = nv.nvmlDeviceGetCurrentClocksThrottleReasons(self.h)
+                for n, bit in names.items():
+                    if mask & bit:
+                        self.reasons.add(n)
+            except Exception:
+                pass
+            self._stop.wait(self.period)
+
+    def __enter__(self):
+        if self._ok:
+            self._t = threading.Thread(target=self._run, daemon=True)
+            self._t.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self._t:
+            self._t.join()
+
+    def summary(self):
+        return {"sm_mhz": statistics.median(self.samples) if self.samples else None,
+                "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons), "samples": len(self.samples)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the reference's answer on the host cores
+
+def cpu_answer_rate(db, client, perms, r, N1, seconds, threads):
+    """Independent answers on `threads` host threads for about `seconds`;
+    returns (queries/s, kind, answers, threads)."""
+    import ctypes
+
+    from oracle import pyoracle as po
+    c = dict(client, perms=perms)
+    if po.ref_available():
+        L, kind = po.ref(), "reference"
+
+        def one():
+            resp = np.zeros(2 * N, np.uint64)
+            t = ctypes.c_double()
+            L.ref_answer(po._p(db), r, N1, po._p(c["query"]), po._p(c["baby"]), po._p(c["giant"]),
+                         po._p(c["packing"]), po._p(c["rgsw"]), po._p(c["perms"]), po._p(resp), None, None,
+                         ctypes.byref(t))
+    else:
+        kind = "port"
+
+        def one():
+            po.answer(db, r, N1, c)
+    counts = [0] * threads
+    t_end = [0.0]
+    start = time.perf_counter()
+    deadline = start + seconds
+
+    def worker(i):
+        while True:
+            one()
+            counts[i] += 1
+            if time.perf_counter() >= deadline:
+                break
+    ths = [threading.Thread(target=worker, args=(i,)) for i in range(threads)]
+    for t in ths:
+        t.start()
+    for t in ths:
+        t.join()
+    t_end[0] = time.perf_counter() - start
+    n = sum(counts)
+    return n / t_end[0], kind, n, threads
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+# ---------------------------------------------------------------------------
+
+def read_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    return 6650.0, "fallback (6.65 TB/s, earlier measurement on this pool)"
+
+
+def read_traffic(r):
+    """DRAM bytes per scan launch from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "k_scan_256mb.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.strip().startswith("dram_bytes_per_launch_r16:"):
+            try:
+                return int(float(line.split(":", 1)[1].split()[0]) * r / 16)
+            except ValueError:
+                return None
+    return None
+
+
+def run_gpu(args, rank, world, local_rank):
+    import torch
+
+    import kspir_b200 as kb
+    from kspir_b200 import synth
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    r, N1 = args.r, args.N1
+    db = synth.gen_db(args.seed, r, N1)
+    cl = synth.gen_client(args.seed + rank, r, N1)
+    perms = kb.permutation_matrix(N1)
+    ctx = kb.Context(r, N1, device=local_rank)
+    ctx.upload_db(db)
+    ctx.upload_perms(perms)
+    ctx.upload_client(0, cl["baby"], cl["giant"], cl["packing"], cl["rgsw"])
+
+    # device-resident query and response
+    dq = torch.from_numpy(cl["query"].view(np.int64).copy()).cuda()
+    dr = torch.empty(2 * N, dtype=torch.int64, device="cuda")
+    stream = torch.cuda.Stream()
+    host_ref = ctx.answer(0, cl["query"])   # host path, for a consistency check of the device path
+
+    def step():
+        ctx.answer_device(0, dq.data_ptr(), dr.data_ptr(), stream.cuda_stream)
+
+    with torch.cuda.stream(stream):
+        for _ in range(max(args.warmup, 3)):
+            step()
+    torch.cuda.synchronize()
+    if not np.array_equal(dr.cpu().numpy().view(np.uint64), host_ref):
+        raise RuntimeError("device-path response differs from the host-path response")
+
+    ctx.timing_reset()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clocks:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms = ev0.elapsed_time(ev1)
+    answers, launches, tot_ms, phases = ctx.timing_summary()
+    ctx.sync()
+
+    # end to end through the C ABI: pinned host query in, response out, every step
+    qh = torch.from_numpy(cl["query"].view(np.int64).copy()).pin_memory()
+    rh = torch.empty(2 * N, dtype=torch.int64).pin_memory()
+    qh_np = qh.numpy().view(np.uint64)
+    rh_np = rh.numpy().view(np.uint64)
+    for _ in range(3):
+        ctx.answer(0, qh_np, out=rh_np)
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ctx.answer(0, qh_np, out=rh_np)
+    e2e_s = time.perf_counter() - t0
+    if not np.array_equal(rh_np, host_ref):
+        raise RuntimeError("e2e response differs")
+
+    if dist:
+        t = torch.tensor([ms, e2e_s], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, e2e_s = float(t[0]), float(t[1])
+
+    if rank == 0:
+        db_bytes = r * N * N // 2 * 8
+        scan_ms = phases[1] / max(answers, 1)
+        peak, peak_src = read_peaks()
+        achieved = db_bytes / (scan_ms * 1e-3) / 1e9
+        out = {
+            "metric": METRIC,
+            "value": world * args.steps / (ms * 1e-3),
+            "unit": "queries/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "u64",
+            "data": "synthetic (seeded uniform canonical words; reference shapes)",
+            "config": workload_config(args),
+            "phases_ms_per_step": {"baby_steps": phases[0] / answers, "db_scan": scan_ms,
+                                   "giant_steps": phases[2] / answers, "external_products": phases[3] / answers,
+                                   "packing": phases[4] / answers},
+            "roofline": {"bound": "hbm", "kernel": "k_scan", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_src,
+                         "algorithmic_bytes_per_launch": db_bytes, "traffic": read_traffic(r)},
+            "e2e": {"value": world * args.steps / e2e_s, "unit": "queries/s",
+                    "h2d_bytes_per_step": 4 * N * 8, "d2h_bytes_per_step": 2 * N * 8},
+            "gpu_launches": int(launches) * world,
+            "clocks": clocks.summary(),
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            threads = host_threads()
+            rate, kind, n, th = cpu_answer_rate(db, cl, perms, r, N1, args.cpu_seconds, threads)
+            out["cpu_baseline"] = {"value": rate, "unit": "queries/s", "cores": th, "kind": kind,
+                                   "sample": f"{n} full answers (r={r}, N1={N1}) in ~{args.cpu_seconds:.0f} s, "
+                                             f"one independent query per thread"}
+        print(json.dumps(out), flush=True)
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    from kspir_b200 import synth
+    from oracle import pyoracle as po
+    r, N1 = args.r, args.N1
+    db = synth.gen_db(args.seed, r, N1)
+    cl = synth.gen_client(args.seed, r, N1)
+    perms = po.permutation_matrix(N1)
+    threads = host_threads()
+    # each step: one answer per host thread, all at once
+    per_step = 1
+    for _ in range(args.warmup):
+        cpu_answer_rate(db, cl, perms, r, N1, 0.0, threads)
+    t0 = time.perf_counter()
+    total = 0
+    kind = "port"
+    for _ in range(args.steps):
+        _, kind, n, _ = cpu_answer_rate(db, cl, perms, r, N1, 0.0, threads)
+        total += n
+    dt = time.perf_counter() - t0
+    value = total / dt
+    out = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+        "data": "synthetic (seeded uniform canonical words; reference shapes)", "config": workload_config(args),
+        "cpu_baseline": {"value": value, "unit": "queries/s", "cores": threads, "kind": kind,
+                         "sample": f"{per_step} answer per thread per step on {threads} threads"},
+        "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", args.gpus if args.gpus == 1 else 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_gpu(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

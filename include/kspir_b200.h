@@ -1,0 +1,144 @@
+/*
+ * kspir_b200 -- B200-native online answer of the KsPIR single-server PIR.
+ *
+ * C ABI.  Plain pointers and sizes, int status codes, no exceptions.  Every
+ * array uses the word layouts of the reference's own objects (u64 words,
+ * N = 4096, values canonical modulo the stated modulus):
+ *
+ *   datacrt  [r][N][N2][N1]   reference database_tocrt output, src/crt.cpp:859-885
+ *                             (word = (v mod q1) | (v mod q2) << 32)
+ *   query    [2][2][N]        query1[0] = (a, b) mod crtMod, query1[1] = (a, b) mod bsMod,
+ *                             coefficient form (src/twosteps.cpp:279-318, encrypt.cpp:443-495)
+ *   perms    [N1][N] int32    compute_permutation_matrix(permutations, N1, N), utils.cpp:1591
+ *   baby     [N1/2][6][2][N]  AutoKeyBSGSRNS::keyMap[5^i], i = 1..N1/2 (lwe.h:381-466):
+ *                             rows 0-2 mod crtMod, rows 3-5 mod bsMod, each (a, b), NTT form
+ *   giant    [N2-1][2][2][N]  AutoKeyBSGSRNS::keyMap[5^(N1*c)], c = 1..N2-1
+ *   packing  [log2 r][4][2][N] AutoKey::keyMap[N/2^l + 1], l = 0..log2 r - 1 (lwe.h:175-234)
+ *   rgsw     [4][2][N]        RGSWCiphertext rows (a[j], b[j]), j = 0..3 (lwe.h:113-170)
+ *   result   [r][2][N]        first-dimension results, NTT form
+ *   rlwes    [r][2][N]        external products, coefficient form
+ *   response [2][N]           packed response (a, b), coefficient form
+ *
+ * Gadget parameters are the reference's test-pir configuration: baby steps
+ * ell 3 / base 2^20 / Bg 2^20 (lwe.h:391-393), giant steps ell 2 / 2^20 / 2^18
+ * (lwe.h:402-404), RGSW ell 2 / 2^20 / 2^18 (test-pir.cpp:71), packing
+ * ell 4 / 0 / 2^14 (test-pir.cpp:88).
+ *
+ * Results are word-for-word those of the reference on the same inputs.
+ * Unlike the reference, a query, key or RLWE word that is not canonical is
+ * rejected with KSPIR_ERR_INVALID_ARG.
+ */
+#ifndef KSPIR_B200_H
+#define KSPIR_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KSPIR_OK 0
+#define KSPIR_ERR_INVALID_ARG -1   /* bad size, pointer, or non-canonical word */
+#define KSPIR_ERR_CUDA -2          /* a CUDA call failed (kspir_last_error has the text) */
+#define KSPIR_ERR_NOT_READY -3     /* database, permutations or client keys missing */
+#define KSPIR_ERR_OOM -4           /* device allocation failed */
+#define KSPIR_ERR_TIMEOUT -5       /* a bounded device-side wait gave up */
+#define KSPIR_ERR_BUSY -6          /* no free slot (serving admission) */
+
+#define KSPIR_N 4096
+
+typedef struct kspir_ctx kspir_ctx;
+
+typedef struct kspir_params {
+    int32_t r;            /* packing number = number of sub-databases, power of two, 1..512 */
+    int32_t N1;           /* baby steps, power of two, 32..512; N2 = N/2/N1 */
+    int32_t max_clients;  /* client key slots held on the device */
+    int32_t max_inflight; /* concurrent query workspaces (1 for the plain path) */
+} kspir_params;
+
+/* Context bound to one CUDA device.  Allocates the per-query workspaces. */
+int kspir_ctx_create(int device, const kspir_params* params, kspir_ctx** out);
+int kspir_ctx_destroy(kspir_ctx* ctx);
+const char* kspir_last_error(const kspir_ctx* ctx);
+const char* kspir_strerror(int code);
+
+/* Replaces the datacrt argument of matrix_vector_mul_bsgs_rns_crt_large
+ * (reference twosteps.h:55-57): the whole preprocessed database, host memory,
+ * r * N * N / 2 words, kept resident on the device. */
+int kspir_db_upload(kspir_ctx* ctx, const uint64_t* datacrt, size_t words);
+
+/* Replaces the permutations argument of matrix_vector_mul_bsgs_rns_crt_large
+ * (twosteps.h:55-57). */
+int kspir_perms_upload(kspir_ctx* ctx, const int32_t* perms, size_t count);
+
+/* Replaces the autoKey (AutoKeyBSGSRNS, twosteps.h:55-57), packing key
+ * (AutoKey, answer.h:79-80) and RGSW query (externalProduct, lwe.h:292) of one
+ * client, kept resident in slot `client`. */
+int kspir_client_keys_upload(kspir_ctx* ctx, int client, const uint64_t* baby, const uint64_t* giant,
+                             const uint64_t* packing, const uint64_t* rgsw);
+
+/* The server's online answer, reference tests/test-pir.cpp:110-116
+ * (matrix_vector_mul_bsgs_rns_crt_large -> externalProduct x r -> packingRLWEs),
+ * host buffers in and out.  The caller's query is not modified. */
+int kspir_answer(kspir_ctx* ctx, int client, const uint64_t* query, uint64_t* response);
+
+/* Same on device buffers (query [2][2][N], response [2][N]), enqueued on
+ * `stream` (a cudaStream_t, or NULL for the context's stream); returns once
+ * enqueued.  Call kspir_sync to wait and collect device-side errors. */
+int kspir_answer_device(kspir_ctx* ctx, int client, const uint64_t* d_query, uint64_t* d_response, void* stream);
+int kspir_sync(kspir_ctx* ctx);
+
+/* Reference matrix_vector_mul_bsgs_rns_crt_large (twosteps.h:55-57,
+ * twosteps.cpp:1527-1579) for one client: query_inout is modswitched in place
+ * to NTT form mod crtMod exactly like the reference's input[0] (twosteps.cpp:
+ * 1073-1086) and result ([r][2][N], NTT form) receives the r first-dimension
+ * results.  Host buffers. */
+int kspir_matrix_vector_mul_bsgs_rns_crt_large(kspir_ctx* ctx, int client, uint64_t* query_inout,
+                                               uint64_t* result);
+
+/* Reference externalProduct (lwe.h:292, lwe.cpp:761-808) for `count`
+ * ciphertexts: result[j] += g^-1(first_dim[j]) x RGSW, returned in
+ * coefficient form; first_dim ([count][2][N], NTT form) is converted to
+ * coefficient form in place, as the reference does.  Host buffers. */
+int kspir_external_product(kspir_ctx* ctx, int client, uint64_t* result, uint64_t* first_dim, int count);
+
+/* Reference packingRLWEs (answer.h:79-80, answer.cpp:800-835): packs r
+ * coefficient-form RLWEs ([r][2][N]) into response ([2][N], coefficient
+ * form).  Host buffers; rlwes is read only. */
+int kspir_packing_rlwes(kspir_ctx* ctx, int client, const uint64_t* rlwes, uint64_t* response);
+
+/* Fills perms ([N1][N] int32) with the matrix the reference's
+ * compute_permutation_matrix(permutations, N1, N) builds (utils.cpp:1591-1619):
+ * row i is the NTT-slot gather that applies X -> X^(5^i).  No device needed. */
+int kspir_permutation_matrix(int32_t* perms, int N1);
+
+/* Device time of the last kspir_answer / kspir_answer_device on the
+ * context's stream, in milliseconds, and per-phase split
+ * (baby steps, DB scan, giant steps, external products, packing). */
+int kspir_last_timing(kspir_ctx* ctx, float* total_ms, float* phase_ms /* [5] or NULL */);
+
+/* Timing of every answer enqueued since kspir_timing_reset (the most recent
+ * 512 are kept): the count, the kernels launched, and the summed device time
+ * in milliseconds in total and per phase (same split as kspir_last_timing).
+ * Waits for those answers to finish. */
+int kspir_timing_reset(kspir_ctx* ctx);
+int kspir_timing_summary(kspir_ctx* ctx, int* answers, long* launches, float* total_ms, float* phase_ms);
+
+/* Diagnostics: copies an intermediate of the last answer out of workspace 0,
+ * as reference words (host buffer of exactly the stated size):
+ *   KSPIR_STAGE_CIPHERBUF [N][N1][2]  reorientCipher output (twosteps.cpp:1386-1403)
+ *   KSPIR_STAGE_SCAN      [r][N2][2][N] fastMultiplyQueryByDatabaseDim1InvCRT outputs
+ *   KSPIR_STAGE_RESULT    [r][2][N]   first-dimension results (NTT form)
+ *   KSPIR_STAGE_EXT       [r][2][N]   external products (coefficient form) */
+#define KSPIR_STAGE_CIPHERBUF 0
+#define KSPIR_STAGE_SCAN 1
+#define KSPIR_STAGE_RESULT 2
+#define KSPIR_STAGE_EXT 3
+int kspir_fetch_stage(kspir_ctx* ctx, int stage, uint64_t* out, size_t words);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* KSPIR_B200_H */

@@ -1,0 +1,145 @@
+// Device-side arithmetic shared by every KsPIR kernel.
+//
+// Representation.  The reference computes modulo crtMod = q1*q2 (56 bits,
+// reference src/crt.h:16-18) and bsMod (24 bits, crt.h:32) on 64-bit words
+// through HEXL.  Every HEXL operation on the answer path is exact modular
+// arithmetic with canonical outputs, so a value mod crtMod is held here as its
+// two 28-bit residues (mod q1, mod q2) in 32-bit words, and bsMod is a third
+// 32-bit channel.  The NTT with root_of_unity_crt (crt.h:81) is, residue by
+// residue, the NTT with psi mod q1 and psi mod q2.  A canonical 56-bit (or
+// crtMod*bsMod 80-bit) integer is formed by CRT only where the reference
+// leaves modular arithmetic: the gadget decompositions and the response words.
+#pragma once
+
+#include <stdint.h>
+
+namespace kspir {
+
+constexpr int kN = 4096;          // ring dimension, reference params.h:16
+constexpr int kLogN = 12;
+constexpr uint32_t kQ1 = 268369921u;   // crt.h:16
+constexpr uint32_t kQ2 = 249561089u;   // crt.h:17
+constexpr uint64_t kCrtMod = (uint64_t)kQ1 * kQ2;
+constexpr uint32_t kBsMod = 16760833u; // crt.h:32
+constexpr uint64_t kBsModInvCrt = 51309461009346113ull;  // bsMod^-1 mod crtMod, crt.h:33
+constexpr uint32_t kCrtModInvBs = 3920321u;              // crtMod^-1 mod bsMod, crt.h:34
+
+// channels of the RNS representation
+enum Chan : int { CH_Q1 = 0, CH_Q2 = 1, CH_BS = 2, CH_COUNT = 3 };
+
+// Per-channel constants, filled on the host (context.cu) and kept in
+// __constant__ memory.
+struct ChanConst {
+    uint32_t q;
+    uint32_t two_q;
+    uint64_t barrett;      // floor(2^64 / q)
+    uint32_t ninv, ninv_p; // N^-1 mod q and its Shoup companion
+    uint32_t bsinv, bsinv_p;  // bsMod^-1 mod crtMod, reduced mod q (crt channels only)
+};
+
+struct DevConst {
+    ChanConst ch[CH_COUNT];
+    uint32_t q1inv_mod_q2;     // q1^-1 mod q2 (Garner)
+    uint32_t q1inv_mod_q2_p;
+};
+
+// Defined here: the library is one translation unit (kspir.cu includes every
+// kernel header), so no relocatable device code is needed.
+__constant__ DevConst c_dev;
+
+// ---------------------------------------------------------------------------
+// 32-bit residue arithmetic (q < 2^28)
+
+__device__ __forceinline__ uint32_t shoup_lazy(uint32_t x, uint32_t w, uint32_t wp, uint32_t q) {
+    // x*w mod q in [0, 2q) for any 32-bit x; wp = floor(w * 2^32 / q)
+    uint32_t t = __umulhi(x, wp);
+    return x * w - t * q;
+}
+
+__device__ __forceinline__ uint32_t shoup_mul(uint32_t x, uint32_t w, uint32_t wp, uint32_t q) {
+    uint32_t r = shoup_lazy(x, w, wp, q);
+    return r >= q ? r - q : r;
+}
+
+// Exact reduction of a product or a short sum of products (< 2^62) by Barrett.
+__device__ __forceinline__ uint32_t reduce64(uint64_t p, uint32_t q, uint64_t barrett) {
+    uint64_t qh = __umul64hi(p, barrett);
+    uint64_t r = p - qh * q;
+    while (r >= q) r -= q;   // at most twice for p < 2^62
+    return (uint32_t)r;
+}
+
+__device__ __forceinline__ uint32_t mulmod(uint32_t a, uint32_t b, int ch) {
+    return reduce64((uint64_t)a * b, c_dev.ch[ch].q, c_dev.ch[ch].barrett);
+}
+
+__device__ __forceinline__ uint32_t addmod(uint32_t a, uint32_t b, uint32_t q) {
+    uint32_t s = a + b;
+    return s >= q ? s - q : s;
+}
+
+__device__ __forceinline__ uint32_t submod(uint32_t a, uint32_t b, uint32_t q) {
+    return a >= b ? a - b : a + q - b;
+}
+
+// A signed small integer (|v| < q) as a canonical residue.
+__device__ __forceinline__ uint32_t signed_to_res(int64_t v, uint32_t q) {
+    return v < 0 ? (uint32_t)(v + (int64_t)q) : (uint32_t)v;
+}
+
+// ---------------------------------------------------------------------------
+// crtMod <-> residues
+
+// canonical value mod crtMod from its residues (Garner)
+__device__ __forceinline__ uint64_t crt_compose_res(uint32_t r1, uint32_t r2) {
+    uint32_t r1m = r1 >= kQ2 ? r1 - kQ2 : r1;           // r1 mod q2 (q1 < 2 q2)
+    uint32_t d = r2 >= r1m ? r2 - r1m : r2 + kQ2 - r1m;  // (r2 - r1) mod q2
+    uint32_t t = shoup_mul(d, c_dev.q1inv_mod_q2, c_dev.q1inv_mod_q2_p, kQ2);
+    return (uint64_t)r1 + (uint64_t)kQ1 * t;
+}
+
+__device__ __forceinline__ uint32_t mod_q1(uint64_t v) { return reduce64(v, kQ1, c_dev.ch[CH_Q1].barrett); }
+__device__ __forceinline__ uint32_t mod_q2(uint64_t v) { return reduce64(v, kQ2, c_dev.ch[CH_Q2].barrett); }
+__device__ __forceinline__ uint32_t mod_bs(uint64_t v) { return reduce64(v, kBsMod, c_dev.ch[CH_BS].barrett); }
+
+// ---------------------------------------------------------------------------
+// 128-bit helpers (hi:lo pairs)
+
+struct u128 { uint64_t lo, hi; };
+
+__device__ __forceinline__ u128 mul_64x64(uint64_t a, uint64_t b) {
+    u128 r; r.lo = a * b; r.hi = __umul64hi(a, b); return r;
+}
+
+__device__ __forceinline__ u128 add128(u128 a, u128 b) {
+    u128 r; r.lo = a.lo + b.lo; r.hi = a.hi + b.hi + (r.lo < a.lo ? 1 : 0); return r;
+}
+
+__device__ __forceinline__ u128 sub128(u128 a, u128 b) {
+    u128 r; r.lo = a.lo - b.lo; r.hi = a.hi - b.hi - (a.lo < b.lo ? 1 : 0); return r;
+}
+
+__device__ __forceinline__ bool gt128(u128 a, u128 b) {
+    return a.hi > b.hi || (a.hi == b.hi && a.lo > b.lo);
+}
+
+__device__ __forceinline__ u128 shr128(u128 a, int s) {  // 0 < s < 64
+    u128 r; r.lo = (a.lo >> s) | (a.hi << (64 - s)); r.hi = a.hi >> s; return r;
+}
+
+// ---------------------------------------------------------------------------
+// automorphism X -> X^g, coefficient domain, as a gather:
+// out[k] = +-in[i] with i*g = k or k+N (mod 2N).  `neg_canonical` selects the
+// negation: the reference's automorphic_rns writes 0 for -0 (twosteps.cpp:776-778);
+// the inline loops of evalAutoRNSCRT / evalAuto write q (twosteps.cpp:629-630,
+// answer.cpp:606-607).  Downstream every consumer treats q exactly like 0, so
+// the kernels only need the canonical form.
+__device__ __forceinline__ int auto_src(int k, uint32_t ginv, bool* neg) {
+    uint32_t i0 = ((uint32_t)k * ginv) & (2 * kN - 1);
+    *neg = i0 >= (uint32_t)kN;
+    return (int)(i0 & (kN - 1));
+}
+
+__device__ __forceinline__ uint32_t negmod(uint32_t x, uint32_t q) { return x ? q - x : 0; }
+
+}  // namespace kspir

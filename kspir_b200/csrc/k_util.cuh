@@ -1,0 +1,65 @@
+// Generic building blocks: batched transforms driven by job lists, residue
+// composition into 64-bit words, and small element-wise helpers.
+#pragma once
+
+#include "common.cuh"
+#include "ntt.cuh"
+
+namespace kspir {
+
+// One transform: read N residues from src (stride 1), transform on channel
+// `ch`, write to dst[k * dst_stride] (dst may equal src).
+struct NttJob {
+    const uint32_t* src;
+    uint32_t* dst;
+    int32_t ch;
+    int32_t dst_stride;
+};
+
+template <int T, bool INVERSE>
+__global__ void __launch_bounds__(T) k_ntt_jobs(const NttJob* __restrict__ jobs, NttTables tabs) {
+    __shared__ uint32_t s[kN];
+    const NttJob jb = jobs[blockIdx.x];
+    const uint4* src4 = reinterpret_cast<const uint4*>(jb.src);
+    uint4* s4 = reinterpret_cast<uint4*>(s);
+    for (int k = threadIdx.x; k < kN / 4; k += T) s4[k] = src4[k];
+    if (INVERSE) cta_ntt_inverse<T>(s, tabs.tw[jb.ch], jb.ch);
+    else cta_ntt_forward<T>(s, tabs.tw[jb.ch], jb.ch);
+    if (jb.dst_stride == 1) {
+        uint4* dst4 = reinterpret_cast<uint4*>(jb.dst);
+        for (int k = threadIdx.x; k < kN / 4; k += T) dst4[k] = s4[k];
+    } else {
+        for (int k = threadIdx.x; k < kN; k += T) jb.dst[(size_t)k * jb.dst_stride] = s[k];
+    }
+}
+
+// words[p][k] = canonical crtMod value of residues (res[p][0][k], res[p][1][k])
+// for `polys` consecutive [2][N] residue polynomials.
+__global__ void k_compose_words(const uint32_t* __restrict__ res, uint64_t* __restrict__ words, int polys) {
+    int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= polys * kN) return;
+    int p = idx / kN, k = idx % kN;
+    const uint32_t* r = res + (size_t)p * 2 * kN;
+    words[idx] = crt_compose_res(r[k], r[kN + k]);
+}
+
+// res[p][ch][k] = words[p][k] mod q_ch (ch = q1, q2) for `polys` polynomials.
+__global__ void k_split_words(const uint64_t* __restrict__ words, uint32_t* __restrict__ res, int polys) {
+    int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= polys * kN) return;
+    int p = idx / kN, k = idx % kN;
+    uint64_t v = words[idx];
+    uint32_t* r = res + (size_t)p * 2 * kN;
+    r[k] = mod_q1(v);
+    r[kN + k] = mod_q2(v);
+}
+
+// Validation of caller words: flags[0] |= 1 when some word is >= its modulus.
+__global__ void k_check_canonical(const uint64_t* __restrict__ words, size_t n, uint64_t modulus,
+                                  int* __restrict__ flag) {
+    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    for (; i < n; i += (size_t)gridDim.x * blockDim.x)
+        if (words[i] >= modulus) atomicOr(flag, 1);
+}
+
+}  // namespace kspir

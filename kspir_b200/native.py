@@ -1,0 +1,221 @@
+"""ctypes binding of the C ABI in ``include/kspir_b200.h``.
+
+The product path always runs through ``libkspir_b200.so``; there is no CPU
+fallback.  Loading fails loudly when the library has not been built.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+N = 4096
+Q1 = 268369921
+Q2 = 249561089
+CRTMOD = Q1 * Q2
+BSMOD = 16760833
+
+OK = 0
+ERR_INVALID_ARG = -1
+ERR_CUDA = -2
+ERR_NOT_READY = -3
+ERR_OOM = -4
+ERR_TIMEOUT = -5
+ERR_BUSY = -6
+
+STAGE_CIPHERBUF = 0
+STAGE_SCAN = 1
+STAGE_RESULT = 2
+STAGE_EXT = 3
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libkspir_b200.so")
+
+# every entry point of include/kspir_b200.h with its ctypes signature
+_vp = ctypes.c_void_p
+_i = ctypes.c_int
+_sz = ctypes.c_size_t
+SIGNATURES = {
+    "kspir_ctx_create": (_i, [_i, _vp, _vp]),
+    "kspir_ctx_destroy": (_i, [_vp]),
+    "kspir_last_error": (ctypes.c_char_p, [_vp]),
+    "kspir_strerror": (ctypes.c_char_p, [_i]),
+    "kspir_db_upload": (_i, [_vp, _vp, _sz]),
+    "kspir_perms_upload": (_i, [_vp, _vp, _sz]),
+    "kspir_client_keys_upload": (_i, [_vp, _i, _vp, _vp, _vp, _vp]),
+    "kspir_answer": (_i, [_vp, _i, _vp, _vp]),
+    "kspir_answer_device": (_i, [_vp, _i, _vp, _vp, _vp]),
+    "kspir_sync": (_i, [_vp]),
+    "kspir_matrix_vector_mul_bsgs_rns_crt_large": (_i, [_vp, _i, _vp, _vp]),
+    "kspir_external_product": (_i, [_vp, _i, _vp, _vp, _i]),
+    "kspir_packing_rlwes": (_i, [_vp, _i, _vp, _vp]),
+    "kspir_last_timing": (_i, [_vp, _vp, _vp]),
+    "kspir_fetch_stage": (_i, [_vp, _i, _vp, _sz]),
+    "kspir_permutation_matrix": (_i, [_vp, _i]),
+    "kspir_timing_reset": (_i, [_vp]),
+    "kspir_timing_summary": (_i, [_vp, _vp, _vp, _vp, _vp]),
+}
+
+
+class Params(ctypes.Structure):
+    _fields_ = [("r", ctypes.c_int32), ("N1", ctypes.c_int32),
+                ("max_clients", ctypes.c_int32), ("max_inflight", ctypes.c_int32)]
+
+
+_lib = None
+
+
+def load(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Loads the CUDA library (raises if it is missing or incomplete)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"kspir_b200 CUDA library not built: {path} (run kspir_b200/build.py)")
+    lib = ctypes.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def ptr(a: np.ndarray | None):
+    return None if a is None else ctypes.c_void_p(a.ctypes.data)
+
+
+def permutation_matrix(N1: int) -> np.ndarray:
+    """[N1][N] int32, the reference's compute_permutation_matrix (utils.cpp:1591-1619)."""
+    out = np.empty(N1 * N, dtype=np.int32)
+    rc = load().kspir_permutation_matrix(ptr(out), N1)
+    if rc:
+        raise KspirError(rc, "permutation_matrix")
+    return out
+
+
+class KspirError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"kspir error {code}: {msg}")
+        self.code = code
+
+
+def _u64(a) -> np.ndarray:
+    a = np.ascontiguousarray(a, dtype=np.uint64)
+    return a
+
+
+class Context:
+    """One device context: resident database, permutations, client keys and
+    query workspaces (include/kspir_b200.h)."""
+
+    def __init__(self, r: int, N1: int = 128, device: int = 0, max_clients: int = 1, max_inflight: int = 1):
+        self.lib = load()
+        self.r, self.N1, self.N2 = r, N1, N // 2 // N1
+        self.levels = r.bit_length() - 1
+        self._h = ctypes.c_void_p()
+        p = Params(r, N1, max_clients, max_inflight)
+        rc = self.lib.kspir_ctx_create(device, ctypes.byref(p), ctypes.byref(self._h))
+        if rc:
+            raise KspirError(rc, self.lib.kspir_strerror(rc).decode())
+
+    # -- plumbing ---------------------------------------------------------
+    def _check(self, rc: int):
+        if rc:
+            msg = self.lib.kspir_last_error(self._h).decode() if self._h else ""
+            raise KspirError(rc, msg or self.lib.kspir_strerror(rc).decode())
+
+    def close(self):
+        if self._h:
+            self.lib.kspir_ctx_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    # -- resident data ----------------------------------------------------
+    def upload_db(self, datacrt):
+        d = _u64(datacrt).reshape(-1)
+        self._check(self.lib.kspir_db_upload(self._h, ptr(d), d.size))
+
+    def upload_perms(self, perms):
+        p = np.ascontiguousarray(perms, dtype=np.int32).reshape(-1)
+        self._check(self.lib.kspir_perms_upload(self._h, ptr(p), p.size))
+
+    def upload_client(self, client: int, baby, giant, packing, rgsw):
+        arrs = [None if a is None else _u64(a).reshape(-1) for a in (baby, giant, packing, rgsw)]
+        self._check(self.lib.kspir_client_keys_upload(self._h, client, *[ptr(a) for a in arrs]))
+
+    # -- answer -----------------------------------------------------------
+    def answer(self, client: int, query, out: np.ndarray | None = None) -> np.ndarray:
+        q = _u64(query).reshape(-1)
+        if out is None:
+            out = np.empty(2 * N, dtype=np.uint64)
+        self._check(self.lib.kspir_answer(self._h, client, ptr(q), ptr(out)))
+        return out
+
+    def answer_device(self, client: int, d_query: int, d_response: int, stream: int | None = None):
+        self._check(self.lib.kspir_answer_device(self._h, client, ctypes.c_void_p(d_query),
+                                                 ctypes.c_void_p(d_response),
+                                                 ctypes.c_void_p(stream) if stream else None))
+
+    def sync(self):
+        self._check(self.lib.kspir_sync(self._h))
+
+    def last_timing(self):
+        tot = ctypes.c_float()
+        ph = (ctypes.c_float * 5)()
+        self._check(self.lib.kspir_last_timing(self._h, ctypes.byref(tot), ph))
+        return tot.value, list(ph)
+
+    def timing_reset(self):
+        self._check(self.lib.kspir_timing_reset(self._h))
+
+    def timing_summary(self):
+        """(answers, kernel launches, summed ms, summed ms per phase) since timing_reset."""
+        n = ctypes.c_int()
+        la = ctypes.c_long()
+        tot = ctypes.c_float()
+        ph = (ctypes.c_float * 5)()
+        self._check(self.lib.kspir_timing_summary(self._h, ctypes.byref(n), ctypes.byref(la), ctypes.byref(tot), ph))
+        return n.value, la.value, tot.value, list(ph)
+
+    # -- the reference's three functions ------------------------------------
+    def matrix_vector_mul(self, client: int, query):
+        q = _u64(query).reshape(-1).copy()
+        res = np.empty(self.r * 2 * N, dtype=np.uint64)
+        self._check(self.lib.kspir_matrix_vector_mul_bsgs_rns_crt_large(self._h, client, ptr(q), ptr(res)))
+        return res, q
+
+    def external_product(self, client: int, result, first_dim):
+        res = _u64(result).reshape(-1).copy()
+        fd = _u64(first_dim).reshape(-1).copy()
+        count = res.size // (2 * N)
+        self._check(self.lib.kspir_external_product(self._h, client, ptr(res), ptr(fd), count))
+        return res, fd
+
+    def packing(self, client: int, rlwes):
+        rl = _u64(rlwes).reshape(-1)
+        out = np.empty(2 * N, dtype=np.uint64)
+        self._check(self.lib.kspir_packing_rlwes(self._h, client, ptr(rl), ptr(out)))
+        return out
+
+    def fetch_stage(self, stage: int) -> np.ndarray:
+        sizes = {STAGE_CIPHERBUF: N * self.N1 * 2, STAGE_SCAN: self.r * self.N2 * 2 * N,
+                 STAGE_RESULT: self.r * 2 * N, STAGE_EXT: self.r * 2 * N}
+        out = np.empty(sizes[stage], dtype=np.uint64)
+        self._check(self.lib.kspir_fetch_stage(self._h, stage, ptr(out), out.size))
+        return out

@@ -1,0 +1,52 @@
+"""Seeded synthetic inputs with the shapes and value ranges of the reference's
+online answer (the reference samples its database and keys with glibc rand();
+these stand in for them, with every word canonical for its modulus).
+
+* ``gen_db``: a preprocessed database in the packed CRT layout of
+  database_tocrt (reference src/crt.cpp:859-885): word = (v mod q1) | (v mod q2) << 32,
+  v uniform mod crtMod -- r sub-databases of N x N/2 words (r = 16: the
+  256 MB-record database of tests/test-pir.cpp, 1 GiB preprocessed).
+* ``gen_client``: query (mod crtMod, mod bsMod), baby/giant/packing keys and
+  the RGSW query, uniformly random canonical words in the layouts of
+  include/kspir_b200.h.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+N = 4096
+Q1 = 268369921
+Q2 = 249561089
+CRTMOD = Q1 * Q2
+BSMOD = 16760833
+
+
+def _uniform(rng, n, q):
+    return rng.integers(0, q, size=n, dtype=np.uint64)
+
+
+def gen_db(seed: int, r: int, N1: int) -> np.ndarray:
+    rng = np.random.default_rng(np.random.SeedSequence([seed, 0xDB]))
+    n = r * N * N // 2
+    out = np.empty(n, dtype=np.uint64)
+    step = 1 << 24
+    for s in range(0, n, step):
+        m = min(step, n - s)
+        lo = rng.integers(0, Q1, size=m, dtype=np.uint64)
+        hi = rng.integers(0, Q2, size=m, dtype=np.uint64)
+        out[s:s + m] = lo | (hi << np.uint64(32))
+    return out
+
+
+def gen_client(seed: int, r: int, N1: int) -> dict:
+    N2 = N // 2 // N1
+    levels = int(r).bit_length() - 1
+    rng = np.random.default_rng(np.random.SeedSequence([seed, 0xC1]))
+    q = np.concatenate([_uniform(rng, 2 * N, CRTMOD), _uniform(rng, 2 * N, BSMOD)])
+    baby = np.empty((N1 // 2, 6, 2 * N), dtype=np.uint64)
+    baby[:, :3] = _uniform(rng, (N1 // 2) * 3 * 2 * N, CRTMOD).reshape(N1 // 2, 3, 2 * N)
+    baby[:, 3:] = _uniform(rng, (N1 // 2) * 3 * 2 * N, BSMOD).reshape(N1 // 2, 3, 2 * N)
+    giant = _uniform(rng, (N2 - 1) * 2 * 2 * N, CRTMOD)
+    packing = _uniform(rng, levels * 4 * 2 * N, CRTMOD)
+    rgsw = _uniform(rng, 4 * 2 * N, CRTMOD)
+    return dict(query=q, baby=baby.reshape(-1), giant=giant, packing=packing, rgsw=rgsw)

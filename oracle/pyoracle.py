@@ -7,8 +7,8 @@ the HEXL restatement).  Only ``tests/``, ``__graft_entry__.smoke()`` and the
 CPU-baseline leg of ``bench.py`` import this module; the product path never
 does.
 
-Also holds the seeded synthetic-input generator shared by the tests and the
-benchmark (splitmix64-seeded numpy PCG64 streams; every word canonical).
+The seeded synthetic inputs come from ``kspir_b200.synth`` (shared with the
+benchmark); the permutation matrix from the oracle's own restatement.
 """
 from __future__ import annotations
 
@@ -18,6 +18,8 @@ import subprocess
 import threading
 
 import numpy as np
+
+from kspir_b200 import synth as _synth
 
 N = 4096
 Q1 = 268369921
@@ -123,38 +125,17 @@ def sizes(r: int, N1: int) -> dict:
                 perms=N1 * N, result=r * 2 * N, response=2 * N)
 
 
-def _uniform(rng, n, q):
-    return rng.integers(0, q, size=n, dtype=np.uint64)
-
-
 def gen_db(seed: int, r: int, N1: int) -> np.ndarray:
-    """A preprocessed database in the reference's packed CRT layout
-    (crt.cpp:859-885): word = (v mod q1) | (v mod q2) << 32 with v uniform mod crtMod."""
-    rng = np.random.default_rng(np.random.SeedSequence([seed, 0xDB]))
-    n = r * N * N // 2
-    out = np.empty(n, dtype=np.uint64)
-    step = 1 << 24
-    for s in range(0, n, step):
-        m = min(step, n - s)
-        lo = rng.integers(0, Q1, size=m, dtype=np.uint64)
-        hi = rng.integers(0, Q2, size=m, dtype=np.uint64)
-        out[s:s + m] = lo | (hi << np.uint64(32))
-    return out
+    """Seeded synthetic database (kspir_b200.synth.gen_db)."""
+    return _synth.gen_db(seed, r, N1)
 
 
 def gen_client(seed: int, r: int, N1: int) -> dict:
-    """Query, keys and RGSW with uniformly random canonical words (layouts of kspir_oracle.h)."""
-    sz = sizes(r, N1)
-    rng = np.random.default_rng(np.random.SeedSequence([seed, 0xC1]))
-    q = np.concatenate([_uniform(rng, 2 * N, CRTMOD), _uniform(rng, 2 * N, BSMOD)])
-    baby = np.empty((N1 // 2, 6, 2 * N), dtype=np.uint64)
-    baby[:, :3] = _uniform(rng, (N1 // 2) * 3 * 2 * N, CRTMOD).reshape(N1 // 2, 3, 2 * N)
-    baby[:, 3:] = _uniform(rng, (N1 // 2) * 3 * 2 * N, BSMOD).reshape(N1 // 2, 3, 2 * N)
-    giant = _uniform(rng, sz["giant"], CRTMOD)
-    packing = _uniform(rng, sz["packing"], CRTMOD)
-    rgsw = _uniform(rng, sz["rgsw"], CRTMOD)
-    return dict(query=q, baby=baby.reshape(-1), giant=giant, packing=packing, rgsw=rgsw,
-                perms=permutation_matrix(N1))
+    """Seeded synthetic client material plus the permutation matrix of the
+    oracle's restatement of compute_permutation_matrix (utils.cpp:1591-1619)."""
+    c = _synth.gen_client(seed, r, N1)
+    c["perms"] = permutation_matrix(N1)
+    return c
 
 
 # ---------------------------------------------------------------------------
