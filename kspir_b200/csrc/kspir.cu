@@ -187,6 +187,22 @@ int set_err(kspir_ctx* c, int code, const std::string& msg) {
                            std::string(#call) + ": " + cudaGetErrorString(e_));              \
     } while (0)
 
+// Every host<->device copy goes through the context's (non-blocking) stream and
+// is waited for: a plain cudaMemcpy runs on the legacy stream, which a
+// non-blocking stream does not order against, and a pageable host->device
+// cudaMemcpy may return before its DMA has landed.
+int copy_sync(kspir_ctx* c, void* dst, const void* src, size_t bytes, cudaMemcpyKind kind) {
+    KS_CUDA(c, cudaMemcpyAsync(dst, src, bytes, kind, c->stream));
+    KS_CUDA(c, cudaStreamSynchronize(c->stream));
+    return KSPIR_OK;
+}
+
+#define KS_COPY(ctx, dst, src, bytes, kind)                      \
+    do {                                                         \
+        int rc_ = copy_sync(ctx, dst, src, bytes, kind);         \
+        if (rc_) return rc_;                                     \
+    } while (0)
+
 int init_constants(kspir_ctx* c) {
     DevConst dc{};
     const uint32_t qs[3] = {kQ1, kQ2, kBsMod};
@@ -202,7 +218,8 @@ int init_constants(kspir_ctx* c) {
     }
     dc.q1inv_mod_q2 = (uint32_t)h_invmod(kQ1 % kQ2, kQ2);
     dc.q1inv_mod_q2_p = shoup32(dc.q1inv_mod_q2, kQ2);
-    KS_CUDA(c, cudaMemcpyToSymbol(c_dev, &dc, sizeof(dc)));
+    KS_CUDA(c, cudaMemcpyToSymbolAsync(c_dev, &dc, sizeof(dc), 0, cudaMemcpyHostToDevice, c->stream));
+    KS_CUDA(c, cudaStreamSynchronize(c->stream));
 
     // twiddles: crt channels use root_of_unity_crt (reference crt.h:81) reduced
     // per prime; bsMod uses HEXL's minimal primitive root
@@ -221,16 +238,16 @@ int init_constants(kspir_ctx* c) {
         }
     }
     KS_CUDA(c, cudaMalloc(&c->tw, tw.size() * 4));
-    KS_CUDA(c, cudaMemcpy(c->tw, tw.data(), tw.size() * 4, cudaMemcpyHostToDevice));
+    KS_COPY(c, c->tw, tw.data(), tw.size() * 4, cudaMemcpyHostToDevice);
     for (int ch = 0; ch < 3; ch++) c->ntabs.tw[ch] = c->tw + (size_t)ch * 4 * kN;
 
     std::vector<uint16_t> sb((size_t)c->N1h * kN), sg((size_t)std::max(1, c->N2 - 1) * kN);
     for (int i = 0; i < c->N1h; i++) slot_permutation(pow5(i + 1), sb.data() + (size_t)i * kN);
     for (int cc = 1; cc < c->N2; cc++) slot_permutation(pow5((uint32_t)(c->N1 * cc)), sg.data() + (size_t)(cc - 1) * kN);
     KS_CUDA(c, cudaMalloc(&c->sigma_baby, sb.size() * 2));
-    KS_CUDA(c, cudaMemcpy(c->sigma_baby, sb.data(), sb.size() * 2, cudaMemcpyHostToDevice));
+    KS_COPY(c, c->sigma_baby, sb.data(), sb.size() * 2, cudaMemcpyHostToDevice);
     KS_CUDA(c, cudaMalloc(&c->sigma_giant, sg.size() * 2));
-    KS_CUDA(c, cudaMemcpy(c->sigma_giant, sg.data(), sg.size() * 2, cudaMemcpyHostToDevice));
+    KS_COPY(c, c->sigma_giant, sg.data(), sg.size() * 2, cudaMemcpyHostToDevice);
 
     c->gad.baby = make_gadget_bsgs(3, 1u << 20, 1u << 20);
     c->gad.giant = make_gadget_b(2, 1u << 20, 1u << 18);
@@ -275,7 +292,8 @@ int init_workspace(kspir_ctx* c, WsSlot& s) {
     size_t total = 0;
     for (auto& pt : parts) total = align_up(total, 256) + pt.bytes;
     KS_CUDA(c, cudaMalloc(&s.mem, total));
-    KS_CUDA(c, cudaMemset(s.mem, 0, total));
+    KS_CUDA(c, cudaMemsetAsync(s.mem, 0, total, c->stream));
+    KS_CUDA(c, cudaStreamSynchronize(c->stream));
     size_t off = 0;
     for (auto& pt : parts) {
         off = align_up(off, 256);
@@ -347,7 +365,7 @@ int init_workspace(kspir_ctx* c, WsSlot& s) {
             }
     }
     KS_CUDA(c, cudaMalloc(&s.jobs, jobs.size() * sizeof(NttJob)));
-    KS_CUDA(c, cudaMemcpy(s.jobs, jobs.data(), jobs.size() * sizeof(NttJob), cudaMemcpyHostToDevice));
+    KS_COPY(c, s.jobs, jobs.data(), jobs.size() * sizeof(NttJob), cudaMemcpyHostToDevice);
     return KSPIR_OK;
 }
 
@@ -468,9 +486,10 @@ int check_ready(kspir_ctx* c, int client) {
 int finish(kspir_ctx* c, WsSlot& s) {
     KS_CUDA(c, cudaStreamSynchronize(c->stream));
     int herr = 0;
-    KS_CUDA(c, cudaMemcpy(&herr, s.ws.err, sizeof(int), cudaMemcpyDeviceToHost));
+    KS_COPY(c, &herr, s.ws.err, sizeof(int), cudaMemcpyDeviceToHost);
     if (herr) {
-        cudaMemset(s.ws.err, 0, sizeof(int));
+        cudaMemsetAsync(s.ws.err, 0, sizeof(int), c->stream);
+        cudaStreamSynchronize(c->stream);
         return set_err(c, KSPIR_ERR_TIMEOUT, "a bounded device wait gave up (code " + std::to_string(herr) + ")");
     }
     return KSPIR_OK;
@@ -563,7 +582,7 @@ int kspir_db_upload(kspir_ctx* c, const uint64_t* datacrt, size_t words) {
     if (words != need) return set_err(c, KSPIR_ERR_INVALID_ARG, "database size must be r*N*N/2 words");
     KS_CUDA(c, cudaSetDevice(c->device));
     if (!c->db) KS_CUDA(c, cudaMalloc(&c->db, need * 8));
-    KS_CUDA(c, cudaMemcpy(c->db, datacrt, need * 8, cudaMemcpyHostToDevice));
+    KS_COPY(c, c->db, datacrt, need * 8, cudaMemcpyHostToDevice);
     c->db_loaded = true;
     return KSPIR_OK;
 }
@@ -574,7 +593,7 @@ int kspir_perms_upload(kspir_ctx* c, const int32_t* perms, size_t count) {
     for (size_t i = 0; i < count; i++)
         if (perms[i] < 0 || perms[i] >= kN) return set_err(c, KSPIR_ERR_INVALID_ARG, "permutation entry out of range");
     KS_CUDA(c, cudaSetDevice(c->device));
-    KS_CUDA(c, cudaMemcpy(c->perms, perms, count * 4, cudaMemcpyHostToDevice));
+    KS_COPY(c, c->perms, perms, count * 4, cudaMemcpyHostToDevice);
     c->perms_loaded = true;
     return KSPIR_OK;
 }
@@ -622,7 +641,7 @@ int kspir_client_keys_upload(kspir_ctx* c, int client, const uint64_t* baby, con
     KS_CUDA(c, cudaMalloc(&stage, stage_words * 8));
     auto split = [&](const uint64_t* h, size_t polys, uint32_t* dst) -> int {
         if (!polys) return KSPIR_OK;
-        KS_CUDA(c, cudaMemcpy(stage, h, polys * kN * 8, cudaMemcpyHostToDevice));
+        KS_COPY(c, stage, h, polys * kN * 8, cudaMemcpyHostToDevice);
         k_split_words<<<blocks_for((long)polys * kN, 256), 256, 0, c->stream>>>(stage, dst, (int)polys);
         KS_CUDA(c, cudaStreamSynchronize(c->stream));
         return KSPIR_OK;
@@ -634,9 +653,8 @@ int kspir_client_keys_upload(kspir_ctx* c, int client, const uint64_t* baby, con
     if (!rc) {
         std::vector<uint32_t> bs32(bs_rows.size());
         for (size_t i = 0; i < bs_rows.size(); i++) bs32[i] = (uint32_t)bs_rows[i];
-        cudaError_t e = cudaMemcpy(const_cast<uint32_t*>(cl.keys.baby_bs), bs32.data(), bs32.size() * 4,
-                                   cudaMemcpyHostToDevice);
-        if (e != cudaSuccess) rc = set_err(c, KSPIR_ERR_CUDA, cudaGetErrorString(e));
+        rc = copy_sync(c, const_cast<uint32_t*>(cl.keys.baby_bs), bs32.data(), bs32.size() * 4,
+                       cudaMemcpyHostToDevice);
     }
     cudaFree(stage);
     if (rc) return rc;
@@ -744,7 +762,7 @@ int kspir_matrix_vector_mul_bsgs_rns_crt_large(kspir_ctx* c, int client, uint64_
     rc = finish(c, s);
     if (rc) return rc;
     std::vector<uint64_t> cb((size_t)kN * c->N1 * 2);
-    KS_CUDA(c, cudaMemcpy(cb.data(), s.ws.cipherbuf, cb.size() * 8, cudaMemcpyDeviceToHost));
+    KS_COPY(c, cb.data(), s.ws.cipherbuf, cb.size() * 8, cudaMemcpyDeviceToHost);
     for (int comp = 0; comp < 2; comp++)
         for (int k = 0; k < kN; k++) {
             const uint64_t wv = cb[(size_t)k * c->N1 * 2 + comp];
@@ -826,7 +844,7 @@ int kspir_fetch_stage(kspir_ctx* c, int stage, uint64_t* out, size_t words) {
     if (stage == KSPIR_STAGE_CIPHERBUF) {
         const size_t n = (size_t)kN * c->N1 * 2;
         if (words != n) return set_err(c, KSPIR_ERR_INVALID_ARG, "size mismatch");
-        KS_CUDA(c, cudaMemcpy(out, s.ws.cipherbuf, n * 8, cudaMemcpyDeviceToHost));
+        KS_COPY(c, out, s.ws.cipherbuf, n * 8, cudaMemcpyDeviceToHost);
         return KSPIR_OK;
     }
     const uint32_t* src = nullptr;

@@ -593,6 +593,14 @@ static void eval_auto_rns_crt(uint64_t* result, uint64_t* output, int N2, int N1
     free(ta); free(tb); free(tmp); free(dec);
 }
 
+/* the giant steps of one sub-database on its scan output (output is INTT'd in place) */
+int ko_giant_steps(uint64_t* result, uint64_t* output, int N1, const uint64_t* giant) {
+    int N2 = N / 2 / N1;
+    memcpy(result, output, 8 * 2 * N);
+    eval_auto_rns_crt(result, output, N2, N1, giant);
+    return 0;
+}
+
 /* matrix_vector_mul_bsgs_rns_crt_large, twosteps.cpp:1527-1579 */
 int ko_matrix_vector_mul(const uint64_t* datacrt, int r, int N1, uint64_t* query_inout,
                          const uint64_t* baby, const uint64_t* giant, const int32_t* perms,

@@ -44,6 +44,10 @@ int ko_matrix_vector_mul(const uint64_t* datacrt, int r, int N1, uint64_t* query
                          const uint64_t* baby, const uint64_t* giant, const int32_t* perms,
                          uint64_t* result, uint64_t* cipherbuf_out);
 
+/* Giant steps of one sub-database (evalAutoRNSCRT, twosteps.cpp:599-677) on its
+ * scan output [N2][2][N] (NTT form, INTT'd in place): result [2][N]. */
+int ko_giant_steps(uint64_t* result, uint64_t* output, int N1, const uint64_t* giant);
+
 /* ext_inout += g^-1(first_dim) x rgsw; first_dim goes NTT -> coefficient form in place. */
 int ko_external_product(uint64_t* ext_inout, uint64_t* first_dim_inout, const uint64_t* rgsw);
 

@@ -77,6 +77,7 @@ def lib():
             L.ko_barrett_coeff.restype = ctypes.c_uint64
             L.ko_permutation_matrix.argtypes = [vp, ctypes.c_int]
             L.ko_pow_mod_index.argtypes = [ctypes.c_int, ctypes.c_int]
+            L.ko_giant_steps.argtypes = [vp, vp, ctypes.c_int, vp]
             _lib = L
     return _lib
 
@@ -183,6 +184,14 @@ def packing(rlwes, r, keys):
     if rc:
         raise RuntimeError(f"ko_packing rc={rc}")
     return resp
+
+
+def giant_steps(output, N1, giant):
+    """evalAutoRNSCRT of one sub-database on its scan output ([N2][2][N] words)."""
+    out = output.copy()
+    res = np.zeros(2 * N, dtype=np.uint64)
+    lib().ko_giant_steps(_p(res), _p(out), N1, _p(giant))
+    return res
 
 
 def scan(db_sub, cipherbuf, N1):
