@@ -108,6 +108,33 @@ int kspir_external_product(kspir_ctx* ctx, int client, uint64_t* result, uint64_
  * form).  Host buffers; rlwes is read only. */
 int kspir_packing_rlwes(kspir_ctx* ctx, int client, const uint64_t* rlwes, uint64_t* response);
 
+/* No counterpart in the reference.  The external product of
+ * kspir_external_product (reference externalProduct, lwe.cpp:761-808, with
+ * the RGSW parameters of test-pir.cpp:71) for callers that cannot allocate
+ * device memory -- e.g. a plugin whose host owns all device memory through its
+ * own pool, or code that must not trigger the device synchronisation that
+ * cudaMalloc/cudaFree can cause.  It calls no cudaMalloc, cudaFree or other
+ * allocating routine and needs no kspir_ctx.  All pointers are device memory
+ * owned by the caller:
+ *   d_rgsw      [4][2][N]       RGSW rows, NTT form
+ *   d_result    [count][2][N]   in: NTT-domain accumulators (zero for a fresh
+ *                               product); out: results, coefficient form
+ *   d_first_dim [count][2][N]   in: NTT form; out: coefficient form
+ * count <= KSPIR_NOALLOC_MAX_COUNT; larger counts are rejected with
+ * KSPIR_ERR_INVALID_ARG, as are non-canonical words (outputs then untouched).
+ * Work is enqueued on `stream` (a cudaStream_t, NULL = the legacy default
+ * stream) and the call returns after it completes.
+ * Scratch: a fixed file-scope device array of about 6.3 MiB (plus 192 KiB of
+ * transform tables) that every GPU loading this library holds until the
+ * process exits.  All calls on a device share it, so calls that overlap on
+ * the GPU (other threads, other streams) race and must be serialised by the
+ * caller.  The first call on each device also sets that device up (constant
+ * tables and the device address of the scratch array); make that first call
+ * before any stream capture. */
+#define KSPIR_NOALLOC_MAX_COUNT 16
+int kspir_external_product_noalloc(int device, const uint64_t* d_rgsw, uint64_t* d_result, uint64_t* d_first_dim,
+                                   int count, void* stream);
+
 /* Fills perms ([N1][N] int32) with the matrix the reference's
  * compute_permutation_matrix(permutations, N1, N) builds (utils.cpp:1591-1619):
  * row i is the NTT-slot gather that applies X -> X^(5^i).  No device needed. */

@@ -9,6 +9,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -865,3 +866,189 @@ int kspir_fetch_stage(kspir_ctx* c, int stage, uint64_t* out, size_t words) {
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// External product without any allocation (kspir_external_product_noalloc).
+//
+// Some callers cannot call cudaMalloc: a plugin inside a host process that owns
+// every byte of device memory through its own pool, code that runs while the
+// process must not synchronize the device (cudaMalloc/cudaFree can), or a
+// runtime that forbids allocation after start-up.  This entry point gives them
+// the external product with no allocation of any kind: its scratch is the
+// file-scope array below, which every GPU that loads this library holds until
+// the process exits.  The caller passes its inputs and outputs in device
+// memory it already owns.
+
+namespace {
+
+constexpr int kNoAllocMaxCount = 16;   // ciphertexts per call
+constexpr size_t kNaPoly = kN;         // u32 words per residue polynomial
+// per ciphertext: first_dim residues (4), accumulator residues (4), coefficient
+// form (4), digits (8), products (4) = 24 polynomials
+constexpr size_t kNaPerCt = 24 * kNaPoly;
+constexpr size_t kNaJobsWords = (size_t)kNoAllocMaxCount * 12 * sizeof(NttJob) / 4;
+constexpr size_t kNaScratchWords = (size_t)kNoAllocMaxCount * kNaPerCt   // per-ciphertext polynomials
+                                   + 16 * kNaPoly                         // RGSW residues [4][2][2][N]
+                                   + 64                                   // flag words
+                                   + kNaJobsWords;                        // transform job list
+
+// Scratch shared by every call on a device; it keeps the previous call's
+// contents.  Twiddle tables of the no-allocation path live beside it.
+static __device__ __align__(256) uint32_t g_na_scratch[kNaScratchWords];
+static __device__ __align__(256) uint32_t g_na_tw[3 * 4 * kN];
+
+struct NaDevice {
+    bool ready = false;
+    uint32_t* scratch = nullptr;   // device address of g_na_scratch on this device
+    uint32_t* tw = nullptr;        // device address of g_na_tw on this device
+};
+NaDevice g_na[64];
+std::mutex g_na_mutex;
+
+// twiddles psi^brv(k), psi^-brv(k) and Shoup companions, computed on the device
+__global__ void k_na_twiddles(uint32_t* tw, uint32_t q0, uint32_t q1, uint32_t q2, uint32_t p0, uint32_t p1,
+                              uint32_t p2) {
+    const int ch = blockIdx.y;
+    const uint32_t q = ch == 0 ? q0 : ch == 1 ? q1 : q2;
+    const uint32_t psi = ch == 0 ? p0 : ch == 1 ? p1 : p2;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < kN; k += gridDim.x * blockDim.x) {
+        uint32_t e = __brev((uint32_t)k) >> (32 - kLogN);
+        auto pw = [&](uint32_t x) {
+            uint64_t r = 1, b = psi;
+            while (x) {
+                if (x & 1) r = r * b % q;
+                b = b * b % q;
+                x >>= 1;
+            }
+            return (uint32_t)r;
+        };
+        uint32_t w = pw(e);
+        uint32_t iw = pw((2 * kN - e) % (2 * kN));   // psi^(2N) = 1
+        uint32_t* t = tw + (size_t)ch * 4 * kN;
+        t[k] = w;
+        t[kN + k] = (uint32_t)(((uint64_t)w << 32) / q);
+        t[2 * kN + k] = iw;
+        t[3 * kN + k] = (uint32_t)(((uint64_t)iw << 32) / q);
+    }
+}
+
+// job list for count <= kNoAllocMaxCount: inverse transforms of the first
+// kNoAllocMaxCount*4 polynomials, then forward transforms of the digits
+__global__ void k_na_jobs(NttJob* jobs, uint32_t* fd_res, uint32_t* ecoef, uint32_t* edig) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < kNoAllocMaxCount * 4) {
+        jobs[t].src = fd_res + (size_t)t * kN;
+        jobs[t].dst = ecoef + (size_t)t * kN;
+        jobs[t].ch = t & 1;
+        jobs[t].dst_stride = 1;
+    } else if (t < kNoAllocMaxCount * 12) {
+        const int u = t - kNoAllocMaxCount * 4;
+        jobs[t].src = edig + (size_t)u * kN;
+        jobs[t].dst = edig + (size_t)u * kN;
+        jobs[t].ch = u & 1;
+        jobs[t].dst_stride = 1;
+    }
+}
+
+struct NaLayout {
+    uint32_t *fd_res, *acc_res, *ecoef, *edig, *ext, *rgsw, *flag;
+    NttJob* jobs;
+};
+
+NaLayout na_layout(uint32_t* s) {
+    NaLayout L;
+    const size_t M = kNoAllocMaxCount;
+    L.fd_res = s;
+    L.acc_res = L.fd_res + M * 4 * kNaPoly;
+    L.ecoef = L.acc_res + M * 4 * kNaPoly;
+    L.edig = L.ecoef + M * 4 * kNaPoly;
+    L.ext = L.edig + M * 8 * kNaPoly;
+    L.rgsw = L.ext + M * 4 * kNaPoly;
+    L.flag = L.rgsw + 16 * kNaPoly;
+    L.jobs = reinterpret_cast<NttJob*>(L.flag + 64);
+    return L;
+}
+
+// Once per device, with that device current: constants, twiddles, job list,
+// and the device addresses of the static arrays.
+int na_setup(int device, cudaStream_t st) {
+    NaDevice& d = g_na[device];
+    if (d.ready) return KSPIR_OK;
+    if (cudaGetSymbolAddress((void**)&d.scratch, g_na_scratch) != cudaSuccess) return KSPIR_ERR_CUDA;
+    if (cudaGetSymbolAddress((void**)&d.tw, g_na_tw) != cudaSuccess) return KSPIR_ERR_CUDA;
+    DevConst dc{};
+    const uint32_t qs[3] = {kQ1, kQ2, kBsMod};
+    for (int ch = 0; ch < 3; ch++) {
+        ChanConst& cc = dc.ch[ch];
+        cc.q = qs[ch];
+        cc.two_q = 2 * qs[ch];
+        cc.barrett = ~0ull / qs[ch];
+        cc.ninv = (uint32_t)h_invmod(kN, qs[ch]);
+        cc.ninv_p = shoup32(cc.ninv, qs[ch]);
+        cc.bsinv = ch < 2 ? (uint32_t)(kBsModInvCrt % qs[ch]) : 0;
+        cc.bsinv_p = shoup32(cc.bsinv, qs[ch]);
+    }
+    dc.q1inv_mod_q2 = (uint32_t)h_invmod(kQ1 % kQ2, kQ2);
+    dc.q1inv_mod_q2_p = shoup32(dc.q1inv_mod_q2, kQ2);
+    if (cudaMemcpyToSymbolAsync(c_dev, &dc, sizeof(dc), 0, cudaMemcpyHostToDevice, st) != cudaSuccess)
+        return KSPIR_ERR_CUDA;
+    const uint64_t root_crt = 3375402822066082ull;
+    k_na_twiddles<<<dim3(16, 3), 256, 0, st>>>(d.tw, kQ1, kQ2, kBsMod, (uint32_t)(root_crt % kQ1),
+                                              (uint32_t)(root_crt % kQ2), (uint32_t)h_min_root(kBsMod));
+    NaLayout L = na_layout(d.scratch);
+    k_na_jobs<<<1, kNoAllocMaxCount * 12, 0, st>>>(L.jobs, L.fd_res, L.ecoef, L.edig);
+    if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess) return KSPIR_ERR_CUDA;
+    d.ready = true;
+    return KSPIR_OK;
+}
+
+}  // namespace
+
+extern "C" int kspir_external_product_noalloc(int device, const uint64_t* d_rgsw, uint64_t* d_result,
+                                              uint64_t* d_first_dim, int count, void* stream) {
+    if (device < 0 || device >= 64 || !d_rgsw || !d_result || !d_first_dim) return KSPIR_ERR_INVALID_ARG;
+    if (count < 1 || count > kNoAllocMaxCount) return KSPIR_ERR_INVALID_ARG;
+    int prev = 0;
+    if (cudaGetDevice(&prev) != cudaSuccess) return KSPIR_ERR_CUDA;
+    if (cudaSetDevice(device) != cudaSuccess) return KSPIR_ERR_CUDA;
+    cudaStream_t st = (cudaStream_t)stream;
+    int rc = KSPIR_OK;
+    {
+        std::lock_guard<std::mutex> lock(g_na_mutex);
+        rc = na_setup(device, st);
+    }
+    if (rc == KSPIR_OK) {
+        const NaDevice& d = g_na[device];
+        NaLayout L = na_layout(d.scratch);
+        NttTables tabs;
+        for (int ch = 0; ch < 3; ch++) tabs.tw[ch] = d.tw + (size_t)ch * 4 * kN;
+        GadgetS g;
+        g.ell = 2; g.base_bits = 20; g.gbits = 18;   // RGSW of test-pir.cpp:71
+        const size_t n = (size_t)count * 2 * kN;
+        cudaMemsetAsync(L.flag, 0, 64 * 4, st);   // the flag must start at zero on every call
+        k_check_canonical<<<64, 256, 0, st>>>(d_result, n, kCrtMod, (int*)L.flag);
+        k_check_canonical<<<64, 256, 0, st>>>(d_first_dim, n, kCrtMod, (int*)L.flag);
+        k_check_canonical<<<16, 256, 0, st>>>(d_rgsw, 8 * (size_t)kN, kCrtMod, (int*)L.flag);
+        k_split_words<<<blocks_for((long)n, 256), 256, 0, st>>>(d_first_dim, L.fd_res, count * 2);
+        k_split_words<<<blocks_for((long)n, 256), 256, 0, st>>>(d_result, L.acc_res, count * 2);
+        k_split_words<<<blocks_for(8L * kN, 256), 256, 0, st>>>(d_rgsw, L.rgsw, 8);
+        k_ntt_jobs<256, true><<<count * 4, 256, 0, st>>>(L.jobs, tabs);
+        k_ext_decomp<<<blocks_for((long)count * kN, 256), 256, 0, st>>>(L.ecoef, L.edig, count, g);
+        k_ntt_jobs<256, false><<<count * 8, 256, 0, st>>>(L.jobs + kNoAllocMaxCount * 4, tabs);
+        k_ext_mac_intt<512><<<count * 4, 512, 0, st>>>(L.edig, L.rgsw, L.acc_res, L.ext, 4, tabs);
+        int flag = 0;
+        if (cudaGetLastError() != cudaSuccess ||
+            cudaMemcpyAsync(&flag, L.flag, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess) {
+            rc = KSPIR_ERR_CUDA;
+        } else if (flag) {
+            rc = KSPIR_ERR_INVALID_ARG;   // outputs left untouched
+        } else {
+            k_compose_words<<<blocks_for((long)n, 256), 256, 0, st>>>(L.ext, d_result, count * 2);
+            k_compose_words<<<blocks_for((long)n, 256), 256, 0, st>>>(L.ecoef, d_first_dim, count * 2);
+            if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess) rc = KSPIR_ERR_CUDA;
+        }
+    }
+    cudaSetDevice(prev);
+    return rc;
+}

@@ -52,6 +52,7 @@ SIGNATURES = {
     "kspir_last_timing": (_i, [_vp, _vp, _vp]),
     "kspir_fetch_stage": (_i, [_vp, _i, _vp, _sz]),
     "kspir_permutation_matrix": (_i, [_vp, _i]),
+    "kspir_external_product_noalloc": (_i, [_i, _vp, _vp, _vp, _i, _vp]),
     "kspir_timing_reset": (_i, [_vp]),
     "kspir_timing_summary": (_i, [_vp, _vp, _vp, _vp, _vp]),
 }
