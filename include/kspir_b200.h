@@ -52,7 +52,7 @@ typedef struct kspir_ctx kspir_ctx;
 
 typedef struct kspir_params {
     int32_t r;            /* packing number = number of sub-databases, power of two, 1..512 */
-    int32_t N1;           /* baby steps, power of two, 32..512; N2 = N/2/N1 */
+    int32_t N1;           /* baby steps, power of two, 64..512; N2 = N/2/N1 */
     int32_t max_clients;  /* client key slots held on the device */
     int32_t max_inflight; /* concurrent query workspaces (1 for the plain path) */
 } kspir_params;
@@ -60,7 +60,7 @@ typedef struct kspir_params {
 /* Context bound to one CUDA device.  Allocates the per-query workspaces. */
 int kspir_ctx_create(int device, const kspir_params* params, kspir_ctx** out);
 int kspir_ctx_destroy(kspir_ctx* ctx);
-const char* kspir_last_error(const kspir_ctx* ctx);
+const char* kspir_last_error(const kspir_ctx* ctx);   /* NULL: the calling thread's last error */
 const char* kspir_strerror(int code);
 
 /* Replaces the datacrt argument of matrix_vector_mul_bsgs_rns_crt_large

@@ -38,7 +38,6 @@ struct BabyArgs {
     int32_t N1;
     int32_t col_base;        // cipherbuf column of key index 0
     int32_t inter_idx;       // key index whose pre-modswitch state is exported, or -1
-    int32_t ell;
 };
 
 // 5^e mod 2N
@@ -52,91 +51,102 @@ __device__ __forceinline__ uint32_t pow5_mod2n(uint32_t e) {
     return r;
 }
 
-template <int T>
-__global__ void __launch_bounds__(T) k_baby_rot(BabyArgs a, ClientKeysDev keys, NttTables tabs) {
-    extern __shared__ uint32_t sm[];
-    uint32_t* Sa = sm;
-    uint32_t* Sb = sm + kN;
-    uint32_t* W = sm + 2 * kN;
-    uint32_t* Ra = sm + 3 * kN;
-    uint32_t* Rb = sm + 4 * kN;
+constexpr int kBabySmem = kN * 8 + kN * 4;   // twiddles + one polynomial
+constexpr int kPerThread = kN / kNttThreads; // 8 coefficients per thread
 
-    const int ki = blockIdx.x;                 // key index: rotation by 5^(ki+1)
+// One CTA per (rotation, component, crt prime): blockIdx.x = 4*ki + 2*comp + ch.
+// Each CTA recomputes the bsMod part of its component (one inverse transform)
+// so the four CTAs of a rotation run in parallel.
+template <int ELL>
+__global__ void __launch_bounds__(kNttThreads) k_baby_rot(BabyArgs a, ClientKeysDev keys, NttTables tabs) {
+    extern __shared__ __align__(16) uint8_t smem_raw[];
+    uint2* tws = reinterpret_cast<uint2*>(smem_raw);
+    uint32_t* S = reinterpret_cast<uint32_t*>(smem_raw + kN * 8);
+
+    const int ki = blockIdx.x >> 2;            // key index: rotation by 5^(ki+1)
+    const int comp = (blockIdx.x >> 1) & 1;    // 0 = a, 1 = b
+    const int ch = blockIdx.x & 1;             // crt prime
     const int col = a.col_base + ki;
     const bool inter = (ki == a.inter_idx);
-    const int ell = a.ell;
+    const int tid = threadIdx.x;
     const int32_t* __restrict__ perm = a.perms + (size_t)(ki + 1) * kN;
-    const uint16_t* __restrict__ sig = a.sigma + (size_t)ki * kN;
-    const uint32_t* __restrict__ kbs = keys.baby_bs + (size_t)ki * ell * 2 * kN;
-    const uint32_t* __restrict__ kcrt = keys.baby_crt + (size_t)ki * ell * 2 * 2 * kN;
+    const uint32_t* __restrict__ kbs = keys.baby_bs + (size_t)ki * ELL * 2 * kN;
+    const uint32_t* __restrict__ kcrt = keys.baby_crt + (size_t)ki * ELL * 2 * 2 * kN;
     const uint32_t* __restrict__ dig = a.dig;
-    const ChanConst cb = c_dev.ch[CH_BS];
 
-    // bsMod channel: A_bs, B_bs
-    for (int k = threadIdx.x; k < kN; k += T) {
-        const int p = perm[k];
-        uint64_t sa = 0, sb = 0;
-        for (int j = 0; j < ell; j++) {
-            const uint64_t d = dig[(j * 3 + CH_BS) * kN + p];
-            sa += d * kbs[(j * 2 + 0) * kN + k];
-            sb += d * kbs[(j * 2 + 1) * kN + k];
+    stage_twiddles(tws, tabs, CH_BS, NTT_INV);
+    int pk[kPerThread];
+#pragma unroll
+    for (int it = 0; it < kPerThread; it++) pk[it] = __ldg(perm + tid + it * kNttThreads);
+
+    // bsMod part of this component: -sum_j d_j[perm] * key_j
+    {
+        const ChanConst cb = c_dev.ch[CH_BS];
+        uint64_t acc[kPerThread];
+#pragma unroll
+        for (int it = 0; it < kPerThread; it++) acc[it] = 0;
+#pragma unroll
+        for (int j = 0; j < ELL; j++) {
+            const uint32_t* d = dig + (size_t)(j * 3 + CH_BS) * kN;
+            const uint32_t* kk = kbs + (size_t)(j * 2 + comp) * kN;
+#pragma unroll
+            for (int it = 0; it < kPerThread; it++)
+                acc[it] += (uint64_t)__ldg(d + pk[it]) * __ldg(kk + tid + it * kNttThreads);
         }
-        Sa[k] = negmod(reduce64(sa, cb.q, cb.barrett), cb.q);
-        Sb[k] = negmod(reduce64(sb, cb.q, cb.barrett), cb.q);
+#pragma unroll
+        for (int it = 0; it < kPerThread; it++)
+            S[tid + it * kNttThreads] = negmod(reduce64(acc[it], cb.q, cb.barrett), cb.q);
     }
-    cta_ntt_inverse<T>(Sa, tabs.tw[CH_BS], CH_BS);
-    cta_ntt_inverse<T>(Sb, tabs.tw[CH_BS], CH_BS);
+    cta_ntt_inverse(S, tws, CH_BS);
 
-    // x2b += auto_g(b mod bsMod)   (automorphic_rns, twosteps.cpp:1045-1048)
-    const uint32_t ginv = pow5_mod2n(2048u - (uint32_t)(ki + 1));
-    for (int k = threadIdx.x; k < kN; k += T) {
-        bool neg;
-        const int src = auto_src(k, ginv, &neg);
-        uint32_t v = a.srcBbs[src];
-        if (neg) v = negmod(v, cb.q);
-        Sb[k] = addmod(Sb[k], v, cb.q);
-        if (inter) {
-            a.inter_bs[k] = Sa[k];
-            a.inter_bs[kN + k] = Sb[k];
+    if (comp == 1) {
+        // x2b += auto_g(b mod bsMod)   (automorphic_rns, twosteps.cpp:1045-1048)
+        const uint32_t ginv = pow5_mod2n(2048u - (uint32_t)(ki + 1));
+        const uint32_t qb = c_dev.ch[CH_BS].q;
+#pragma unroll
+        for (int it = 0; it < kPerThread; it++) {
+            const int k = tid + it * kNttThreads;
+            bool neg;
+            const int src = auto_src(k, ginv, &neg);
+            uint32_t v = __ldg(a.srcBbs + src);
+            if (neg) v = negmod(v, qb);
+            S[k] = addmod(S[k], v, qb);
         }
     }
-    __syncthreads();
+    if (inter && ch == 0) {
+#pragma unroll
+        for (int it = 0; it < kPerThread; it++) {
+            const int k = tid + it * kNttThreads;
+            a.inter_bs[comp * kN + k] = S[k];
+        }
+    }
+    __syncthreads();   // S complete and the inverse twiddles no longer read
+    stage_twiddles(tws, tabs, ch, NTT_FWD);
+    cta_ntt_forward(S, tws, ch);   // NTT_ch(x2), x2 < bsMod < q
 
-    uint64_t* __restrict__ cbuf = a.cipherbuf;
-#pragma unroll 1
-    for (int ch = CH_Q1; ch <= CH_Q2; ch++) {
-        const ChanConst cc = c_dev.ch[ch];
-        // a component
-        for (int k = threadIdx.x; k < kN; k += T) W[k] = Sa[k];
-        cta_ntt_forward<T>(W, tabs.tw[ch], ch);
-        for (int k = threadIdx.x; k < kN; k += T) {
-            const int p = perm[k];
-            uint64_t s = 0;
-            for (int j = 0; j < ell; j++)
-                s += (uint64_t)dig[(j * 3 + ch) * kN + p] * kcrt[((j * 2 + 0) * 2 + ch) * kN + k];
-            const uint32_t A = negmod(reduce64(s, cc.q, cc.barrett), cc.q);
-            if (inter) a.interA[ch * kN + k] = A;
-            const uint32_t ra = shoup_mul(submod(A, W[k], cc.q), cc.bsinv, cc.bsinv_p, cc.q);
-            if (ch == CH_Q1) Ra[k] = ra;
-            else cbuf[((size_t)k * a.N1 + col) * 2 + 0] = (uint64_t)Ra[k] | ((uint64_t)ra << 32);
-        }
-        __syncthreads();
-        // b component
-        for (int k = threadIdx.x; k < kN; k += T) W[k] = Sb[k];
-        cta_ntt_forward<T>(W, tabs.tw[ch], ch);
-        for (int k = threadIdx.x; k < kN; k += T) {
-            const int p = perm[k];
-            uint64_t s = 0;
-            for (int j = 0; j < ell; j++)
-                s += (uint64_t)dig[(j * 3 + ch) * kN + p] * kcrt[((j * 2 + 1) * 2 + ch) * kN + k];
-            const uint32_t Bn = negmod(reduce64(s, cc.q, cc.barrett), cc.q);
-            const uint32_t Bt = addmod(Bn, a.srcB[ch * kN + sig[k]], cc.q);
-            if (inter) a.interB[ch * kN + k] = Bt;
-            const uint32_t rb = shoup_mul(submod(Bt, W[k], cc.q), cc.bsinv, cc.bsinv_p, cc.q);
-            if (ch == CH_Q1) Rb[k] = rb;
-            else cbuf[((size_t)k * a.N1 + col) * 2 + 1] = (uint64_t)Rb[k] | ((uint64_t)rb << 32);
-        }
-        __syncthreads();
+    const ChanConst cc = c_dev.ch[ch];
+    const uint16_t* __restrict__ sig = a.sigma + (size_t)ki * kN;
+    uint64_t acc[kPerThread];
+#pragma unroll
+    for (int it = 0; it < kPerThread; it++) acc[it] = 0;
+#pragma unroll
+    for (int j = 0; j < ELL; j++) {
+        const uint32_t* d = dig + (size_t)(j * 3 + ch) * kN;
+        const uint32_t* kk = kcrt + (size_t)((j * 2 + comp) * 2 + ch) * kN;
+#pragma unroll
+        for (int it = 0; it < kPerThread; it++)
+            acc[it] += (uint64_t)__ldg(d + pk[it]) * __ldg(kk + tid + it * kNttThreads);
+    }
+    uint32_t* cb32 = reinterpret_cast<uint32_t*>(a.cipherbuf);
+    uint32_t* inter_out = comp == 0 ? a.interA : a.interB;
+#pragma unroll
+    for (int it = 0; it < kPerThread; it++) {
+        const int k = tid + it * kNttThreads;
+        uint32_t A = negmod(reduce64(acc[it], cc.q, cc.barrett), cc.q);
+        if (comp == 1) A = addmod(A, __ldg(a.srcB + ch * kN + sig[k]), cc.q);
+        if (inter) inter_out[ch * kN + k] = A;
+        const uint32_t r = shoup_mul(submod(A, S[k], cc.q), cc.bsinv, cc.bsinv_p, cc.q);
+        cb32[(((size_t)k * a.N1 + col) * 2 + comp) * 2 + ch] = r;
     }
 }
 

@@ -6,16 +6,22 @@
 // (reorientCipher).  For every sub-database r, NTT slot z and giant row i:
 //   a_lo = sum_k lo(DB) * lo(a_k)      a_hi = sum_k hi(DB) * hi(a_k)
 //   b_lo = sum_k lo(DB) * lo(b_k)      b_hi = sum_k hi(DB) * hi(b_k)
-// exact 64-bit sums (products < 2^56, N1 <= 128 terms -> < 2^63), and the
-// reference composes out = crt_compose(a_lo, a_hi), which is the canonical
-// crtMod value with residues (a_lo mod q1, a_hi mod q2).  The kernel stores
-// those residues directly: sout[r][i][comp][ch][z].
+// exact 64-bit sums (products < 2^56, N1 <= 512 terms; any wrap mod 2^64 is
+// the reference's too), and the reference composes out = crt_compose(a_lo,
+// a_hi), which is the canonical crtMod value with residues (a_lo mod q1,
+// a_hi mod q2).  The kernel stores those residues: sout[r][i][comp][ch][z].
 //
 // Data movement: one 16 KiB slab DB[r][z] (N2 x N1 words) plus the 16*N1-byte
-// cipherbuf row z per work item, brought in by 1-D bulk copies (TMA engine)
-// into an NST-deep shared-memory ring; a producer warp issues, 8 consumer warps
-// (4 groups of 64 threads, one item per group) multiply-accumulate with
-// IMAD.WIDE and reduce across the TPR = N1/32 threads that share a row.
+// cipherbuf row z per work item, brought in by 1-D bulk copies (TMA engine,
+// no multicast) into an NST-deep shared-memory ring (12 stages at N1 = 128);
+// one producer warp issues, CONS consumer warps each take one item at a time.
+//
+// Consumer mapping (one warp per slab): lane = 8 * r + c covers rows
+// {r, r+4, ...} and 16-byte chunks {c, c+8, ...}.  Eight lanes of a row read
+// 128 contiguous bytes of it (no bank conflicts), the four lanes that share a
+// chunk read the same cipherbuf bytes (broadcast), and each cipherbuf chunk is
+// loaded once per lane and reused across its rows.  Partial sums are reduced
+// across the eight lanes of a row with shuffles.
 #pragma once
 
 #include "common.cuh"
@@ -23,35 +29,45 @@
 
 namespace kspir {
 
-constexpr int kScanThreads = 288;            // 8 consumer warps + 1 producer warp
-constexpr int kScanStages = 8;
-constexpr int kScanGroups = 4;
-constexpr uint64_t kWaitLimitNs = 2000000000ull;   // 2 s per bounded wait
+constexpr uint64_t kWaitLimitNs = 2000000000ull;     // 2 s per bounded wait
+
+// Stage ownership: consumer warp w takes items w, w + CONS, ... and stage
+// j % NST with NST a multiple of CONS, so every stage belongs to one warp and
+// that warp never waits more than one phase ahead of the barrier (an mbarrier
+// parity wait cannot tell phase u-1 from u+1).
 
 template <int N1>
 struct ScanCfg {
     static constexpr int N2 = kN / 2 / N1;
-    static constexpr int TPR = N1 / 32;                 // threads per row
+    static constexpr int CHUNKS = N1 / 2;               // 16-byte chunks per row
+    static constexpr int RPL = N2 / 4;                  // rows per lane
+    static constexpr int CPL = CHUNKS / 8;              // chunks per lane
     static constexpr int SLAB = kN / 2 * 8;             // DB bytes per item
     static constexpr int QSLAB = 2 * N1 * 8;            // cipherbuf bytes per item
     static constexpr int STAGE = SLAB + QSLAB;
-    static constexpr int SMEM = kScanStages * STAGE + 2 * kScanStages * 8;
+    static constexpr int CONS = N1 <= 128 ? 6 : 4;      // consumer warps
+    static constexpr int NST = N1 <= 128 ? 12 : 8;      // ring stages, a multiple of CONS
+    static constexpr int THREADS = 32 * (CONS + 1);
+    static constexpr int SMEM = NST * STAGE + 2 * NST * 8;
+    static_assert(NST % CONS == 0, "stages must be owned by one consumer warp each");
+    static_assert(SMEM <= 227 * 1024, "shared memory budget");
+    static_assert(RPL >= 1 && CPL >= 1, "N1 must be in [64, 512]");
 };
 
 template <int N1>
-__global__ void __launch_bounds__(kScanThreads, 1)
+__global__ void __launch_bounds__(ScanCfg<N1>::THREADS, 1)
     k_scan(const uint64_t* __restrict__ db, const uint64_t* __restrict__ cbuf, uint32_t* __restrict__ sout,
            int R, int* __restrict__ err) {
     using C = ScanCfg<N1>;
     extern __shared__ __align__(128) uint8_t smem[];
-    uint64_t* full = reinterpret_cast<uint64_t*>(smem + kScanStages * C::STAGE);
-    uint64_t* empty = full + kScanStages;
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + C::NST * C::STAGE);
+    uint64_t* empty = full + C::NST;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
     if (tid == 0) {
-        for (int s = 0; s < kScanStages; s++) {
+        for (int s = 0; s < C::NST; s++) {
             mbar_init(&full[s], 1);
-            mbar_init(&empty[s], 2);   // the two consumer warps of the owning group
+            mbar_init(&empty[s], 1);   // the consuming warp
         }
         fence_mbar_init();
     }
@@ -60,14 +76,14 @@ __global__ void __launch_bounds__(kScanThreads, 1)
     const long total = (long)R * kN;
     const long nloc = blockIdx.x < total ? (total - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
 
-    if (warp == 8) {
+    if (warp == C::CONS) {
         // producer
         if (lane == 0) {
             long issued = 0;
             for (long j = 0; j < nloc; j++) {
-                const int s = (int)(j % kScanStages);
-                if (j >= kScanStages) {
-                    const uint32_t par = (uint32_t)((j / kScanStages - 1) & 1);
+                const int s = (int)(j % C::NST);
+                if (j >= C::NST) {
+                    const uint32_t par = (uint32_t)((j / C::NST - 1) & 1);
                     if (!mbar_wait_bounded(&empty[s], par, kWaitLimitNs)) {
                         atomicOr(err, 1);
                         break;
@@ -82,65 +98,70 @@ __global__ void __launch_bounds__(kScanThreads, 1)
                 issued = j + 1;
             }
             // never leave the CTA with copies in flight into its shared memory
-            const long first = issued > kScanStages ? issued - kScanStages : 0;
+            const long first = issued > C::NST ? issued - C::NST : 0;
             for (long j = first; j < issued; j++)
-                if (!mbar_wait_bounded(&full[j % kScanStages], (uint32_t)((j / kScanStages) & 1), kWaitLimitNs))
+                if (!mbar_wait_bounded(&full[j % C::NST], (uint32_t)((j / C::NST) & 1), kWaitLimitNs))
                     atomicOr(err, 4);
         }
         return;
     }
 
     // consumers
-    const int g = warp >> 1;              // slab group
-    const int t = tid & 63;               // thread within group
-    const int i = t / C::TPR;             // giant row
-    const int qd = t % C::TPR;            // quarter within row
-    for (long j = g; j < nloc; j += kScanGroups) {
-        const int s = (int)(j % kScanStages);
-        if (!mbar_wait_bounded(&full[s], (uint32_t)((j / kScanStages) & 1), kWaitLimitNs)) {
+    const int lr = lane >> 3;    // row lane 0..3
+    const int lc = lane & 7;     // chunk lane 0..7
+    for (long j = warp; j < nloc; j += C::CONS) {
+        const int s = (int)(j % C::NST);
+        if (!mbar_wait_bounded(&full[s], (uint32_t)((j / C::NST) & 1), kWaitLimitNs)) {
             atomicOr(err, 2);
             break;
         }
         const uint8_t* st = smem + (size_t)s * C::STAGE;
-        const uint64_t* D = reinterpret_cast<const uint64_t*>(st) + (size_t)i * N1;
-        const uint64_t* Qs = reinterpret_cast<const uint64_t*>(st + C::SLAB);
-        uint64_t alo = 0, ahi = 0, blo = 0, bhi = 0;
+        const uint4* D4 = reinterpret_cast<const uint4*>(st);             // [N2][CHUNKS] chunks of 2 words
+        const uint4* Q4 = reinterpret_cast<const uint4*>(st + C::SLAB);   // [N1] (a_k, b_k) pairs
+        uint64_t acc[C::RPL][4];
 #pragma unroll
-        for (int m = 0; m < 16; m++) {
-            // 16-byte chunk of the row, rotated by the row index so that the
-            // lanes of different rows hit different banks
-            const int kc = qd + C::TPR * ((m + i) & 15);
-            const uint4 w = *reinterpret_cast<const uint4*>(D + 2 * kc);
-            const uint4 qa = *reinterpret_cast<const uint4*>(Qs + 4 * kc);
-            const uint4 qb = *reinterpret_cast<const uint4*>(Qs + 4 * kc + 2);
-            alo += (uint64_t)w.x * qa.x;
-            alo += (uint64_t)w.z * qb.x;
-            ahi += (uint64_t)w.y * qa.y;
-            ahi += (uint64_t)w.w * qb.y;
-            blo += (uint64_t)w.x * qa.z;
-            blo += (uint64_t)w.z * qb.z;
-            bhi += (uint64_t)w.y * qa.w;
-            bhi += (uint64_t)w.w * qb.w;
+        for (int rr = 0; rr < C::RPL; rr++) acc[rr][0] = acc[rr][1] = acc[rr][2] = acc[rr][3] = 0;
+#pragma unroll
+        for (int cc = 0; cc < C::CPL; cc++) {
+            const int kc = lc + 8 * cc;                   // chunk = words 2kc, 2kc+1
+            const uint4 qa = Q4[2 * kc];                  // (a_2kc, b_2kc)
+            const uint4 qb = Q4[2 * kc + 1];              // (a_2kc+1, b_2kc+1)
+#pragma unroll
+            for (int rr = 0; rr < C::RPL; rr++) {
+                const uint4 w = D4[(lr + 4 * rr) * C::CHUNKS + kc];
+                acc[rr][0] += (uint64_t)w.x * qa.x;
+                acc[rr][0] += (uint64_t)w.z * qb.x;
+                acc[rr][1] += (uint64_t)w.y * qa.y;
+                acc[rr][1] += (uint64_t)w.w * qb.y;
+                acc[rr][2] += (uint64_t)w.x * qa.z;
+                acc[rr][2] += (uint64_t)w.z * qb.z;
+                acc[rr][3] += (uint64_t)w.y * qa.w;
+                acc[rr][3] += (uint64_t)w.w * qb.w;
+            }
         }
         __syncwarp();
         if (lane == 0) mbar_arrive(&empty[s]);
 #pragma unroll
-        for (int off = 1; off < C::TPR; off <<= 1) {
-            alo += __shfl_xor_sync(0xffffffffu, alo, off);
-            ahi += __shfl_xor_sync(0xffffffffu, ahi, off);
-            blo += __shfl_xor_sync(0xffffffffu, blo, off);
-            bhi += __shfl_xor_sync(0xffffffffu, bhi, off);
-        }
+        for (int rr = 0; rr < C::RPL; rr++)
+#pragma unroll
+            for (int v = 0; v < 4; v++) {
+                uint64_t x = acc[rr][v];
+                x += __shfl_xor_sync(0xffffffffu, x, 1);
+                x += __shfl_xor_sync(0xffffffffu, x, 2);
+                x += __shfl_xor_sync(0xffffffffu, x, 4);
+                acc[rr][v] = x;
+            }
         const long it = blockIdx.x + j * gridDim.x;
         const long r = it / kN, z = it % kN;
-        uint32_t* o = sout + ((size_t)(r * C::N2 + i) * 4) * kN + z;
-        for (int oi = qd; oi < 4; oi += C::TPR) {
-            uint32_t v;
-            if (oi == 0) v = mod_q1(alo);
-            else if (oi == 1) v = mod_q2(ahi);
-            else if (oi == 2) v = mod_q1(blo);
-            else v = mod_q2(bhi);
-            o[(size_t)oi * kN] = v;   // [comp][ch]: 0 = a q1, 1 = a q2, 2 = b q1, 3 = b q2
+        // RPL rows x 4 outputs per row lane, spread over its 8 chunk lanes
+#pragma unroll
+        for (int o = 0; o < C::RPL * 4; o++) {
+            if ((o & 7) != lc) continue;
+            const int rr = o >> 2, v = o & 3;
+            const int i = lr + 4 * rr;
+            const uint64_t x = acc[rr][v];
+            const uint32_t res = (v & 1) ? mod_q2(x) : mod_q1(x);   // v: 0 = a q1, 1 = a q2, 2 = b q1, 3 = b q2
+            sout[((size_t)(r * C::N2 + i) * 4 + v) * kN + z] = res;
         }
     }
 }

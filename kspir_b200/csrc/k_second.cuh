@@ -63,6 +63,7 @@ __global__ void k_giant_accum(const uint32_t* __restrict__ sout, const uint32_t*
     const uint32_t* so = sout + (size_t)r * N2 * 4 * kN;      // [N2][2 comp][2 ch][N]
     uint32_t ra = so[(0 * 2 + ch) * kN + k];
     uint32_t rb = so[(1 * 2 + ch) * kN + k];
+#pragma unroll 5
     for (int c = 1; c < N2; c++) {
         const uint32_t* d = gdig + ((size_t)r * (N2 - 1) + (c - 1)) * ell * 2 * kN;
         const uint32_t* key = gkeys + (size_t)(c - 1) * ell * 2 * 2 * kN;
@@ -107,18 +108,25 @@ __global__ void k_ext_decomp(const uint32_t* __restrict__ ecoef, uint32_t* __res
     }
 }
 
+// dynamic shared memory of the fused multiply-accumulate + inverse-transform kernels
+constexpr int kMacSmem = kN * 8 + kN * 4;
+
 // One CTA per (r, comp, ch): ext = INTT( init + sum_row digit_row * rgsw[row].comp ),
 // init being the caller's NTT-domain accumulator (zero on the answer path,
 // test-pir.cpp:102-104) or null.
-template <int T>
-__global__ void __launch_bounds__(T) k_ext_mac_intt(const uint32_t* __restrict__ edig,
-                                                    const uint32_t* __restrict__ rgsw,
-                                                    const uint32_t* __restrict__ init,
-                                                    uint32_t* __restrict__ ext, int rows, NttTables tabs) {
-    __shared__ uint32_t s[kN];
+__global__ void __launch_bounds__(kNttThreads) k_ext_mac_intt(const uint32_t* __restrict__ edig,
+                                                              const uint32_t* __restrict__ rgsw,
+                                                              const uint32_t* __restrict__ init,
+                                                              uint32_t* __restrict__ ext, int rows, NttTables tabs) {
+    extern __shared__ __align__(16) uint8_t smem_raw[];
+    uint2* tws = reinterpret_cast<uint2*>(smem_raw);
+    uint32_t* s = reinterpret_cast<uint32_t*>(smem_raw + kN * 8);
+    constexpr int T = kNttThreads;
     const int ch = blockIdx.x % 2, comp = (blockIdx.x / 2) % 2, r = blockIdx.x / 4;
     const ChanConst cc = c_dev.ch[ch];
+    stage_twiddles(tws, tabs, ch, NTT_INV);
     const uint32_t* d = edig + (size_t)r * rows * 2 * kN;
+#pragma unroll
     for (int k = threadIdx.x; k < kN; k += T) {
         uint64_t acc = 0;
         for (int row = 0; row < rows; row++)
@@ -126,8 +134,9 @@ __global__ void __launch_bounds__(T) k_ext_mac_intt(const uint32_t* __restrict__
         const uint32_t m = reduce64(acc, cc.q, cc.barrett);
         s[k] = init ? addmod(init[((size_t)r * 4 + comp * 2 + ch) * kN + k], m, cc.q) : m;
     }
-    cta_ntt_inverse<T>(s, tabs.tw[ch], ch);
+    cta_ntt_inverse(s, tws, ch);
     uint32_t* o = ext + ((size_t)r * 4 + comp * 2 + ch) * kN;
+#pragma unroll
     for (int k = threadIdx.x; k < kN; k += T) o[k] = s[k];
 }
 
@@ -185,16 +194,20 @@ __global__ void k_pack_prep(const uint32_t* __restrict__ ext, uint32_t* __restri
 // and the final addAndEqual of convertTwoRLWEs:
 //   a' = -sum_d dig_d * key[d].a,  b' = NTT(temp.b) - sum_d dig_d * key[d].b,
 //   rlwes[j] = INTT(a', b') + c2.
-template <int T>
-__global__ void __launch_bounds__(T) k_pack_mac_intt(const uint32_t* __restrict__ pdig,
-                                                     const uint32_t* __restrict__ ptb,
-                                                     const uint32_t* __restrict__ pc2,
-                                                     const uint32_t* __restrict__ key,
-                                                     uint32_t* __restrict__ ext, int ell, NttTables tabs) {
-    __shared__ uint32_t s[kN];
+__global__ void __launch_bounds__(kNttThreads) k_pack_mac_intt(const uint32_t* __restrict__ pdig,
+                                                               const uint32_t* __restrict__ ptb,
+                                                               const uint32_t* __restrict__ pc2,
+                                                               const uint32_t* __restrict__ key,
+                                                               uint32_t* __restrict__ ext, int ell, NttTables tabs) {
+    extern __shared__ __align__(16) uint8_t smem_raw[];
+    uint2* tws = reinterpret_cast<uint2*>(smem_raw);
+    uint32_t* s = reinterpret_cast<uint32_t*>(smem_raw + kN * 8);
+    constexpr int T = kNttThreads;
     const int ch = blockIdx.x % 2, comp = (blockIdx.x / 2) % 2, j = blockIdx.x / 4;
     const ChanConst cc = c_dev.ch[ch];
+    stage_twiddles(tws, tabs, ch, NTT_INV);
     const uint32_t* d = pdig + (size_t)j * ell * 2 * kN;
+#pragma unroll
     for (int k = threadIdx.x; k < kN; k += T) {
         uint64_t acc = 0;
         for (int dd = 0; dd < ell; dd++)
@@ -202,9 +215,10 @@ __global__ void __launch_bounds__(T) k_pack_mac_intt(const uint32_t* __restrict_
         const uint32_t m = reduce64(acc, cc.q, cc.barrett);
         s[k] = comp == 0 ? negmod(m, cc.q) : submod(ptb[((size_t)j * 2 + ch) * kN + k], m, cc.q);
     }
-    cta_ntt_inverse<T>(s, tabs.tw[ch], ch);
+    cta_ntt_inverse(s, tws, ch);
     const uint32_t* c2 = pc2 + ((size_t)j * 4 + comp * 2 + ch) * kN;
     uint32_t* o = ext + ((size_t)j * 4 + comp * 2 + ch) * kN;
+#pragma unroll
     for (int k = threadIdx.x; k < kN; k += T) o[k] = addmod(s[k], c2[k], cc.q);
 }
 

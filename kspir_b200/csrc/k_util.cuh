@@ -16,20 +16,28 @@ struct NttJob {
     int32_t dst_stride;
 };
 
-template <int T, bool INVERSE>
-__global__ void __launch_bounds__(T) k_ntt_jobs(const NttJob* __restrict__ jobs, NttTables tabs) {
-    __shared__ uint32_t s[kN];
+// dynamic shared memory: 16 KiB polynomial + 32 KiB twiddles
+constexpr int kNttJobSmem = kN * 4 + kN * 8;
+
+template <bool INVERSE>
+__global__ void __launch_bounds__(kNttThreads) k_ntt_jobs(const NttJob* __restrict__ jobs, NttTables tabs) {
+    extern __shared__ __align__(16) uint8_t smem_raw[];
+    uint2* tws = reinterpret_cast<uint2*>(smem_raw);
+    uint32_t* s = reinterpret_cast<uint32_t*>(smem_raw + kN * 8);
     const NttJob jb = jobs[blockIdx.x];
+    stage_twiddles(tws, tabs, jb.ch, INVERSE ? NTT_INV : NTT_FWD);
     const uint4* src4 = reinterpret_cast<const uint4*>(jb.src);
     uint4* s4 = reinterpret_cast<uint4*>(s);
-    for (int k = threadIdx.x; k < kN / 4; k += T) s4[k] = src4[k];
-    if (INVERSE) cta_ntt_inverse<T>(s, tabs.tw[jb.ch], jb.ch);
-    else cta_ntt_forward<T>(s, tabs.tw[jb.ch], jb.ch);
+#pragma unroll
+    for (int k = threadIdx.x; k < kN / 4; k += kNttThreads) s4[k] = src4[k];
+    if (INVERSE) cta_ntt_inverse(s, tws, jb.ch);
+    else cta_ntt_forward(s, tws, jb.ch);
     if (jb.dst_stride == 1) {
         uint4* dst4 = reinterpret_cast<uint4*>(jb.dst);
-        for (int k = threadIdx.x; k < kN / 4; k += T) dst4[k] = s4[k];
+#pragma unroll
+        for (int k = threadIdx.x; k < kN / 4; k += kNttThreads) dst4[k] = s4[k];
     } else {
-        for (int k = threadIdx.x; k < kN; k += T) jb.dst[(size_t)k * jb.dst_stride] = s[k];
+        for (int k = threadIdx.x; k < kN; k += kNttThreads) jb.dst[(size_t)k * jb.dst_stride] = s[k];
     }
 }
 

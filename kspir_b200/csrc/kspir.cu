@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <array>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -166,6 +167,11 @@ struct kspir_ctx {
     int nsm = 148;
     std::vector<ClientSlot> clients;
     std::vector<WsSlot> ws;
+    // CUDA graphs of the four non-scan phases, per (workspace, client)
+    struct PhaseGraphs { bool ready = false; cudaGraphExec_t g[4] = {nullptr, nullptr, nullptr, nullptr}; };
+    std::vector<PhaseGraphs> graphs;   // [ws * max_clients + client]
+    cudaStream_t capture = nullptr;
+    bool use_graphs = true;
     // phase events of recent answers: ring[i][0..5] brackets baby / scan / giant / ext / packing
     std::vector<std::array<cudaEvent_t, 6>> ring;
     long answers = 0;          // answers enqueued since the last kspir_timing_reset
@@ -175,8 +181,11 @@ struct kspir_ctx {
 
 namespace {
 
+thread_local std::string g_thread_err;   // errors without a context (creation)
+
 int set_err(kspir_ctx* c, int code, const std::string& msg) {
     if (c) c->err = msg;
+    g_thread_err = msg;
     return code;
 }
 
@@ -226,21 +235,23 @@ int init_constants(kspir_ctx* c) {
     // per prime; bsMod uses HEXL's minimal primitive root
     const uint64_t root_crt = 3375402822066082ull;
     const uint64_t roots[3] = {root_crt % kQ1, root_crt % kQ2, h_min_root(kBsMod)};
+    // per channel uint2 [2][N]: {psi^brv(k), Shoup} then {psi^-brv(k), Shoup}
     std::vector<uint32_t> tw(3 * 4 * kN);
     for (int ch = 0; ch < 3; ch++) {
         const uint64_t q = qs[ch], psi = roots[ch], pinv = h_invmod(psi, q);
         uint32_t* t = tw.data() + (size_t)ch * 4 * kN;
         for (int k = 0; k < kN; k++) {
             uint32_t e = h_bitrev12(k);
-            t[k] = (uint32_t)h_powmod(psi, e, q);
-            t[kN + k] = shoup32(t[k], (uint32_t)q);
-            t[2 * kN + k] = (uint32_t)h_powmod(pinv, e, q);
-            t[3 * kN + k] = shoup32(t[2 * kN + k], (uint32_t)q);
+            const uint32_t w = (uint32_t)h_powmod(psi, e, q), iw = (uint32_t)h_powmod(pinv, e, q);
+            t[2 * k] = w;
+            t[2 * k + 1] = shoup32(w, (uint32_t)q);
+            t[2 * kN + 2 * k] = iw;
+            t[2 * kN + 2 * k + 1] = shoup32(iw, (uint32_t)q);
         }
     }
     KS_CUDA(c, cudaMalloc(&c->tw, tw.size() * 4));
     KS_COPY(c, c->tw, tw.data(), tw.size() * 4, cudaMemcpyHostToDevice);
-    for (int ch = 0; ch < 3; ch++) c->ntabs.tw[ch] = c->tw + (size_t)ch * 4 * kN;
+    for (int ch = 0; ch < 3; ch++) c->ntabs.tw[ch] = reinterpret_cast<const uint2*>(c->tw + (size_t)ch * 4 * kN);
 
     std::vector<uint16_t> sb((size_t)c->N1h * kN), sg((size_t)std::max(1, c->N2 - 1) * kN);
     for (int i = 0; i < c->N1h; i++) slot_permutation(pow5(i + 1), sb.data() + (size_t)i * kN);
@@ -379,19 +390,19 @@ inline int blocks_for(long n, int t) { return (int)((n + t - 1) / t); }
 void enqueue_baby(kspir_ctx* c, WsSlot& s, const ClientKeysDev& keys, cudaStream_t st) {
     Workspace& w = s.ws;
     k_query_prep<<<kN / 256, 256, 0, st>>>(w, c->gad.baby);
-    k_ntt_jobs<256, false><<<s.n_q, 256, 0, st>>>(s.jobs + s.seg_q, c->ntabs);
+    k_ntt_jobs<false><<<s.n_q, kNttThreads, kNttJobSmem, st>>>(s.jobs + s.seg_q, c->ntabs);
     BabyArgs a1{};
     a1.dig = w.dig0; a1.srcB = w.qbn; a1.srcBbs = w.qbbs; a1.perms = c->perms; a1.sigma = c->sigma_baby;
     a1.cipherbuf = w.cipherbuf; a1.interA = w.interA; a1.interB = w.interB; a1.inter_bs = w.inter_bs;
-    a1.N1 = c->N1; a1.col_base = 1; a1.inter_idx = c->N1h - 2; a1.ell = c->gad.baby.ell;
-    if (c->N1h - 1 > 0) k_baby_rot<512><<<c->N1h - 1, 512, 5 * kN * 4, st>>>(a1, keys, c->ntabs);
-    k_ntt_jobs<1024, true><<<2, 1024, 0, st>>>(s.jobs + s.seg_inter, c->ntabs);
+    a1.N1 = c->N1; a1.col_base = 1; a1.inter_idx = c->N1h - 2;
+    if (c->N1h - 1 > 0) k_baby_rot<3><<<(c->N1h - 1) * 4, kNttThreads, kBabySmem, st>>>(a1, keys, c->ntabs);
+    k_ntt_jobs<true><<<2, kNttThreads, kNttJobSmem, st>>>(s.jobs + s.seg_inter, c->ntabs);
     k_inter_decomp<<<kN / 256, 256, 0, st>>>(w, c->gad.baby);
-    k_ntt_jobs<512, false><<<9, 512, 0, st>>>(s.jobs + s.seg_dig1, c->ntabs);
+    k_ntt_jobs<false><<<9, kNttThreads, kNttJobSmem, st>>>(s.jobs + s.seg_dig1, c->ntabs);
     BabyArgs a2 = a1;
     a2.dig = w.dig1; a2.srcB = w.interB; a2.srcBbs = w.inter_bs + kN;
     a2.col_base = c->N1h; a2.inter_idx = -1;
-    k_baby_rot<512><<<c->N1h, 512, 5 * kN * 4, st>>>(a2, keys, c->ntabs);
+    k_baby_rot<3><<<c->N1h * 4, kNttThreads, kBabySmem, st>>>(a2, keys, c->ntabs);
 }
 
 void enqueue_scan(kspir_ctx* c, WsSlot& s, cudaStream_t st) {
@@ -399,8 +410,8 @@ void enqueue_scan(kspir_ctx* c, WsSlot& s, cudaStream_t st) {
     const int R = c->p.r;
     switch (c->N1) {
 #define KS_SCAN(n) \
-    case n: k_scan<n><<<c->nsm, kScanThreads, ScanCfg<n>::SMEM, st>>>(c->db, w.cipherbuf, w.sout, R, w.err); break;
-        KS_SCAN(32) KS_SCAN(64) KS_SCAN(128) KS_SCAN(256) KS_SCAN(512)
+    case n: k_scan<n><<<c->nsm, ScanCfg<n>::THREADS, ScanCfg<n>::SMEM, st>>>(c->db, w.cipherbuf, w.sout, R, w.err); break;
+        KS_SCAN(64) KS_SCAN(128) KS_SCAN(256) KS_SCAN(512)
 #undef KS_SCAN
     }
 }
@@ -409,10 +420,10 @@ void enqueue_giant(kspir_ctx* c, WsSlot& s, const ClientKeysDev& keys, cudaStrea
     Workspace& w = s.ws;
     const int R = c->p.r;
     if (c->N2 > 1) {
-        k_ntt_jobs<256, true><<<s.n_ginv, 256, 0, st>>>(s.jobs + s.seg_ginv, c->ntabs);
+        k_ntt_jobs<true><<<s.n_ginv, kNttThreads, kNttJobSmem, st>>>(s.jobs + s.seg_ginv, c->ntabs);
         k_giant_decomp<<<blocks_for((long)R * (c->N2 - 1) * kN, 256), 256, 0, st>>>(w.gcoef, w.gdig, R, c->N1,
                                                                                     c->gad.giant);
-        k_ntt_jobs<256, false><<<s.n_gfwd, 256, 0, st>>>(s.jobs + s.seg_gfwd, c->ntabs);
+        k_ntt_jobs<false><<<s.n_gfwd, kNttThreads, kNttJobSmem, st>>>(s.jobs + s.seg_gfwd, c->ntabs);
     }
     k_giant_accum<<<blocks_for((long)R * 2 * kN, 256), 256, 0, st>>>(w.sout, w.gdig, keys.giant, c->sigma_giant,
                                                                       w.result, R, c->N1, c->gad.giant.ell);
@@ -423,10 +434,12 @@ void enqueue_giant(kspir_ctx* c, WsSlot& s, const ClientKeysDev& keys, cudaStrea
 void enqueue_ext(kspir_ctx* c, WsSlot& s, const ClientKeysDev& keys, int count, const uint32_t* init,
                  cudaStream_t st) {
     Workspace& w = s.ws;
-    k_ntt_jobs<256, true><<<count * 4, 256, 0, st>>>(s.jobs + s.seg_einv, c->ntabs);
+    k_ntt_jobs<true><<<count * 4, kNttThreads, kNttJobSmem, st>>>(s.jobs + s.seg_einv, c->ntabs);
     k_ext_decomp<<<blocks_for((long)count * kN, 256), 256, 0, st>>>(w.ecoef, w.edig, count, c->gad.ext);
-    k_ntt_jobs<256, false><<<count * 2 * c->gad.ext.ell * 2, 256, 0, st>>>(s.jobs + s.seg_efwd, c->ntabs);
-    k_ext_mac_intt<512><<<count * 4, 512, 0, st>>>(w.edig, keys.rgsw, init, w.ext, 2 * c->gad.ext.ell, c->ntabs);
+    k_ntt_jobs<false><<<count * 2 * c->gad.ext.ell * 2, kNttThreads, kNttJobSmem, st>>>(s.jobs + s.seg_efwd,
+                                                                                      c->ntabs);
+    k_ext_mac_intt<<<count * 4, kNttThreads, kMacSmem, st>>>(w.edig, keys.rgsw, init, w.ext, 2 * c->gad.ext.ell,
+                                                             c->ntabs);
 }
 
 void enqueue_packing(kspir_ctx* c, WsSlot& s, const ClientKeysDev& keys, cudaStream_t st) {
@@ -436,9 +449,10 @@ void enqueue_packing(kspir_ctx* c, WsSlot& s, const ClientKeysDev& keys, cudaStr
         const int I = 1 << lv;
         const uint32_t ginv = inv_mod_2n((uint32_t)(kN / I + 1));
         k_pack_prep<<<blocks_for((long)I * kN, 256), 256, 0, st>>>(w.ext, w.pdig, w.ptb, w.pc2, I, ginv, c->gad.pack);
-        k_ntt_jobs<256, false><<<I * (pe * 2 + 2), 256, 0, st>>>(s.jobs + s.seg_pfwd[lv], c->ntabs);
-        k_pack_mac_intt<512><<<I * 4, 512, 0, st>>>(w.pdig, w.ptb, w.pc2, keys.packing + (size_t)lv * pe * 4 * kN,
-                                                    w.ext, pe, c->ntabs);
+        k_ntt_jobs<false><<<I * (pe * 2 + 2), kNttThreads, kNttJobSmem, st>>>(s.jobs + s.seg_pfwd[lv], c->ntabs);
+        k_pack_mac_intt<<<I * 4, kNttThreads, kMacSmem, st>>>(w.pdig, w.ptb, w.pc2,
+                                                              keys.packing + (size_t)lv * pe * 4 * kN, w.ext, pe,
+                                                              c->ntabs);
     }
     k_compose_words<<<2 * kN / 256, 256, 0, st>>>(w.ext, w.resp64, 2);
 }
@@ -450,23 +464,69 @@ long answer_launches(const kspir_ctx* c) {
     return n;
 }
 
-void enqueue_answer(kspir_ctx* c, WsSlot& s, const ClientKeysDev& keys, cudaStream_t st) {
+// Captures the four non-scan phases of one (workspace, client) pair as CUDA
+// graphs (the scan stays a direct launch so its duration is bracketed by the
+// per-answer events).  Pointers are fixed for the context's lifetime, so the
+// graphs stay valid when keys or the database are re-uploaded.
+int build_graphs(kspir_ctx* c, int wsi, int client) {
+    auto& pg = c->graphs[(size_t)wsi * c->p.max_clients + client];
+    if (pg.ready) return KSPIR_OK;
+    WsSlot& s = c->ws[wsi];
+    const ClientKeysDev keys = c->clients[client].keys;
+    cudaStream_t cs = c->capture;
+    for (int ph = 0; ph < 4; ph++) {
+        cudaGraph_t g = nullptr;
+        KS_CUDA(c, cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+        if (ph == 0) enqueue_baby(c, s, keys, cs);
+        else if (ph == 1) enqueue_giant(c, s, keys, cs);
+        else if (ph == 2) enqueue_ext(c, s, keys, c->p.r, nullptr, cs);
+        else enqueue_packing(c, s, keys, cs);
+        KS_CUDA(c, cudaStreamEndCapture(cs, &g));
+        cudaError_t e = cudaGraphInstantiate(&pg.g[ph], g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return set_err(c, KSPIR_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+    }
+    pg.ready = true;
+    return KSPIR_OK;
+}
+
+int enqueue_answer(kspir_ctx* c, int wsi, int client, cudaStream_t st) {
+    WsSlot& s = c->ws[wsi];
+    const ClientKeysDev& keys = c->clients[client].keys;
     const int slot = (int)(c->answers % kTimingRing);
     auto& ev = c->ring[slot];
-    cudaEventRecord(ev[0], st);
-    enqueue_baby(c, s, keys, st);
-    cudaEventRecord(ev[1], st);
-    enqueue_scan(c, s, st);
-    cudaEventRecord(ev[2], st);
-    enqueue_giant(c, s, keys, st);
-    cudaEventRecord(ev[3], st);
-    enqueue_ext(c, s, keys, c->p.r, nullptr, st);
-    cudaEventRecord(ev[4], st);
-    enqueue_packing(c, s, keys, st);
-    cudaEventRecord(ev[5], st);
+    if (c->use_graphs) {
+        int rc = build_graphs(c, wsi, client);
+        if (rc) return rc;
+        auto& pg = c->graphs[(size_t)wsi * c->p.max_clients + client];
+        cudaEventRecord(ev[0], st);
+        KS_CUDA(c, cudaGraphLaunch(pg.g[0], st));
+        cudaEventRecord(ev[1], st);
+        enqueue_scan(c, s, st);
+        cudaEventRecord(ev[2], st);
+        KS_CUDA(c, cudaGraphLaunch(pg.g[1], st));
+        cudaEventRecord(ev[3], st);
+        KS_CUDA(c, cudaGraphLaunch(pg.g[2], st));
+        cudaEventRecord(ev[4], st);
+        KS_CUDA(c, cudaGraphLaunch(pg.g[3], st));
+        cudaEventRecord(ev[5], st);
+    } else {
+        cudaEventRecord(ev[0], st);
+        enqueue_baby(c, s, keys, st);
+        cudaEventRecord(ev[1], st);
+        enqueue_scan(c, s, st);
+        cudaEventRecord(ev[2], st);
+        enqueue_giant(c, s, keys, st);
+        cudaEventRecord(ev[3], st);
+        enqueue_ext(c, s, keys, c->p.r, nullptr, st);
+        cudaEventRecord(ev[4], st);
+        enqueue_packing(c, s, keys, st);
+        cudaEventRecord(ev[5], st);
+    }
     c->answers++;
     c->launches += answer_launches(c);
     c->last_slot = slot;
+    return KSPIR_OK;
 }
 
 bool canonical(const uint64_t* w, size_t n, uint64_t q) {
@@ -516,13 +576,13 @@ const char* kspir_strerror(int code) {
     }
 }
 
-const char* kspir_last_error(const kspir_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+const char* kspir_last_error(const kspir_ctx* ctx) { return ctx ? ctx->err.c_str() : g_thread_err.c_str(); }
 
 int kspir_ctx_create(int device, const kspir_params* params, kspir_ctx** out) {
     if (!params || !out) return KSPIR_ERR_INVALID_ARG;
     const kspir_params p = *params;
     auto pow2 = [](int v) { return v > 0 && (v & (v - 1)) == 0; };
-    if (!pow2(p.r) || p.r > 512 || !pow2(p.N1) || p.N1 < 32 || p.N1 > 512 || p.max_clients < 1 ||
+    if (!pow2(p.r) || p.r > 512 || !pow2(p.N1) || p.N1 < 64 || p.N1 > 512 || p.max_clients < 1 ||
         p.max_inflight < 1)
         return KSPIR_ERR_INVALID_ARG;
     std::unique_ptr<kspir_ctx> c(new kspir_ctx());
@@ -534,11 +594,12 @@ int kspir_ctx_create(int device, const kspir_params* params, kspir_ctx** out) {
     c->levels = ilog2i(p.r);
     KS_CUDA(c.get(), cudaSetDevice(device));
     KS_CUDA(c.get(), cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    KS_CUDA(c.get(), cudaStreamCreateWithFlags(&c->capture, cudaStreamNonBlocking));
+    if (const char* e = getenv("KSPIR_NO_GRAPHS")) c->use_graphs = !(e[0] == '1');
     KS_CUDA(c.get(), cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device));
-    KS_CUDA(c.get(), cudaFuncSetAttribute(k_baby_rot<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, 5 * kN * 4));
 #define KS_ATTR(n) \
     KS_CUDA(c.get(), cudaFuncSetAttribute(k_scan<n>, cudaFuncAttributeMaxDynamicSharedMemorySize, ScanCfg<n>::SMEM));
-    KS_ATTR(32) KS_ATTR(64) KS_ATTR(128) KS_ATTR(256) KS_ATTR(512)
+    KS_ATTR(64) KS_ATTR(128) KS_ATTR(256) KS_ATTR(512)
 #undef KS_ATTR
     int rc = init_constants(c.get());
     if (rc) return rc;
@@ -548,6 +609,7 @@ int kspir_ctx_create(int device, const kspir_params* params, kspir_ctx** out) {
         for (auto& e : evs) KS_CUDA(c.get(), cudaEventCreate(&e));
     c->clients.resize(p.max_clients);
     c->ws.resize(p.max_inflight);
+    c->graphs.resize((size_t)p.max_inflight * p.max_clients);
     for (auto& s : c->ws) {
         rc = init_workspace(c.get(), s);
         if (rc) return rc;
@@ -566,6 +628,9 @@ int kspir_ctx_destroy(kspir_ctx* c) {
     }
     for (auto& evs : c->ring)
         for (auto& e : evs) if (e) cudaEventDestroy(e);
+    for (auto& pg : c->graphs)
+        for (auto& g : pg.g) if (g) cudaGraphExecDestroy(g);
+    if (c->capture) cudaStreamDestroy(c->capture);
     for (auto& cl : c->clients) cudaFree(cl.mem);
     cudaFree(c->db);
     cudaFree(c->perms);
@@ -671,7 +736,8 @@ int kspir_answer_device(kspir_ctx* c, int client, const uint64_t* d_query, uint6
     WsSlot& s = c->ws[0];
     KS_CUDA(c, cudaSetDevice(c->device));
     KS_CUDA(c, cudaMemcpyAsync(s.ws.q64, d_query, 4 * kN * 8, cudaMemcpyDeviceToDevice, st));
-    enqueue_answer(c, s, c->clients[client].keys, st);
+    rc = enqueue_answer(c, 0, client, st);
+    if (rc) return rc;
     KS_CUDA(c, cudaMemcpyAsync(d_response, s.ws.resp64, 2 * kN * 8, cudaMemcpyDeviceToDevice, st));
     KS_CUDA(c, cudaGetLastError());
     return KSPIR_OK;
@@ -692,7 +758,8 @@ int kspir_answer(kspir_ctx* c, int client, const uint64_t* query, uint64_t* resp
     WsSlot& s = c->ws[0];
     KS_CUDA(c, cudaSetDevice(c->device));
     KS_CUDA(c, cudaMemcpyAsync(s.ws.q64, query, 4 * kN * 8, cudaMemcpyHostToDevice, c->stream));
-    enqueue_answer(c, s, c->clients[client].keys, c->stream);
+    rc = enqueue_answer(c, 0, client, c->stream);
+    if (rc) return rc;
     KS_CUDA(c, cudaGetLastError());
     KS_CUDA(c, cudaMemcpyAsync(response, s.ws.resp64, 2 * kN * 8, cudaMemcpyDeviceToHost, c->stream));
     return finish(c, s);
@@ -924,11 +991,11 @@ __global__ void k_na_twiddles(uint32_t* tw, uint32_t q0, uint32_t q1, uint32_t q
         };
         uint32_t w = pw(e);
         uint32_t iw = pw((2 * kN - e) % (2 * kN));   // psi^(2N) = 1
-        uint32_t* t = tw + (size_t)ch * 4 * kN;
-        t[k] = w;
-        t[kN + k] = (uint32_t)(((uint64_t)w << 32) / q);
-        t[2 * kN + k] = iw;
-        t[3 * kN + k] = (uint32_t)(((uint64_t)iw << 32) / q);
+        uint32_t* t = tw + (size_t)ch * 4 * kN;   // uint2 [2][N]
+        t[2 * k] = w;
+        t[2 * k + 1] = (uint32_t)(((uint64_t)w << 32) / q);
+        t[2 * kN + 2 * k] = iw;
+        t[2 * kN + 2 * k + 1] = (uint32_t)(((uint64_t)iw << 32) / q);
     }
 }
 
@@ -1021,7 +1088,7 @@ extern "C" int kspir_external_product_noalloc(int device, const uint64_t* d_rgsw
         const NaDevice& d = g_na[device];
         NaLayout L = na_layout(d.scratch);
         NttTables tabs;
-        for (int ch = 0; ch < 3; ch++) tabs.tw[ch] = d.tw + (size_t)ch * 4 * kN;
+        for (int ch = 0; ch < 3; ch++) tabs.tw[ch] = reinterpret_cast<const uint2*>(d.tw + (size_t)ch * 4 * kN);
         GadgetS g;
         g.ell = 2; g.base_bits = 20; g.gbits = 18;   // RGSW of test-pir.cpp:71
         const size_t n = (size_t)count * 2 * kN;
@@ -1032,10 +1099,10 @@ extern "C" int kspir_external_product_noalloc(int device, const uint64_t* d_rgsw
         k_split_words<<<blocks_for((long)n, 256), 256, 0, st>>>(d_first_dim, L.fd_res, count * 2);
         k_split_words<<<blocks_for((long)n, 256), 256, 0, st>>>(d_result, L.acc_res, count * 2);
         k_split_words<<<blocks_for(8L * kN, 256), 256, 0, st>>>(d_rgsw, L.rgsw, 8);
-        k_ntt_jobs<256, true><<<count * 4, 256, 0, st>>>(L.jobs, tabs);
+        k_ntt_jobs<true><<<count * 4, kNttThreads, kNttJobSmem, st>>>(L.jobs, tabs);
         k_ext_decomp<<<blocks_for((long)count * kN, 256), 256, 0, st>>>(L.ecoef, L.edig, count, g);
-        k_ntt_jobs<256, false><<<count * 8, 256, 0, st>>>(L.jobs + kNoAllocMaxCount * 4, tabs);
-        k_ext_mac_intt<512><<<count * 4, 512, 0, st>>>(L.edig, L.rgsw, L.acc_res, L.ext, 4, tabs);
+        k_ntt_jobs<false><<<count * 8, kNttThreads, kNttJobSmem, st>>>(L.jobs + kNoAllocMaxCount * 4, tabs);
+        k_ext_mac_intt<<<count * 4, kNttThreads, kMacSmem, st>>>(L.edig, L.rgsw, L.acc_res, L.ext, 4, tabs);
         int flag = 0;
         if (cudaGetLastError() != cudaSuccess ||
             cudaMemcpyAsync(&flag, L.flag, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||

@@ -1,115 +1,142 @@
 // CTA-level negacyclic NTT of length 4096 on one residue channel, operating on
-// a shared-memory array.  Every kernel that needs a transform calls these so
-// the transform is fused with its producer and consumer.
+// a shared-memory array, so every kernel fuses its transforms with their
+// producers and consumers.
 //
 // Order and root follow HEXL as the reference uses it: the forward transform
 // maps natural order to bit-reversed order, slot j holding
 // sum_k x_k psi^((2 bitrev(j) + 1) k)  (reference utils.cpp:1473-1478), and the
 // inverse includes N^-1.  Outputs are canonical.
 //
-// Radix-4 passes (two butterfly layers per __syncthreads) of Harvey lazy
-// butterflies with Shoup twiddles.  Twiddle tables (per channel, in global
-// memory, read through the read-only path):
-//   tw[0*N + k] = psi^brv(k)      tw[1*N + k] = Shoup companion
-//   tw[2*N + k] = psi^-brv(k)     tw[3*N + k] = Shoup companion
+// 512 threads, one radix-8 unit (8 elements, three butterfly layers) per
+// thread per pass: four passes and four __syncthreads per transform.  Harvey
+// lazy butterflies on 32-bit words (q < 2^28, values < 4q < 2^30) with Shoup
+// twiddles.  The twiddles of one direction of one channel are staged into
+// shared memory first (stage_twiddles) as uint2 {w, floor(w 2^32 / q)}.
+//
+// Device table layout per channel: uint2 tw[2][N]; tw[0][k] = psi^brv(k),
+// tw[1][k] = psi^-brv(k), each with its Shoup companion.
 #pragma once
 
 #include "common.cuh"
 
 namespace kspir {
 
+constexpr int kNttThreads = 512;
+
 struct NttTables {
-    const uint32_t* tw[CH_COUNT];   // 4*N words per channel
+    const uint2* tw[CH_COUNT];   // [2][N] per channel
 };
 
-// Forward transform of s[0..N) in place.  Input in [0, 4q) (canonical inputs
-// are fine), output canonical.  T = blockDim.x (a multiple of 32, <= 1024).
-template <int T>
-__device__ __forceinline__ void cta_ntt_forward(uint32_t* s, const uint32_t* __restrict__ tw, int ch) {
-    const uint32_t q = c_dev.ch[ch].q, q2 = c_dev.ch[ch].two_q;
-    const uint32_t* __restrict__ w = tw;
-    const uint32_t* __restrict__ wp = tw + kN;
-    __syncthreads();
-#pragma unroll 1
-    for (int m = 1; m < kN; m <<= 2) {
-        const int h = kN / (2 * m);         // half-size of layer m
-        const int hh = h >> 1;               // half-size of layer 2m
-        const int lg_hh = __ffs(hh) - 1;
+enum NttDir : int { NTT_FWD = 0, NTT_INV = 1 };
+
+// Copies the twiddles of (channel, direction) into shared memory.  The caller
+// synchronises (the transforms start with __syncthreads).
+__device__ __forceinline__ void stage_twiddles(uint2* tws, const NttTables& tabs, int ch, int dir) {
+    const uint4* g = reinterpret_cast<const uint4*>(tabs.tw[ch] + (size_t)dir * kN);
+    uint4* s = reinterpret_cast<uint4*>(tws);
 #pragma unroll
-        for (int u = threadIdx.x; u < kN / 4; u += T) {
-            const int i = u >> lg_hh, j = u & (hh - 1);
-            const int e0 = 2 * i * h + j;
-            const uint32_t W1 = __ldg(w + m + i), W1p = __ldg(wp + m + i);
-            const uint32_t W2 = __ldg(w + 2 * m + 2 * i), W2p = __ldg(wp + 2 * m + 2 * i);
-            const uint32_t W3 = __ldg(w + 2 * m + 2 * i + 1), W3p = __ldg(wp + 2 * m + 2 * i + 1);
-            uint32_t x0 = s[e0], x1 = s[e0 + hh], x2 = s[e0 + h], x3 = s[e0 + h + hh];
-            // layer m: (x0, x2), (x1, x3) with W1
-            if (x0 >= q2) x0 -= q2;
-            if (x1 >= q2) x1 -= q2;
-            uint32_t t2 = shoup_lazy(x2, W1, W1p, q);
-            uint32_t t3 = shoup_lazy(x3, W1, W1p, q);
-            uint32_t y0 = x0 + t2, y2 = x0 - t2 + q2;
-            uint32_t y1 = x1 + t3, y3 = x1 - t3 + q2;
-            // layer 2m: (y0, y1) with W2, (y2, y3) with W3
-            if (y0 >= q2) y0 -= q2;
-            if (y2 >= q2) y2 -= q2;
-            uint32_t t1 = shoup_lazy(y1, W2, W2p, q);
-            uint32_t t3b = shoup_lazy(y3, W3, W3p, q);
-            s[e0] = y0 + t1;
-            s[e0 + hh] = y0 - t1 + q2;
-            s[e0 + h] = y2 + t3b;
-            s[e0 + h + hh] = y2 - t3b + q2;
-        }
-        __syncthreads();
-    }
-#pragma unroll
-    for (int k = threadIdx.x; k < kN; k += T) {
-        uint32_t x = s[k];
-        if (x >= q2) x -= q2;
-        if (x >= q) x -= q;
-        s[k] = x;
-    }
-    __syncthreads();
+    for (int k = threadIdx.x; k < kN / 2; k += kNttThreads) s[k] = __ldg(g + k);
 }
 
-// Inverse transform of s[0..N) in place (includes N^-1).  Input in [0, 2q)
-// (canonical inputs are fine), output canonical.
-template <int T>
-__device__ __forceinline__ void cta_ntt_inverse(uint32_t* s, const uint32_t* __restrict__ tw, int ch) {
+__device__ __forceinline__ void fwd_bfly(uint32_t& X, uint32_t& Y, uint2 w, uint32_t q, uint32_t q2) {
+    uint32_t x = X >= q2 ? X - q2 : X;
+    uint32_t t = shoup_lazy(Y, w.x, w.y, q);
+    X = x + t;
+    Y = x - t + q2;
+}
+
+__device__ __forceinline__ void inv_bfly(uint32_t& X, uint32_t& Y, uint2 w, uint32_t q, uint32_t q2) {
+    uint32_t s = X + Y;
+    s = s >= q2 ? s - q2 : s;
+    uint32_t d = shoup_lazy(X - Y + q2, w.x, w.y, q);
+    X = s;
+    Y = d;
+}
+
+// Forward transform of s[0..N) in place; input in [0, 4q) (canonical inputs are
+// fine), output canonical.  tws holds the forward twiddles of `ch`.
+__device__ __forceinline__ void cta_ntt_forward(uint32_t* s, const uint2* tws, int ch) {
     const uint32_t q = c_dev.ch[ch].q, q2 = c_dev.ch[ch].two_q;
-    const uint32_t* __restrict__ w = tw + 2 * kN;
-    const uint32_t* __restrict__ wp = tw + 3 * kN;
+    const int u = threadIdx.x;
     __syncthreads();
-#pragma unroll 1
-    for (int m = kN / 2; m >= 2; m >>= 2) {
-        const int h = kN / (2 * m);          // half-size of layer m; layer m/2 has 2h
-        const int lg_h = __ffs(h) - 1;
 #pragma unroll
-        for (int u = threadIdx.x; u < kN / 4; u += T) {
-            const int i = u >> lg_h, j = u & (h - 1);
-            const int e0 = 4 * i * h + j;
-            const uint32_t Wa = __ldg(w + m + 2 * i), Wap = __ldg(wp + m + 2 * i);
-            const uint32_t Wb = __ldg(w + m + 2 * i + 1), Wbp = __ldg(wp + m + 2 * i + 1);
-            const uint32_t Wc = __ldg(w + m / 2 + i), Wcp = __ldg(wp + m / 2 + i);
-            uint32_t x0 = s[e0], x1 = s[e0 + h], x2 = s[e0 + 2 * h], x3 = s[e0 + 3 * h];
-            // layer m: (x0, x1) with Wa, (x2, x3) with Wb
-            uint32_t y0 = x0 + x1; if (y0 >= q2) y0 -= q2;
-            uint32_t y1 = shoup_lazy(x0 - x1 + q2, Wa, Wap, q);
-            uint32_t y2 = x2 + x3; if (y2 >= q2) y2 -= q2;
-            uint32_t y3 = shoup_lazy(x2 - x3 + q2, Wb, Wbp, q);
-            // layer m/2: (y0, y2), (y1, y3) with Wc
-            uint32_t z0 = y0 + y2; if (z0 >= q2) z0 -= q2;
-            uint32_t z2 = shoup_lazy(y0 - y2 + q2, Wc, Wcp, q);
-            uint32_t z1 = y1 + y3; if (z1 >= q2) z1 -= q2;
-            uint32_t z3 = shoup_lazy(y1 - y3 + q2, Wc, Wcp, q);
-            s[e0] = z0; s[e0 + h] = z1; s[e0 + 2 * h] = z2; s[e0 + 3 * h] = z3;
+    for (int p = 0; p < 4; p++) {
+        const int lq = 9 - 3 * p;             // log2 of the element stride within a unit
+        const int q8 = 1 << lq;
+        const int m0 = 1 << (3 * p);
+        const int i0 = u >> lq, j = u & (q8 - 1);
+        const int base = i0 * 8 * q8 + j;
+        uint32_t x[8];
+#pragma unroll
+        for (int t = 0; t < 8; t++) x[t] = s[base + t * q8];
+        const uint2 wa = tws[m0 + i0];
+        const uint2 wb0 = tws[2 * m0 + 2 * i0], wb1 = tws[2 * m0 + 2 * i0 + 1];
+        const uint2 wc0 = tws[4 * m0 + 4 * i0], wc1 = tws[4 * m0 + 4 * i0 + 1];
+        const uint2 wc2 = tws[4 * m0 + 4 * i0 + 2], wc3 = tws[4 * m0 + 4 * i0 + 3];
+#pragma unroll
+        for (int t = 0; t < 4; t++) fwd_bfly(x[t], x[t + 4], wa, q, q2);
+        fwd_bfly(x[0], x[2], wb0, q, q2);
+        fwd_bfly(x[1], x[3], wb0, q, q2);
+        fwd_bfly(x[4], x[6], wb1, q, q2);
+        fwd_bfly(x[5], x[7], wb1, q, q2);
+        fwd_bfly(x[0], x[1], wc0, q, q2);
+        fwd_bfly(x[2], x[3], wc1, q, q2);
+        fwd_bfly(x[4], x[5], wc2, q, q2);
+        fwd_bfly(x[6], x[7], wc3, q, q2);
+        if (p == 3) {
+#pragma unroll
+            for (int t = 0; t < 8; t++) {
+                uint32_t v = x[t] >= q2 ? x[t] - q2 : x[t];
+                x[t] = v >= q ? v - q : v;
+            }
         }
+        // the units of one pass are disjoint: write back without a barrier
+#pragma unroll
+        for (int t = 0; t < 8; t++) s[base + t * q8] = x[t];
         __syncthreads();
     }
+}
+
+// Inverse transform of s[0..N) in place (includes N^-1); input in [0, 2q)
+// (canonical inputs are fine), output canonical.  tws holds the inverse
+// twiddles of `ch`.
+__device__ __forceinline__ void cta_ntt_inverse(uint32_t* s, const uint2* tws, int ch) {
+    const uint32_t q = c_dev.ch[ch].q, q2 = c_dev.ch[ch].two_q;
     const uint32_t ni = c_dev.ch[ch].ninv, nip = c_dev.ch[ch].ninv_p;
-#pragma unroll
-    for (int k = threadIdx.x; k < kN; k += T) s[k] = shoup_mul(s[k], ni, nip, q);
+    const int u = threadIdx.x;
     __syncthreads();
+#pragma unroll
+    for (int p = 3; p >= 0; p--) {
+        const int lq = 9 - 3 * p;
+        const int q8 = 1 << lq;
+        const int m0 = 1 << (3 * p);
+        const int i0 = u >> lq, j = u & (q8 - 1);
+        const int base = i0 * 8 * q8 + j;
+        uint32_t x[8];
+#pragma unroll
+        for (int t = 0; t < 8; t++) x[t] = s[base + t * q8];
+        const uint2 wa = tws[m0 + i0];
+        const uint2 wb0 = tws[2 * m0 + 2 * i0], wb1 = tws[2 * m0 + 2 * i0 + 1];
+        const uint2 wc0 = tws[4 * m0 + 4 * i0], wc1 = tws[4 * m0 + 4 * i0 + 1];
+        const uint2 wc2 = tws[4 * m0 + 4 * i0 + 2], wc3 = tws[4 * m0 + 4 * i0 + 3];
+        inv_bfly(x[0], x[1], wc0, q, q2);
+        inv_bfly(x[2], x[3], wc1, q, q2);
+        inv_bfly(x[4], x[5], wc2, q, q2);
+        inv_bfly(x[6], x[7], wc3, q, q2);
+        inv_bfly(x[0], x[2], wb0, q, q2);
+        inv_bfly(x[1], x[3], wb0, q, q2);
+        inv_bfly(x[4], x[6], wb1, q, q2);
+        inv_bfly(x[5], x[7], wb1, q, q2);
+#pragma unroll
+        for (int t = 0; t < 4; t++) inv_bfly(x[t], x[t + 4], wa, q, q2);
+        if (p == 0) {
+#pragma unroll
+            for (int t = 0; t < 8; t++) x[t] = shoup_mul(x[t], ni, nip, q);
+        }
+#pragma unroll
+        for (int t = 0; t < 8; t++) s[base + t * q8] = x[t];
+        __syncthreads();
+    }
 }
 
 }  // namespace kspir

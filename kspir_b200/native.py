@@ -118,7 +118,8 @@ class Context:
         p = Params(r, N1, max_clients, max_inflight)
         rc = self.lib.kspir_ctx_create(device, ctypes.byref(p), ctypes.byref(self._h))
         if rc:
-            raise KspirError(rc, self.lib.kspir_strerror(rc).decode())
+            detail = self.lib.kspir_last_error(None).decode()
+            raise KspirError(rc, detail or self.lib.kspir_strerror(rc).decode())
 
     # -- plumbing ---------------------------------------------------------
     def _check(self, rc: int):

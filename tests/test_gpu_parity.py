@@ -166,3 +166,24 @@ def test_reference_named_mirror():
     out = np.zeros((2, N), dtype=np.uint64)
     kb.packingRLWEs(out, ext, kb.AutoKey(c["packing"]), N1=N1)
     assert (out.reshape(-1) == want_resp).all()
+
+
+def test_back_to_back_device_answers():
+    # many answers queued without host synchronisation exercise the scan's
+    # producer/consumer ring across every stage phase; all must be identical
+    torch = pytest.importorskip("torch")
+    r, N1, seed, n = 16, 128, 81, 48
+    db = po.gen_db(seed, r, N1)
+    c = po.gen_client(seed, r, N1)
+    want = po.answer(db, r, N1, c)
+    with make_ctx(r, N1, db, c) as ctx:
+        dq = torch.from_numpy(c["query"].view(np.int64).copy()).cuda()
+        out = torch.zeros((n, 2 * N), dtype=torch.int64, device="cuda")
+        stream = torch.cuda.Stream()
+        torch.cuda.synchronize()
+        for i in range(n):
+            ctx.answer_device(0, dq.data_ptr(), out[i].data_ptr(), stream.cuda_stream)
+        ctx.sync()
+        got = out.cpu().numpy().view(np.uint64)
+    for i in range(n):
+        assert np.array_equal(got[i], want), f"answer {i} differs"
