@@ -52,7 +52,7 @@ typedef struct kspir_ctx kspir_ctx;
 
 typedef struct kspir_params {
     int32_t r;            /* packing number = number of sub-databases, power of two, 1..512 */
-    int32_t N1;           /* baby steps, power of two, 64..512; N2 = N/2/N1 */
+    int32_t N1;           /* baby steps: 64, 128 or 256; N2 = N/2/N1 */
     int32_t max_clients;  /* client key slots held on the device */
     int32_t max_inflight; /* concurrent query workspaces (1 for the plain path) */
 } kspir_params;

@@ -142,4 +142,9 @@ __device__ __forceinline__ int auto_src(int k, uint32_t ginv, bool* neg) {
 
 __device__ __forceinline__ uint32_t negmod(uint32_t x, uint32_t q) { return x ? q - x : 0; }
 
+// acc += a * b with a 32x32->64-bit product, as one fused wide multiply-add
+__device__ __forceinline__ void mad_wide(uint64_t& acc, uint32_t a, uint32_t b) {
+    asm("mad.wide.u32 %0, %1, %2, %0;" : "+l"(acc) : "r"(a), "r"(b));
+}
+
 }  // namespace kspir

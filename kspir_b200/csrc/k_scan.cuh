@@ -20,8 +20,10 @@
 // {r, r+4, ...} and 16-byte chunks {c, c+8, ...}.  Eight lanes of a row read
 // 128 contiguous bytes of it (no bank conflicts), the four lanes that share a
 // chunk read the same cipherbuf bytes (broadcast), and each cipherbuf chunk is
-// loaded once per lane and reused across its rows.  Partial sums are reduced
-// across the eight lanes of a row with shuffles.
+// loaded once per lane and reused across its rows.  The 4*RPL partial sums of
+// a lane are reduced across the eight lanes of its row by a transpose-reduce
+// (each shuffle level hands over half of the values), which leaves every lane
+// holding 4*RPL/8 finished outputs.
 #pragma once
 
 #include "common.cuh"
@@ -51,7 +53,9 @@ struct ScanCfg {
     static constexpr int SMEM = NST * STAGE + 2 * NST * 8;
     static_assert(NST % CONS == 0, "stages must be owned by one consumer warp each");
     static_assert(SMEM <= 227 * 1024, "shared memory budget");
-    static_assert(RPL >= 1 && CPL >= 1, "N1 must be in [64, 512]");
+    static constexpr int NV = 4 * RPL;                  // partial sums per lane
+    static constexpr int NOUT = NV / 8;                 // finished outputs per lane
+    static_assert(RPL >= 2 && CPL >= 1, "N1 must be in [64, 256]");
 };
 
 template <int N1>
@@ -118,9 +122,10 @@ __global__ void __launch_bounds__(ScanCfg<N1>::THREADS, 1)
         const uint8_t* st = smem + (size_t)s * C::STAGE;
         const uint4* D4 = reinterpret_cast<const uint4*>(st);             // [N2][CHUNKS] chunks of 2 words
         const uint4* Q4 = reinterpret_cast<const uint4*>(st + C::SLAB);   // [N1] (a_k, b_k) pairs
-        uint64_t acc[C::RPL][4];
+        // v[o], o = 4 * rr + comp_ch: 0 = a q1 (lo), 1 = a q2 (hi), 2 = b q1, 3 = b q2
+        uint64_t v[C::NV];
 #pragma unroll
-        for (int rr = 0; rr < C::RPL; rr++) acc[rr][0] = acc[rr][1] = acc[rr][2] = acc[rr][3] = 0;
+        for (int o = 0; o < C::NV; o++) v[o] = 0;
 #pragma unroll
         for (int cc = 0; cc < C::CPL; cc++) {
             const int kc = lc + 8 * cc;                   // chunk = words 2kc, 2kc+1
@@ -129,39 +134,42 @@ __global__ void __launch_bounds__(ScanCfg<N1>::THREADS, 1)
 #pragma unroll
             for (int rr = 0; rr < C::RPL; rr++) {
                 const uint4 w = D4[(lr + 4 * rr) * C::CHUNKS + kc];
-                acc[rr][0] += (uint64_t)w.x * qa.x;
-                acc[rr][0] += (uint64_t)w.z * qb.x;
-                acc[rr][1] += (uint64_t)w.y * qa.y;
-                acc[rr][1] += (uint64_t)w.w * qb.y;
-                acc[rr][2] += (uint64_t)w.x * qa.z;
-                acc[rr][2] += (uint64_t)w.z * qb.z;
-                acc[rr][3] += (uint64_t)w.y * qa.w;
-                acc[rr][3] += (uint64_t)w.w * qb.w;
+                mad_wide(v[4 * rr + 0], w.x, qa.x);
+                mad_wide(v[4 * rr + 0], w.z, qb.x);
+                mad_wide(v[4 * rr + 1], w.y, qa.y);
+                mad_wide(v[4 * rr + 1], w.w, qb.y);
+                mad_wide(v[4 * rr + 2], w.x, qa.z);
+                mad_wide(v[4 * rr + 2], w.z, qb.z);
+                mad_wide(v[4 * rr + 3], w.y, qa.w);
+                mad_wide(v[4 * rr + 3], w.w, qb.w);
             }
         }
         __syncwarp();
         if (lane == 0) mbar_arrive(&empty[s]);
+        // transpose-reduce over the chunk lanes (offsets 4, 2, 1): at each level
+        // the lane keeps the half of its values selected by its lane bit and
+        // adds the partner's copy of that half
 #pragma unroll
-        for (int rr = 0; rr < C::RPL; rr++)
+        for (int lvl = 0; lvl < 3; lvl++) {
+            const int d = 4 >> lvl;
+            const int hs = C::NV >> (lvl + 1);
+            const bool upper = (lc & d) != 0;
 #pragma unroll
-            for (int v = 0; v < 4; v++) {
-                uint64_t x = acc[rr][v];
-                x += __shfl_xor_sync(0xffffffffu, x, 1);
-                x += __shfl_xor_sync(0xffffffffu, x, 2);
-                x += __shfl_xor_sync(0xffffffffu, x, 4);
-                acc[rr][v] = x;
+            for (int i = 0; i < hs; i++) {
+                const uint64_t send = upper ? v[i] : v[i + hs];
+                const uint64_t keep = upper ? v[i + hs] : v[i];
+                v[i] = keep + __shfl_xor_sync(0xffffffffu, send, d);
             }
+        }
+        // lane lc now holds outputs o = NOUT * lc + t
         const long it = blockIdx.x + j * gridDim.x;
         const long r = it / kN, z = it % kN;
-        // RPL rows x 4 outputs per row lane, spread over its 8 chunk lanes
 #pragma unroll
-        for (int o = 0; o < C::RPL * 4; o++) {
-            if ((o & 7) != lc) continue;
-            const int rr = o >> 2, v = o & 3;
-            const int i = lr + 4 * rr;
-            const uint64_t x = acc[rr][v];
-            const uint32_t res = (v & 1) ? mod_q2(x) : mod_q1(x);   // v: 0 = a q1, 1 = a q2, 2 = b q1, 3 = b q2
-            sout[((size_t)(r * C::N2 + i) * 4 + v) * kN + z] = res;
+        for (int t = 0; t < C::NOUT; t++) {
+            const int o = C::NOUT * lc + t;
+            const int i = lr + 4 * (o >> 2), cv = o & 3;
+            const uint32_t res = (cv & 1) ? mod_q2(v[t]) : mod_q1(v[t]);
+            sout[((size_t)(r * C::N2 + i) * 4 + cv) * kN + z] = res;
         }
     }
 }

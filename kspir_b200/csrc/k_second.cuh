@@ -4,9 +4,10 @@
 //
 // All three are key switches of the same shape: bring `a` to coefficient form,
 // apply an automorphism, gadget-decompose, transform the digits, multiply by
-// the key and accumulate.  They run as element-wise kernels (decompose,
-// accumulate) around batched transforms (k_ntt_jobs) and a fused
-// multiply-accumulate + inverse-transform kernel.
+// the key and accumulate.  Each runs as one fused kernel whose intermediates
+// stay in shared memory (k_giant_fused, k_ext_fused, k_pack_fused).  The
+// unfused element-wise decomposition and multiply-accumulate kernels of the
+// external product remain for the allocation-free entry point.
 #pragma once
 
 #include "ntt.cuh"
@@ -16,72 +17,6 @@ namespace kspir {
 
 // ---------------------------------------------------------------------------
 // giant steps
-
-// For every (r, c >= 1) and coefficient k: the digits of
-// decompose(auto_g(INTT(output[c].a))), g = 5^(N1 c)  (twosteps.cpp:612-641).
-// The reference's inline automorphism leaves q for a negated zero
-// (twosteps.cpp:629); decompose maps q and 0 to the same digits (d = q + offset
-// > q is reduced back to offset), so the canonical negation is equivalent.
-__global__ void k_giant_decomp(const uint32_t* __restrict__ gcoef, uint32_t* __restrict__ gdig, int R,
-                               int N1, GadgetB g) {
-    const int N2 = kN / 2 / N1;
-    const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= (long)R * (N2 - 1) * kN) return;
-    const int k = (int)(idx % kN);
-    const long rc = idx / kN;               // r * (N2-1) + (c-1)
-    const int c = (int)(rc % (N2 - 1)) + 1;
-    const uint32_t e = (uint32_t)(N1 * c) & 2047u;
-    uint32_t gi = 1, b = 5, x = (2048u - e) & 2047u;   // g^-1 = 5^(2048 - N1 c) mod 2N
-    while (x) { if (x & 1) gi = (gi * b) & (2 * kN - 1); b = (b * b) & (2 * kN - 1); x >>= 1; }
-    bool neg;
-    const int src = auto_src(k, gi, &neg);
-    const uint32_t* a = gcoef + rc * 2 * kN;
-    uint64_t v = crt_compose_res(a[src], a[kN + src]);
-    if (neg && v) v = kCrtMod - v;
-    int32_t dig[kMaxEll];
-    decompose_b(v, kCrtMod, g, dig);
-    uint32_t* o = gdig + rc * g.ell * 2 * kN;
-    for (int j = 0; j < g.ell; j++) {
-        o[(j * 2 + 0) * kN + k] = signed_to_res(dig[j], kQ1);
-        o[(j * 2 + 1) * kN + k] = signed_to_res(dig[j], kQ2);
-    }
-}
-
-// result[r] = output[0] + sum_{c>=1} ( -sum_j d_j * key_c[j].a ,
-//                                       NTT(auto_g b_c) - sum_j d_j * key_c[j].b )
-// with NTT(auto_g b_c) = b_c[sigma_g] taken in the NTT domain (twosteps.cpp:642-672).
-__global__ void k_giant_accum(const uint32_t* __restrict__ sout, const uint32_t* __restrict__ gdig,
-                              const uint32_t* __restrict__ gkeys, const uint16_t* __restrict__ gsigma,
-                              uint32_t* __restrict__ result, int R, int N1, int ell) {
-    const int N2 = kN / 2 / N1;
-    const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= (long)R * 2 * kN) return;
-    const int k = (int)(idx % kN);
-    const int ch = (int)((idx / kN) % 2);
-    const long r = idx / (2 * kN);
-    const ChanConst cc = c_dev.ch[ch];
-    const uint32_t* so = sout + (size_t)r * N2 * 4 * kN;      // [N2][2 comp][2 ch][N]
-    uint32_t ra = so[(0 * 2 + ch) * kN + k];
-    uint32_t rb = so[(1 * 2 + ch) * kN + k];
-#pragma unroll 5
-    for (int c = 1; c < N2; c++) {
-        const uint32_t* d = gdig + ((size_t)r * (N2 - 1) + (c - 1)) * ell * 2 * kN;
-        const uint32_t* key = gkeys + (size_t)(c - 1) * ell * 2 * 2 * kN;
-        uint64_t sa = 0, sb = 0;
-        for (int j = 0; j < ell; j++) {
-            const uint64_t dj = d[(j * 2 + ch) * kN + k];
-            sa += dj * key[((j * 2 + 0) * 2 + ch) * kN + k];
-            sb += dj * key[((j * 2 + 1) * 2 + ch) * kN + k];
-        }
-        const uint32_t bc = so[((size_t)c * 4 + 1 * 2 + ch) * kN + gsigma[(size_t)(c - 1) * kN + k]];
-        ra = submod(ra, reduce64(sa, cc.q, cc.barrett), cc.q);
-        rb = addmod(rb, bc, cc.q);
-        rb = submod(rb, reduce64(sb, cc.q, cc.barrett), cc.q);
-    }
-    uint32_t* o = result + (size_t)r * 4 * kN;
-    o[(0 * 2 + ch) * kN + k] = ra;
-    o[(1 * 2 + ch) * kN + k] = rb;
-}
 
 // ---------------------------------------------------------------------------
 // external product
@@ -140,86 +75,297 @@ __global__ void __launch_bounds__(kNttThreads) k_ext_mac_intt(const uint32_t* __
     for (int k = threadIdx.x; k < kN; k += T) o[k] = s[k];
 }
 
-// ---------------------------------------------------------------------------
-// packing, one level of the tree (pairs j < I; rlwes[j] absorbs rlwes[I + j])
+}  // namespace kspir
 
-// convertTwoRLWEs (answer.cpp:720-739) up to the key switch of evalAuto:
-//   c' = X^I * c  (multConst, lwe.cpp:102-119),  r1 = r0 - c',  c2 = c' + r0,
-//   temp = auto_g(r1), g = N/I + 1, digits of decompose(temp.a) and temp.b.
-// multConst and evalAuto leave q for negated zeros; the HEXL add/sub that
-// consume c' and the decomposition treat q exactly like 0.
-__global__ void k_pack_prep(const uint32_t* __restrict__ ext, uint32_t* __restrict__ pdig,
-                            uint32_t* __restrict__ ptb, uint32_t* __restrict__ pc2, int I, uint32_t ginv,
-                            GadgetB g) {
-    const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= (long)I * kN) return;
-    const int k = (int)(idx % kN);
-    const int j = (int)(idx / kN);
-    const uint32_t* r0 = ext + (size_t)j * 4 * kN;
-    const uint32_t* cc = ext + (size_t)(I + j) * 4 * kN;
-    bool neg;   // ginv = (N/I + 1)^-1 mod 2N
-    const int src = auto_src(k, ginv, &neg);
-    // c' at position src: coefficient src - I of c, negated when it wraps
-    const int cs = src - I;
-    uint32_t r1v[2][2];
+namespace kspir {
+
+// ---------------------------------------------------------------------------
+// fused giant step: one CTA per (r, c >= 1) runs the whole key switch of
+// evalAutoRNSCRT for output[c] (twosteps.cpp:612-672) in shared memory:
+//   INTT(a) per prime -> compose -> X -> X^g -> decompose (ell digits)
+//   -> digit transforms -> -sum_j d_j * key[j]  and  b[sigma_g] - sum_j d_j * key[j]
+// and adds both into a 64-bit accumulator of sub-database r (atomics; the
+// canonical contributions of N2-1 giant steps cannot overflow it).
+
+constexpr int kGiantPolys = 4;   // two primes x two digits (ell = 2)
+constexpr int kPerThreadG = kN / kNttThreads;
+constexpr int kGiantSmem = kN * 8 + kGiantPolys * kN * 4;
+
+template <int ELL>
+__global__ void __launch_bounds__(kNttThreads) k_giant_fused(const uint32_t* __restrict__ sout,
+                                                             const uint32_t* __restrict__ gkeys,
+                                                             const uint16_t* __restrict__ gsigma,
+                                                             unsigned long long* __restrict__ acc, int N1,
+                                                             NttTables tabs, GadgetB g) {
+    static_assert(2 * ELL <= kGiantPolys, "shared-memory polynomials");
+    extern __shared__ __align__(16) uint8_t smem_raw[];
+    uint2* tws = reinterpret_cast<uint2*>(smem_raw);
+    uint32_t* P = reinterpret_cast<uint32_t*>(smem_raw + kN * 8);   // [kGiantPolys][N]
+    const int N2 = kN / 2 / N1;
+    const int rc = blockIdx.x;
+    const int r = rc / (N2 - 1), c = rc % (N2 - 1) + 1;
+    const int tid = threadIdx.x;
+    const uint32_t* so = sout + (size_t)r * N2 * 4 * kN;
+
+    // a of output[c], both primes, to coefficient form
 #pragma unroll
-    for (int comp = 0; comp < 2; comp++) {
+    for (int ch = 0; ch < 2; ch++) {
+        stage_twiddles(tws, tabs, ch, NTT_INV);
+        const uint4* src = reinterpret_cast<const uint4*>(so + ((size_t)c * 4 + 0 * 2 + ch) * kN);
+        uint4* dst = reinterpret_cast<uint4*>(P + ch * kN);
 #pragma unroll
-        for (int ch = 0; ch < 2; ch++) {
-            const uint32_t q = ch ? kQ2 : kQ1;
-            // c2 at position k
-            const int ck = k - I;
-            uint32_t cpk = ck >= 0 ? cc[(comp * 2 + ch) * kN + ck] : negmod(cc[(comp * 2 + ch) * kN + ck + kN], q);
-            pc2[((size_t)j * 4 + comp * 2 + ch) * kN + k] = addmod(cpk, r0[(comp * 2 + ch) * kN + k], q);
-            // r1 at position src
-            uint32_t cps = cs >= 0 ? cc[(comp * 2 + ch) * kN + cs] : negmod(cc[(comp * 2 + ch) * kN + cs + kN], q);
-            uint32_t v = submod(r0[(comp * 2 + ch) * kN + src], cps, q);
-            r1v[comp][ch] = neg ? negmod(v, q) : v;
+        for (int k = tid; k < kN / 4; k += kNttThreads) dst[k] = __ldg(src + k);
+        cta_ntt_inverse(P + ch * kN, tws, ch);
+    }
+    // X -> X^g, g = 5^(N1 c), then the digits (registers first: P is overwritten)
+    const uint32_t e = (uint32_t)(N1 * c) & 2047u;
+    uint32_t ginv = 1, b5 = 5, x = (2048u - e) & 2047u;
+    while (x) { if (x & 1) ginv = (ginv * b5) & (2 * kN - 1); b5 = (b5 * b5) & (2 * kN - 1); x >>= 1; }
+    uint32_t dres[kPerThreadG][ELL][2];
+#pragma unroll
+    for (int it = 0; it < kPerThreadG; it++) {
+        const int k = tid + it * kNttThreads;
+        bool neg;
+        const int src = auto_src(k, ginv, &neg);
+        uint64_t v = crt_compose_res(P[src], P[kN + src]);
+        if (neg && v) v = kCrtMod - v;
+        int32_t dig[kMaxEll];
+        decompose_b(v, kCrtMod, g, dig);
+#pragma unroll
+        for (int j = 0; j < ELL; j++) {
+            dres[it][j][0] = signed_to_res(dig[j], kQ1);
+            dres[it][j][1] = signed_to_res(dig[j], kQ2);
         }
     }
-    // temp.b -> ptb, temp.a -> digits
-    ptb[((size_t)j * 2 + 0) * kN + k] = r1v[1][0];
-    ptb[((size_t)j * 2 + 1) * kN + k] = r1v[1][1];
-    const uint64_t va = crt_compose_res(r1v[0][0], r1v[0][1]);
-    int32_t dig[kMaxEll];
-    decompose_b(va, kCrtMod, g, dig);
-    uint32_t* o = pdig + (size_t)j * g.ell * 2 * kN;
-    for (int d = 0; d < g.ell; d++) {
-        o[(d * 2 + 0) * kN + k] = signed_to_res(dig[d], kQ1);
-        o[(d * 2 + 1) * kN + k] = signed_to_res(dig[d], kQ2);
+    __syncthreads();
+#pragma unroll
+    for (int it = 0; it < kPerThreadG; it++)
+#pragma unroll
+        for (int j = 0; j < ELL; j++)
+#pragma unroll
+            for (int ch = 0; ch < 2; ch++) P[(j * 2 + ch) * kN + tid + it * kNttThreads] = dres[it][j][ch];
+    // digit transforms and the key multiply-accumulate, prime by prime
+    const uint32_t* key = gkeys + (size_t)(c - 1) * ELL * 2 * 2 * kN;   // [ELL][2 comp][2 ch][N]
+    const uint16_t* sig = gsigma + (size_t)(c - 1) * kN;
+#pragma unroll 1
+    for (int ch = 0; ch < 2; ch++) {
+        __syncthreads();
+        stage_twiddles(tws, tabs, ch, NTT_FWD);
+        cta_ntt_forward_m<ELL>(P + ch * kN, 2 * kN, tws, ch);   // digits j of this prime: P[j*2+ch]
+        const ChanConst cc = c_dev.ch[ch];
+        unsigned long long* acc_a = acc + ((size_t)(r * 2 + 0) * 2 + ch) * kN;
+        unsigned long long* acc_b = acc + ((size_t)(r * 2 + 1) * 2 + ch) * kN;
+        const uint32_t* bsrc = so + ((size_t)c * 4 + 1 * 2 + ch) * kN;
+#pragma unroll
+        for (int it = 0; it < kPerThreadG; it++) {
+            const int k = tid + it * kNttThreads;
+            uint64_t sa = 0, sb = 0;
+#pragma unroll
+            for (int j = 0; j < ELL; j++) {
+                const uint32_t d = P[(j * 2 + ch) * kN + k];
+                mad_wide(sa, d, __ldg(key + ((j * 2 + 0) * 2 + ch) * kN + k));
+                mad_wide(sb, d, __ldg(key + ((j * 2 + 1) * 2 + ch) * kN + k));
+            }
+            const uint32_t ca = negmod(reduce64(sa, cc.q, cc.barrett), cc.q);
+            const uint32_t cb = addmod(__ldg(bsrc + sig[k]), negmod(reduce64(sb, cc.q, cc.barrett), cc.q), cc.q);
+            atomicAdd(acc_a + k, (unsigned long long)ca);
+            atomicAdd(acc_b + k, (unsigned long long)cb);
+        }
     }
 }
 
-// One CTA per (j, comp, ch): the key switch of evalAuto (answer.cpp:617-645)
-// and the final addAndEqual of convertTwoRLWEs:
-//   a' = -sum_d dig_d * key[d].a,  b' = NTT(temp.b) - sum_d dig_d * key[d].b,
-//   rlwes[j] = INTT(a', b') + c2.
-__global__ void __launch_bounds__(kNttThreads) k_pack_mac_intt(const uint32_t* __restrict__ pdig,
-                                                               const uint32_t* __restrict__ ptb,
-                                                               const uint32_t* __restrict__ pc2,
-                                                               const uint32_t* __restrict__ key,
-                                                               uint32_t* __restrict__ ext, int ell, NttTables tabs) {
+// result[r][comp][ch][k] = (output[0] + accumulated giant steps) mod q
+__global__ void k_giant_finish(const uint32_t* __restrict__ sout, const unsigned long long* __restrict__ acc,
+                               uint32_t* __restrict__ result, int R, int N2) {
+    const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long)R * 4 * kN) return;
+    const int k = (int)(idx % kN);
+    const int cc_ = (int)((idx / kN) % 4);      // comp * 2 + ch
+    const long r = idx / (4 * kN);
+    const ChanConst q = c_dev.ch[cc_ & 1];
+    const uint64_t v = (uint64_t)sout[((size_t)r * N2 * 4 + cc_) * kN + k] + acc[idx];
+    result[idx] = reduce64(v, q.q, q.barrett);
+}
+
+}  // namespace kspir
+
+namespace kspir {
+
+// ---------------------------------------------------------------------------
+// fused packing level: one CTA per (pair j, prime ch) runs convertTwoRLWEs
+// (answer.cpp:720-739) with its evalAuto key switch (answer.cpp:576-648) in
+// shared memory.  It reads level input `in` and writes level output `out`
+// (two buffers: both primes of in[j] are read while the other CTA of the pair
+// writes its prime of out[j]).
+//   c' = X^I c,  r1 = r0 - c',  c2 = c' + r0,  temp = auto_g(r1), g = N/I + 1
+//   a' = -sum_d dig_d * key[d].a,  b' = NTT(temp.b) - sum_d dig_d * key[d].b
+//   out[j] = INTT(a', b') + c2
+constexpr int kPackPolys = 5;    // ell = 4 digits + temp.b
+constexpr int kPackSmem = kN * 8 + kPackPolys * kN * 4;
+
+template <int ELL>
+__global__ void __launch_bounds__(kNttThreads) k_pack_fused(const uint32_t* __restrict__ in,
+                                                            uint32_t* __restrict__ out,
+                                                            const uint32_t* __restrict__ key, int I, uint32_t ginv,
+                                                            NttTables tabs, GadgetB g) {
+    static_assert(ELL + 1 <= kPackPolys, "shared-memory polynomials");
     extern __shared__ __align__(16) uint8_t smem_raw[];
     uint2* tws = reinterpret_cast<uint2*>(smem_raw);
-    uint32_t* s = reinterpret_cast<uint32_t*>(smem_raw + kN * 8);
-    constexpr int T = kNttThreads;
-    const int ch = blockIdx.x % 2, comp = (blockIdx.x / 2) % 2, j = blockIdx.x / 4;
-    const ChanConst cc = c_dev.ch[ch];
-    stage_twiddles(tws, tabs, ch, NTT_INV);
-    const uint32_t* d = pdig + (size_t)j * ell * 2 * kN;
+    uint32_t* P = reinterpret_cast<uint32_t*>(smem_raw + kN * 8);   // [kPackPolys][N]
+    const int j = blockIdx.x >> 1, ch = blockIdx.x & 1;
+    const int tid = threadIdx.x;
+    const uint32_t* r0 = in + (size_t)j * 4 * kN;
+    const uint32_t* cc = in + (size_t)(I + j) * 4 * kN;
+    const uint32_t q = c_dev.ch[ch].q;
+    stage_twiddles(tws, tabs, ch, NTT_FWD);
+    // X^I c at position p of polynomial (comp, prime)
+    auto shifted = [&](int comp, int pch, int p) -> uint32_t {
+        const int s = p - I;
+        const uint32_t qq = pch ? kQ2 : kQ1;
+        return s >= 0 ? __ldg(cc + (comp * 2 + pch) * kN + s) : negmod(__ldg(cc + (comp * 2 + pch) * kN + s + kN), qq);
+    };
+    uint32_t c2v[kPerThreadG][2];
 #pragma unroll
-    for (int k = threadIdx.x; k < kN; k += T) {
-        uint64_t acc = 0;
-        for (int dd = 0; dd < ell; dd++)
-            acc += (uint64_t)d[(dd * 2 + ch) * kN + k] * key[((dd * 2 + comp) * 2 + ch) * kN + k];
-        const uint32_t m = reduce64(acc, cc.q, cc.barrett);
-        s[k] = comp == 0 ? negmod(m, cc.q) : submod(ptb[((size_t)j * 2 + ch) * kN + k], m, cc.q);
+    for (int it = 0; it < kPerThreadG; it++) {
+        const int k = tid + it * kNttThreads;
+#pragma unroll
+        for (int comp = 0; comp < 2; comp++)
+            c2v[it][comp] = addmod(shifted(comp, ch, k), __ldg(r0 + (comp * 2 + ch) * kN + k), q);
+        bool neg;
+        const int src = auto_src(k, ginv, &neg);
+        uint32_t ra[2];
+#pragma unroll
+        for (int pch = 0; pch < 2; pch++) {
+            const uint32_t qq = pch ? kQ2 : kQ1;
+            const uint32_t v = submod(__ldg(r0 + (0 * 2 + pch) * kN + src), shifted(0, pch, src), qq);
+            ra[pch] = neg ? negmod(v, qq) : v;
+        }
+        int32_t dig[kMaxEll];
+        decompose_b(crt_compose_res(ra[0], ra[1]), kCrtMod, g, dig);
+#pragma unroll
+        for (int d = 0; d < ELL; d++) P[d * kN + k] = signed_to_res(dig[d], q);
+        const uint32_t vb = submod(__ldg(r0 + (1 * 2 + ch) * kN + src), shifted(1, ch, src), q);
+        P[ELL * kN + k] = neg ? negmod(vb, q) : vb;
     }
-    cta_ntt_inverse(s, tws, ch);
-    const uint32_t* c2 = pc2 + ((size_t)j * 4 + comp * 2 + ch) * kN;
-    uint32_t* o = ext + ((size_t)j * 4 + comp * 2 + ch) * kN;
+    cta_ntt_forward_m<ELL + 1>(P, kN, tws, ch);
+    const ChanConst cq = c_dev.ch[ch];
 #pragma unroll
-    for (int k = threadIdx.x; k < kN; k += T) o[k] = addmod(s[k], c2[k], cc.q);
+    for (int it = 0; it < kPerThreadG; it++) {
+        const int k = tid + it * kNttThreads;
+        uint64_t sa = 0, sb = 0;
+#pragma unroll
+        for (int d = 0; d < ELL; d++) {
+            const uint32_t dv = P[d * kN + k];
+            mad_wide(sa, dv, __ldg(key + ((d * 2 + 0) * 2 + ch) * kN + k));
+            mad_wide(sb, dv, __ldg(key + ((d * 2 + 1) * 2 + ch) * kN + k));
+        }
+        const uint32_t a2 = negmod(reduce64(sa, cq.q, cq.barrett), q);
+        const uint32_t b2 = submod(P[ELL * kN + k], reduce64(sb, cq.q, cq.barrett), q);
+        P[k] = a2;            // only this thread reads index k of these rows
+        P[kN + k] = b2;
+    }
+    stage_twiddles(tws, tabs, ch, NTT_INV);   // the forward transforms ended with a barrier
+    cta_ntt_inverse_m<2>(P, kN, tws, ch);
+#pragma unroll
+    for (int it = 0; it < kPerThreadG; it++) {
+        const int k = tid + it * kNttThreads;
+#pragma unroll
+        for (int comp = 0; comp < 2; comp++)
+            out[((size_t)j * 4 + comp * 2 + ch) * kN + k] = addmod(P[comp * kN + k], c2v[it][comp], q);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// fused external product: one CTA per (r, prime ch) runs externalProduct
+// (lwe.cpp:761-808) in shared memory:
+//   INTT(first_dim) (both primes, to compose) -> decompose_rlwe (2 ell rows)
+//   -> row transforms -> init + sum_row row * rgsw[row] -> INTT
+constexpr int kExtPolys = 4;
+constexpr int kExtSmem = kN * 8 + kExtPolys * kN * 4;
+
+template <int ELL>
+__global__ void __launch_bounds__(kNttThreads) k_ext_fused(const uint32_t* __restrict__ first_dim,
+                                                           const uint32_t* __restrict__ rgsw,
+                                                           const uint32_t* __restrict__ init,
+                                                           uint32_t* __restrict__ ext,
+                                                           uint32_t* __restrict__ coef_out, NttTables tabs,
+                                                           GadgetS g) {
+    static_assert(2 * ELL <= kExtPolys, "shared-memory polynomials");
+    extern __shared__ __align__(16) uint8_t smem_raw[];
+    uint2* tws = reinterpret_cast<uint2*>(smem_raw);
+    uint32_t* P = reinterpret_cast<uint32_t*>(smem_raw + kN * 8);   // [4][N]
+    const int r = blockIdx.x >> 1, ch = blockIdx.x & 1;
+    const int tid = threadIdx.x;
+    const uint32_t* fd = first_dim + (size_t)r * 4 * kN;          // [comp][prime][N]
+    // first_dim to coefficient form, all four polynomials (P[comp * 2 + prime])
+#pragma unroll
+    for (int pch = 0; pch < 2; pch++) {
+        if (pch) __syncthreads();
+        stage_twiddles(tws, tabs, pch, NTT_INV);
+#pragma unroll
+        for (int comp = 0; comp < 2; comp++) {
+            const uint4* src = reinterpret_cast<const uint4*>(fd + (comp * 2 + pch) * kN);
+            uint4* dst = reinterpret_cast<uint4*>(P + (comp * 2 + pch) * kN);
+#pragma unroll
+            for (int k = tid; k < kN / 4; k += kNttThreads) dst[k] = __ldg(src + k);
+        }
+        cta_ntt_inverse_m<2>(P + pch * kN, 2 * kN, tws, pch);   // a and b of this prime
+    }
+    if (coef_out && ch == 0) {
+        uint4* dst = reinterpret_cast<uint4*>(coef_out + (size_t)r * 4 * kN);
+        const uint4* src = reinterpret_cast<const uint4*>(P);
+#pragma unroll
+        for (int k = tid; k < kN; k += kNttThreads) dst[k] = src[k];
+    }
+    // signed digits of a and b (rows comp * ELL + t), residues of this prime
+    uint32_t dres[kPerThreadG][2 * ELL];
+#pragma unroll
+    for (int it = 0; it < kPerThreadG; it++) {
+        const int k = tid + it * kNttThreads;
+#pragma unroll
+        for (int comp = 0; comp < 2; comp++) {
+            int32_t dig[kMaxEll];
+            decompose_signed(crt_compose_res(P[(comp * 2 + 0) * kN + k], P[(comp * 2 + 1) * kN + k]), kCrtMod, g, dig);
+#pragma unroll
+            for (int t = 0; t < ELL; t++) dres[it][comp * ELL + t] = signed_to_res(dig[t], ch ? kQ2 : kQ1);
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int it = 0; it < kPerThreadG; it++)
+#pragma unroll
+        for (int row = 0; row < 2 * ELL; row++) P[row * kN + tid + it * kNttThreads] = dres[it][row];
+    stage_twiddles(tws, tabs, ch, NTT_FWD);
+    cta_ntt_forward_m<2 * ELL>(P, kN, tws, ch);
+    const ChanConst cq = c_dev.ch[ch];
+    uint32_t outv[kPerThreadG][2];
+#pragma unroll
+    for (int it = 0; it < kPerThreadG; it++) {
+        const int k = tid + it * kNttThreads;
+#pragma unroll
+        for (int comp = 0; comp < 2; comp++) {
+            uint64_t s = 0;
+#pragma unroll
+            for (int row = 0; row < 2 * ELL; row++)
+                mad_wide(s, P[row * kN + k], __ldg(rgsw + ((row * 2 + comp) * 2 + ch) * kN + k));
+            const uint32_t m = reduce64(s, cq.q, cq.barrett);
+            outv[it][comp] = init ? addmod(__ldg(init + ((size_t)r * 4 + comp * 2 + ch) * kN + k), m, cq.q) : m;
+        }
+    }
+#pragma unroll
+    for (int it = 0; it < kPerThreadG; it++) {
+        const int k = tid + it * kNttThreads;
+        P[k] = outv[it][0];        // only this thread reads index k of rows 0, 1
+        P[kN + k] = outv[it][1];
+    }
+    stage_twiddles(tws, tabs, ch, NTT_INV);   // the forward transforms ended with a barrier
+    cta_ntt_inverse_m<2>(P, kN, tws, ch);
+#pragma unroll
+    for (int it = 0; it < kPerThreadG; it++) {
+        const int k = tid + it * kNttThreads;
+#pragma unroll
+        for (int comp = 0; comp < 2; comp++) ext[((size_t)r * 4 + comp * 2 + ch) * kN + k] = P[comp * kN + k];
+    }
 }
 
 }  // namespace kspir

@@ -135,8 +135,7 @@ struct WsSlot {
     void* mem = nullptr;
     uint32_t* stage32 = nullptr;   // scratch residues for the staged entry points
     NttJob* jobs = nullptr;        // device job list
-    int seg_q = 0, n_q = 0, seg_inter = 0, seg_dig1 = 0, seg_ginv = 0, n_ginv = 0, seg_gfwd = 0, n_gfwd = 0;
-    int seg_einv = 0, seg_efwd = 0, seg_pfwd[10] = {0};
+    int seg_q = 0, n_q = 0, seg_inter = 0, seg_dig1 = 0;
 };
 
 constexpr int kTimingRing = 512;   // per-answer event sets kept for kspir_timing_summary
@@ -288,15 +287,11 @@ int init_workspace(kspir_ctx* c, WsSlot& s) {
         {(void**)&w.dig1, 9 * P},
         {(void**)&w.cipherbuf, (size_t)kN * N1 * 2 * 8},
         {(void**)&w.sout, (size_t)r * N2 * 4 * P},
-        {(void**)&w.gcoef, (size_t)r * std::max(1, N2 - 1) * 2 * P},
-        {(void**)&w.gdig, (size_t)r * std::max(1, N2 - 1) * c->gad.giant.ell * 2 * P},
         {(void**)&w.result, (size_t)r * 4 * P},
         {(void**)&w.ecoef, (size_t)r * 4 * P},
-        {(void**)&w.edig, (size_t)r * 2 * c->gad.ext.ell * 2 * P},
         {(void**)&w.ext, (size_t)r * 4 * P},
-        {(void**)&w.pdig, (size_t)half * c->gad.pack.ell * 2 * P},
-        {(void**)&w.ptb, (size_t)half * 2 * P},
-        {(void**)&w.pc2, (size_t)half * 4 * P},
+        {(void**)&w.ext2, (size_t)half * 4 * P},
+        {(void**)&w.gacc, (size_t)r * 4 * kN * 8},
         {(void**)&w.resp64, 2 * kN * 8},
         {(void**)&w.err, 256},
         {(void**)&s.stage32, (size_t)r * 4 * P},
@@ -332,50 +327,6 @@ int init_workspace(kspir_ctx* c, WsSlot& s) {
     s.seg_dig1 = (int)jobs.size();
     for (int j = 0; j < 3; j++)
         for (int ch = 0; ch < 3; ch++) add(w.dig1 + (j * 3 + ch) * kN, w.dig1 + (j * 3 + ch) * kN, ch, 1);
-    s.seg_ginv = (int)jobs.size();
-    for (int rr = 0; rr < r; rr++)
-        for (int cc = 1; cc < N2; cc++)
-            for (int ch = 0; ch < 2; ch++)
-                add(w.sout + (((size_t)rr * N2 + cc) * 4 + 0 * 2 + ch) * kN,
-                    w.gcoef + (((size_t)rr * (N2 - 1) + cc - 1) * 2 + ch) * kN, ch, 1);
-    s.n_ginv = (int)jobs.size() - s.seg_ginv;
-    s.seg_gfwd = (int)jobs.size();
-    const int ge = c->gad.giant.ell;
-    for (int rr = 0; rr < r; rr++)
-        for (int cc = 1; cc < N2; cc++)
-            for (int j = 0; j < ge; j++)
-                for (int ch = 0; ch < 2; ch++) {
-                    uint32_t* p = w.gdig + ((((size_t)rr * (N2 - 1) + cc - 1) * ge + j) * 2 + ch) * kN;
-                    add(p, p, ch, 1);
-                }
-    s.n_gfwd = (int)jobs.size() - s.seg_gfwd;
-    s.seg_einv = (int)jobs.size();
-    for (int rr = 0; rr < r; rr++)
-        for (int q = 0; q < 4; q++) add(w.result + ((size_t)rr * 4 + q) * kN, w.ecoef + ((size_t)rr * 4 + q) * kN, q & 1, 1);
-    s.seg_efwd = (int)jobs.size();
-    const int erows = 2 * c->gad.ext.ell;
-    for (int rr = 0; rr < r; rr++)
-        for (int row = 0; row < erows; row++)
-            for (int ch = 0; ch < 2; ch++) {
-                uint32_t* p = w.edig + (((size_t)rr * erows + row) * 2 + ch) * kN;
-                add(p, p, ch, 1);
-            }
-    const int pe = c->gad.pack.ell;
-    for (int lv = 0; lv < c->levels; lv++) {
-        const int I = 1 << lv;
-        s.seg_pfwd[lv] = (int)jobs.size();
-        for (int j = 0; j < I; j++)
-            for (int d = 0; d < pe; d++)
-                for (int ch = 0; ch < 2; ch++) {
-                    uint32_t* p = w.pdig + (((size_t)j * pe + d) * 2 + ch) * kN;
-                    add(p, p, ch, 1);
-                }
-        for (int j = 0; j < I; j++)
-            for (int ch = 0; ch < 2; ch++) {
-                uint32_t* p = w.ptb + ((size_t)j * 2 + ch) * kN;
-                add(p, p, ch, 1);
-            }
-    }
     KS_CUDA(c, cudaMalloc(&s.jobs, jobs.size() * sizeof(NttJob)));
     KS_COPY(c, s.jobs, jobs.data(), jobs.size() * sizeof(NttJob), cudaMemcpyHostToDevice);
     return KSPIR_OK;
@@ -411,7 +362,7 @@ void enqueue_scan(kspir_ctx* c, WsSlot& s, cudaStream_t st) {
     switch (c->N1) {
 #define KS_SCAN(n) \
     case n: k_scan<n><<<c->nsm, ScanCfg<n>::THREADS, ScanCfg<n>::SMEM, st>>>(c->db, w.cipherbuf, w.sout, R, w.err); break;
-        KS_SCAN(64) KS_SCAN(128) KS_SCAN(256) KS_SCAN(512)
+        KS_SCAN(64) KS_SCAN(128) KS_SCAN(256)
 #undef KS_SCAN
     }
 }
@@ -419,49 +370,42 @@ void enqueue_scan(kspir_ctx* c, WsSlot& s, cudaStream_t st) {
 void enqueue_giant(kspir_ctx* c, WsSlot& s, const ClientKeysDev& keys, cudaStream_t st) {
     Workspace& w = s.ws;
     const int R = c->p.r;
-    if (c->N2 > 1) {
-        k_ntt_jobs<true><<<s.n_ginv, kNttThreads, kNttJobSmem, st>>>(s.jobs + s.seg_ginv, c->ntabs);
-        k_giant_decomp<<<blocks_for((long)R * (c->N2 - 1) * kN, 256), 256, 0, st>>>(w.gcoef, w.gdig, R, c->N1,
-                                                                                    c->gad.giant);
-        k_ntt_jobs<false><<<s.n_gfwd, kNttThreads, kNttJobSmem, st>>>(s.jobs + s.seg_gfwd, c->ntabs);
-    }
-    k_giant_accum<<<blocks_for((long)R * 2 * kN, 256), 256, 0, st>>>(w.sout, w.gdig, keys.giant, c->sigma_giant,
-                                                                      w.result, R, c->N1, c->gad.giant.ell);
+    cudaMemsetAsync(w.gacc, 0, (size_t)R * 4 * kN * 8, st);
+    if (c->N2 > 1)
+        k_giant_fused<2><<<R * (c->N2 - 1), kNttThreads, kGiantSmem, st>>>(w.sout, keys.giant, c->sigma_giant, w.gacc,
+                                                                          c->N1, c->ntabs, c->gad.giant);
+    k_giant_finish<<<blocks_for((long)R * 4 * kN, 256), 256, 0, st>>>(w.sout, w.gacc, w.result, R, c->N2);
 }
 
 // external products of `count` first-dimension results (result -> ext);
-// `init` holds NTT-domain accumulators ([count][2][2][N]) or is null for zero
+// `init` holds NTT-domain accumulators ([count][2][2][N]) or is null for zero;
+// coef_out (or null) receives the first-dimension results in coefficient form
 void enqueue_ext(kspir_ctx* c, WsSlot& s, const ClientKeysDev& keys, int count, const uint32_t* init,
-                 cudaStream_t st) {
+                 uint32_t* coef_out, cudaStream_t st) {
     Workspace& w = s.ws;
-    k_ntt_jobs<true><<<count * 4, kNttThreads, kNttJobSmem, st>>>(s.jobs + s.seg_einv, c->ntabs);
-    k_ext_decomp<<<blocks_for((long)count * kN, 256), 256, 0, st>>>(w.ecoef, w.edig, count, c->gad.ext);
-    k_ntt_jobs<false><<<count * 2 * c->gad.ext.ell * 2, kNttThreads, kNttJobSmem, st>>>(s.jobs + s.seg_efwd,
-                                                                                      c->ntabs);
-    k_ext_mac_intt<<<count * 4, kNttThreads, kMacSmem, st>>>(w.edig, keys.rgsw, init, w.ext, 2 * c->gad.ext.ell,
-                                                             c->ntabs);
+    k_ext_fused<2><<<count * 2, kNttThreads, kExtSmem, st>>>(w.result, keys.rgsw, init, w.ext, coef_out, c->ntabs,
+                                                              c->gad.ext);
 }
 
 void enqueue_packing(kspir_ctx* c, WsSlot& s, const ClientKeysDev& keys, cudaStream_t st) {
     Workspace& w = s.ws;
     const int pe = c->gad.pack.ell;
+    const uint32_t* cur = w.ext;
     for (int lv = c->levels - 1; lv >= 0; lv--) {
         const int I = 1 << lv;
         const uint32_t ginv = inv_mod_2n((uint32_t)(kN / I + 1));
-        k_pack_prep<<<blocks_for((long)I * kN, 256), 256, 0, st>>>(w.ext, w.pdig, w.ptb, w.pc2, I, ginv, c->gad.pack);
-        k_ntt_jobs<false><<<I * (pe * 2 + 2), kNttThreads, kNttJobSmem, st>>>(s.jobs + s.seg_pfwd[lv], c->ntabs);
-        k_pack_mac_intt<<<I * 4, kNttThreads, kMacSmem, st>>>(w.pdig, w.ptb, w.pc2,
-                                                              keys.packing + (size_t)lv * pe * 4 * kN, w.ext, pe,
-                                                              c->ntabs);
+        uint32_t* out = (cur == w.ext) ? w.ext2 : w.ext;
+        k_pack_fused<4><<<I * 2, kNttThreads, kPackSmem, st>>>(cur, out, keys.packing + (size_t)lv * pe * 4 * kN, I,
+                                                               ginv, c->ntabs, c->gad.pack);
+        cur = out;
     }
-    k_compose_words<<<2 * kN / 256, 256, 0, st>>>(w.ext, w.resp64, 2);
+    k_compose_words<<<2 * kN / 256, 256, 0, st>>>(cur, w.resp64, 2);
 }
 
 // kernels launched by one enqueue_answer
 long answer_launches(const kspir_ctx* c) {
-    long n = 7 + 1 + (c->N2 > 1 ? 4 : 1) + 4 + 3L * c->levels + 1;
-    if (c->N1h - 1 <= 0) n -= 1;
-    return n;
+    // baby 7, scan 1, giant 2, external product 1, packing one per level + compose
+    return 7 + 1 + (c->N2 > 1 ? 2 : 1) + 1 + c->levels + 1;
 }
 
 // Captures the four non-scan phases of one (workspace, client) pair as CUDA
@@ -479,7 +423,7 @@ int build_graphs(kspir_ctx* c, int wsi, int client) {
         KS_CUDA(c, cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
         if (ph == 0) enqueue_baby(c, s, keys, cs);
         else if (ph == 1) enqueue_giant(c, s, keys, cs);
-        else if (ph == 2) enqueue_ext(c, s, keys, c->p.r, nullptr, cs);
+        else if (ph == 2) enqueue_ext(c, s, keys, c->p.r, nullptr, nullptr, cs);
         else enqueue_packing(c, s, keys, cs);
         KS_CUDA(c, cudaStreamEndCapture(cs, &g));
         cudaError_t e = cudaGraphInstantiate(&pg.g[ph], g, 0);
@@ -518,7 +462,7 @@ int enqueue_answer(kspir_ctx* c, int wsi, int client, cudaStream_t st) {
         cudaEventRecord(ev[2], st);
         enqueue_giant(c, s, keys, st);
         cudaEventRecord(ev[3], st);
-        enqueue_ext(c, s, keys, c->p.r, nullptr, st);
+        enqueue_ext(c, s, keys, c->p.r, nullptr, nullptr, st);
         cudaEventRecord(ev[4], st);
         enqueue_packing(c, s, keys, st);
         cudaEventRecord(ev[5], st);
@@ -582,7 +526,7 @@ int kspir_ctx_create(int device, const kspir_params* params, kspir_ctx** out) {
     if (!params || !out) return KSPIR_ERR_INVALID_ARG;
     const kspir_params p = *params;
     auto pow2 = [](int v) { return v > 0 && (v & (v - 1)) == 0; };
-    if (!pow2(p.r) || p.r > 512 || !pow2(p.N1) || p.N1 < 64 || p.N1 > 512 || p.max_clients < 1 ||
+    if (!pow2(p.r) || p.r > 512 || !pow2(p.N1) || p.N1 < 64 || p.N1 > 256 || p.max_clients < 1 ||
         p.max_inflight < 1)
         return KSPIR_ERR_INVALID_ARG;
     std::unique_ptr<kspir_ctx> c(new kspir_ctx());
@@ -597,9 +541,12 @@ int kspir_ctx_create(int device, const kspir_params* params, kspir_ctx** out) {
     KS_CUDA(c.get(), cudaStreamCreateWithFlags(&c->capture, cudaStreamNonBlocking));
     if (const char* e = getenv("KSPIR_NO_GRAPHS")) c->use_graphs = !(e[0] == '1');
     KS_CUDA(c.get(), cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device));
+    KS_CUDA(c.get(), cudaFuncSetAttribute(k_giant_fused<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGiantSmem));
+    KS_CUDA(c.get(), cudaFuncSetAttribute(k_ext_fused<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kExtSmem));
+    KS_CUDA(c.get(), cudaFuncSetAttribute(k_pack_fused<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, kPackSmem));
 #define KS_ATTR(n) \
     KS_CUDA(c.get(), cudaFuncSetAttribute(k_scan<n>, cudaFuncAttributeMaxDynamicSharedMemorySize, ScanCfg<n>::SMEM));
-    KS_ATTR(64) KS_ATTR(128) KS_ATTR(256) KS_ATTR(512)
+    KS_ATTR(64) KS_ATTR(128) KS_ATTR(256)
 #undef KS_ATTR
     int rc = init_constants(c.get());
     if (rc) return rc;
@@ -861,7 +808,7 @@ int kspir_external_product(kspir_ctx* c, int client, uint64_t* result, uint64_t*
     uint32_t* acc = s.ws.sout;   // r*N2*4*N >= count*4*N residues
     KS_CUDA(c, cudaMemcpyAsync(words, result, n * 8, cudaMemcpyHostToDevice, st));
     k_split_words<<<blocks_for((long)n, 256), 256, 0, st>>>(words, acc, count * 2);
-    enqueue_ext(c, s, keys, count, acc, st);
+    enqueue_ext(c, s, keys, count, acc, s.ws.ecoef, st);
     k_compose_words<<<blocks_for((long)n, 256), 256, 0, st>>>(s.ws.ext, words, count * 2);
     KS_CUDA(c, cudaGetLastError());
     KS_CUDA(c, cudaMemcpyAsync(result, words, n * 8, cudaMemcpyDeviceToHost, st));

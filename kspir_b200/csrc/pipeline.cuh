@@ -37,15 +37,11 @@ struct Workspace {
     uint32_t* dig1;         // [3][3 ch][N] digits of the intermediate -> NTT form
     uint64_t* cipherbuf;    // [N][N1][2] reference reorientCipher layout (twosteps.cpp:1386)
     uint32_t* sout;         // [r][N2][2 comp][2 ch][N] DB-scan outputs, NTT form
-    uint32_t* gcoef;        // [r][N2-1][2 ch][N] giant inputs a, coefficient form
-    uint32_t* gdig;         // [r][N2-1][2][2 ch][N] giant digits -> NTT form
     uint32_t* result;       // [r][2 comp][2 ch][N] first-dimension results, NTT form
     uint32_t* ecoef;        // [r][2 comp][2 ch][N] result, coefficient form
-    uint32_t* edig;         // [r][4][2 ch][N] external-product digits -> NTT form
     uint32_t* ext;          // [r][2 comp][2 ch][N] external products, coefficient form
-    uint32_t* pdig;         // [r/2][4][2 ch][N] packing digits -> NTT form
-    uint32_t* ptb;          // [r/2][2 ch][N] packing automorphed b -> NTT form
-    uint32_t* pc2;          // [r/2][2 comp][2 ch][N] packing second operand
+    uint32_t* ext2;         // [r/2][2 comp][2 ch][N] packing levels ping-pong with ext
+    unsigned long long* gacc;  // [r][2 comp][2 ch][N] giant-step accumulators
     uint64_t* resp64;       // [2][N] response words
     int* err;               // device error word (bounded waits)
 };
