@@ -54,7 +54,7 @@ typedef struct kspir_params {
     int32_t r;            /* packing number = number of sub-databases, power of two, 1..512 */
     int32_t N1;           /* baby steps: 64, 128 or 256; N2 = N/2/N1 */
     int32_t max_clients;  /* client key slots held on the device */
-    int32_t max_inflight; /* concurrent query workspaces (1 for the plain path) */
+    int32_t max_inflight; /* query workspaces = largest batch (1 for the plain path) */
 } kspir_params;
 
 /* Context bound to one CUDA device.  Allocates the per-query workspaces. */
@@ -88,6 +88,35 @@ int kspir_answer(kspir_ctx* ctx, int client, const uint64_t* query, uint64_t* re
  * enqueued.  Call kspir_sync to wait and collect device-side errors. */
 int kspir_answer_device(kspir_ctx* ctx, int client, const uint64_t* d_query, uint64_t* d_response, void* stream);
 int kspir_sync(kspir_ctx* ctx);
+
+/* Batched answer: n queries of (possibly) different clients in one launch
+ * sequence (every kernel covers all n queries; the first-dimension scan reads
+ * the database once for the whole batch on the tensor cores when the context
+ * has N1 = 128 and max_inflight >= 2).  No reference counterpart as one call:
+ * each response equals kspir_answer(clients[i], query i), which equals the
+ * reference's test-pir.cpp:110-116 on that query.
+ *   queries   [n][2][2][N]   layout of kspir_answer's query
+ *   responses [n][2][N]
+ * 1 <= n <= min(max_inflight, 256).  Host buffers; returns when done. */
+int kspir_answer_batch(kspir_ctx* ctx, int n, const int32_t* clients, const uint64_t* queries, uint64_t* responses);
+
+/* Same on device buffers, enqueued on `stream` (NULL = context stream);
+ * returns once enqueued (kspir_sync waits and reports device errors). */
+int kspir_answer_batch_device(kspir_ctx* ctx, int n, const int32_t* clients, const uint64_t* d_queries,
+                              uint64_t* d_responses, void* stream);
+
+/* Database-scan variant used for a batch of n queries:
+ *   0 CUDA-core scan, one database pass per query
+ *   1..4 tensor-core scan with query tiles of 4, 8, 16, 32 queries
+ * kspir_tune_batch times every variant on the resident database (results are
+ * identical by construction; only speed differs), keeps the fastest for n and
+ * returns it; ms_out ([5] or NULL) receives each variant's scan time (1e30 for
+ * variants not tried).  Do not call while answers are in flight: it uses the
+ * workspaces.  kspir_set_scan_kind forces a variant (-1 = back to the
+ * default), kspir_get_scan_kind reports the one in use. */
+int kspir_tune_batch(kspir_ctx* ctx, int n, int* kind_out, float* ms_out);
+int kspir_set_scan_kind(kspir_ctx* ctx, int n, int kind);
+int kspir_get_scan_kind(kspir_ctx* ctx, int n);
 
 /* Reference matrix_vector_mul_bsgs_rns_crt_large (twosteps.h:55-57,
  * twosteps.cpp:1527-1579) for one client: query_inout is modswitched in place
@@ -140,15 +169,15 @@ int kspir_external_product_noalloc(int device, const uint64_t* d_rgsw, uint64_t*
  * row i is the NTT-slot gather that applies X -> X^(5^i).  No device needed. */
 int kspir_permutation_matrix(int32_t* perms, int N1);
 
-/* Device time of the last kspir_answer / kspir_answer_device on the
- * context's stream, in milliseconds, and per-phase split
- * (baby steps, DB scan, giant steps, external products, packing). */
+/* Device time of the last answer launch (single or batched) in
+ * milliseconds, and per-phase split (baby steps, DB scan, giant steps,
+ * external products, packing). */
 int kspir_last_timing(kspir_ctx* ctx, float* total_ms, float* phase_ms /* [5] or NULL */);
 
-/* Timing of every answer enqueued since kspir_timing_reset (the most recent
- * 512 are kept): the count, the kernels launched, and the summed device time
- * in milliseconds in total and per phase (same split as kspir_last_timing).
- * Waits for those answers to finish. */
+/* Timing of every answer launch since kspir_timing_reset (the most recent
+ * 512 launches are kept): the queries they answered, the kernels launched,
+ * and the summed device time in milliseconds in total and per phase (same
+ * split as kspir_last_timing).  Waits for those launches to finish. */
 int kspir_timing_reset(kspir_ctx* ctx);
 int kspir_timing_summary(kspir_ctx* ctx, int* answers, long* launches, float* total_ms, float* phase_ms);
 
@@ -163,6 +192,9 @@ int kspir_timing_summary(kspir_ctx* ctx, int* answers, long* launches, float* to
 #define KSPIR_STAGE_RESULT 2
 #define KSPIR_STAGE_EXT 3
 int kspir_fetch_stage(kspir_ctx* ctx, int stage, uint64_t* out, size_t words);
+/* Same for the query that ran in workspace slot `slot` (query i of the last
+ * batch ran in slot i). */
+int kspir_fetch_stage_slot(kspir_ctx* ctx, int slot, int stage, uint64_t* out, size_t words);
 
 #ifdef __cplusplus
 }

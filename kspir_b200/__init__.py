@@ -20,12 +20,14 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from .native import (BSMOD, CRTMOD, N, Q1, Q2, Context, KspirError, LIB_PATH, STAGE_CIPHERBUF, STAGE_EXT,
-                     STAGE_RESULT, STAGE_SCAN, load, permutation_matrix)
+from .native import (BSMOD, CRTMOD, N, Q1, Q2, SCAN_CUDA, SCAN_MMA4, SCAN_MMA8, SCAN_MMA16, SCAN_MMA32, SCAN_NAMES,
+                     Context, KspirError, LIB_PATH, STAGE_CIPHERBUF, STAGE_EXT, STAGE_RESULT, STAGE_SCAN, load,
+                     permutation_matrix)
 
 __all__ = [
     "N", "Q1", "Q2", "CRTMOD", "BSMOD", "Context", "KspirError", "load", "LIB_PATH", "permutation_matrix",
     "STAGE_CIPHERBUF", "STAGE_SCAN", "STAGE_RESULT", "STAGE_EXT",
+    "SCAN_CUDA", "SCAN_MMA4", "SCAN_MMA8", "SCAN_MMA16", "SCAN_MMA32", "SCAN_NAMES",
     "AutoKeyBSGSRNS", "AutoKey", "RGSWCiphertext",
     "matrix_vector_mul_bsgs_rns_crt_large", "externalProduct", "packingRLWEs",
 ]

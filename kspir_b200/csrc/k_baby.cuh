@@ -54,12 +54,24 @@ __device__ __forceinline__ uint32_t pow5_mod2n(uint32_t e) {
 constexpr int kBabySmem = kN * 8 + kN * 4;   // twiddles + one polynomial
 constexpr int kPerThread = kN / kNttThreads; // 8 coefficients per thread
 
-// One CTA per (rotation, component, crt prime): blockIdx.x = 4*ki + 2*comp + ch.
+// One CTA per (rotation, component, crt prime): blockIdx.x = 4*ki + 2*comp + ch;
+// blockIdx.y = query of the batch.
 // Each CTA recomputes the bsMod part of its component (one inverse transform)
 // so the four CTAs of a rotation run in parallel.
 template <int ELL>
-__global__ void __launch_bounds__(kNttThreads) k_baby_rot(BabyArgs a, ClientKeysDev keys, NttTables tabs) {
+__global__ void __launch_bounds__(kNttThreads) k_baby_rot(BabyArgs a, ClientKeysDev keys, NttTables tabs, Batch bt) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
+    {
+        const size_t wo = ws_off(bt);
+        a.dig = shifted(a.dig, wo);
+        a.srcB = shifted(a.srcB, wo);
+        a.srcBbs = shifted(a.srcBbs, wo);
+        a.cipherbuf = shifted(a.cipherbuf, wo);
+        a.interA = shifted(a.interA, wo);
+        a.interB = shifted(a.interB, wo);
+        a.inter_bs = shifted(a.inter_bs, wo);
+        keys = keys_at(keys, bt);
+    }
     uint2* tws = reinterpret_cast<uint2*>(smem_raw);
     uint32_t* S = reinterpret_cast<uint32_t*>(smem_raw + kN * 8);
 

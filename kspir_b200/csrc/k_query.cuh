@@ -12,7 +12,8 @@ namespace kspir {
 //  * query b as residues (its crt transform feeds the hoisted b terms);
 //  * the RNS modswitch of the query itself, (x_crt - x_bs) * bsMod^-1 mod
 //    crtMod (twosteps.cpp:1073-1086), as residues before its transform.
-__global__ void k_query_prep(Workspace ws, GadgetBsgs g) {
+__global__ void k_query_prep(Workspace ws, GadgetBsgs g, Batch bt) {
+    ws = ws_at(ws, bt);
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= kN) return;
     const uint64_t a_crt = ws.q64[k], b_crt = ws.q64[kN + k];
@@ -40,7 +41,8 @@ __global__ void k_query_prep(Workspace ws, GadgetBsgs g) {
 // Digits of the intermediate rotation (evalAutoSRNSSecond, twosteps.cpp:1109-1120):
 // decompose_bsgs of its coefficient-form a (crt residues composed to the
 // canonical word) and its bsMod part.
-__global__ void k_inter_decomp(Workspace ws, GadgetBsgs g) {
+__global__ void k_inter_decomp(Workspace ws, GadgetBsgs g, Batch bt) {
+    ws = ws_at(ws, bt);
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= kN) return;
     const uint64_t a_crt = crt_compose_res(ws.inter_acoef[k], ws.inter_acoef[kN + k]);

@@ -9,7 +9,8 @@
 // exact 64-bit sums (products < 2^56, N1 <= 512 terms; any wrap mod 2^64 is
 // the reference's too), and the reference composes out = crt_compose(a_lo,
 // a_hi), which is the canonical crtMod value with residues (a_lo mod q1,
-// a_hi mod q2).  The kernel stores those residues: sout[r][i][comp][ch][z].
+// a_hi mod q2).  The kernel stores those residues in the z-blocked layout of
+// sout_idx (row r * N2 + i, cv = comp * 2 + ch).
 //
 // Data movement: one 16 KiB slab DB[r][z] (N2 x N1 words) plus the 16*N1-byte
 // cipherbuf row z per work item, brought in by 1-D bulk copies (TMA engine,
@@ -169,7 +170,7 @@ __global__ void __launch_bounds__(ScanCfg<N1>::THREADS, 1)
             const int o = C::NOUT * lc + t;
             const int i = lr + 4 * (o >> 2), cv = o & 3;
             const uint32_t res = (cv & 1) ? mod_q2(v[t]) : mod_q1(v[t]);
-            sout[((size_t)(r * C::N2 + i) * 4 + cv) * kN + z] = res;
+            sout[sout_idx((int)r * C::N2 + i, cv, (int)z, R * C::N2)] = res;
         }
     }
 }

@@ -80,7 +80,7 @@ __global__ void __launch_bounds__(kNttThreads) k_ext_mac_intt(const uint32_t* __
 namespace kspir {
 
 // ---------------------------------------------------------------------------
-// fused giant step: one CTA per (r, c >= 1) runs the whole key switch of
+// fused giant step: one CTA per (r, c >= 1) (blockIdx.y = query of the batch) runs the whole key switch of
 // evalAutoRNSCRT for output[c] (twosteps.cpp:612-672) in shared memory:
 //   INTT(a) per prime -> compose -> X -> X^g -> decompose (ell digits)
 //   -> digit transforms -> -sum_j d_j * key[j]  and  b[sigma_g] - sum_j d_j * key[j]
@@ -96,25 +96,29 @@ __global__ void __launch_bounds__(kNttThreads) k_giant_fused(const uint32_t* __r
                                                              const uint32_t* __restrict__ gkeys,
                                                              const uint16_t* __restrict__ gsigma,
                                                              unsigned long long* __restrict__ acc, int N1,
-                                                             NttTables tabs, GadgetB g) {
+                                                             NttTables tabs, GadgetB g, int R, Batch bt) {
     static_assert(2 * ELL <= kGiantPolys, "shared-memory polynomials");
     extern __shared__ __align__(16) uint8_t smem_raw[];
     uint2* tws = reinterpret_cast<uint2*>(smem_raw);
     uint32_t* P = reinterpret_cast<uint32_t*>(smem_raw + kN * 8);   // [kGiantPolys][N]
     const int N2 = kN / 2 / N1;
+    const int rows = R * N2;
     const int rc = blockIdx.x;
     const int r = rc / (N2 - 1), c = rc % (N2 - 1) + 1;
+    const int row = r * N2 + c;
     const int tid = threadIdx.x;
-    const uint32_t* so = sout + (size_t)r * N2 * 4 * kN;
+    sout = shifted(sout, ws_off(bt));
+    acc = shifted(acc, ws_off(bt));
+    gkeys = shifted(gkeys, key_off(bt));
 
     // a of output[c], both primes, to coefficient form
 #pragma unroll
     for (int ch = 0; ch < 2; ch++) {
         stage_twiddles(tws, tabs, ch, NTT_INV);
-        const uint4* src = reinterpret_cast<const uint4*>(so + ((size_t)c * 4 + 0 * 2 + ch) * kN);
         uint4* dst = reinterpret_cast<uint4*>(P + ch * kN);
 #pragma unroll
-        for (int k = tid; k < kN / 4; k += kNttThreads) dst[k] = __ldg(src + k);
+        for (int k = tid; k < kN / 4; k += kNttThreads)
+            dst[k] = __ldg(reinterpret_cast<const uint4*>(sout + sout_idx(row, 0 * 2 + ch, 4 * k, rows)));
         cta_ntt_inverse(P + ch * kN, tws, ch);
     }
     // X -> X^g, g = 5^(N1 c), then the digits (registers first: P is overwritten)
@@ -155,7 +159,6 @@ __global__ void __launch_bounds__(kNttThreads) k_giant_fused(const uint32_t* __r
         const ChanConst cc = c_dev.ch[ch];
         unsigned long long* acc_a = acc + ((size_t)(r * 2 + 0) * 2 + ch) * kN;
         unsigned long long* acc_b = acc + ((size_t)(r * 2 + 1) * 2 + ch) * kN;
-        const uint32_t* bsrc = so + ((size_t)c * 4 + 1 * 2 + ch) * kN;
 #pragma unroll
         for (int it = 0; it < kPerThreadG; it++) {
             const int k = tid + it * kNttThreads;
@@ -167,23 +170,29 @@ __global__ void __launch_bounds__(kNttThreads) k_giant_fused(const uint32_t* __r
                 mad_wide(sb, d, __ldg(key + ((j * 2 + 1) * 2 + ch) * kN + k));
             }
             const uint32_t ca = negmod(reduce64(sa, cc.q, cc.barrett), cc.q);
-            const uint32_t cb = addmod(__ldg(bsrc + sig[k]), negmod(reduce64(sb, cc.q, cc.barrett), cc.q), cc.q);
+            const uint32_t bv = __ldg(sout + sout_idx(row, 1 * 2 + ch, sig[k], rows));
+            const uint32_t cb = addmod(bv, negmod(reduce64(sb, cc.q, cc.barrett), cc.q), cc.q);
             atomicAdd(acc_a + k, (unsigned long long)ca);
             atomicAdd(acc_b + k, (unsigned long long)cb);
         }
     }
 }
 
-// result[r][comp][ch][k] = (output[0] + accumulated giant steps) mod q
-__global__ void k_giant_finish(const uint32_t* __restrict__ sout, const unsigned long long* __restrict__ acc,
-                               uint32_t* __restrict__ result, int R, int N2) {
+// result[r][comp][ch][k] = (output[0] + accumulated giant steps) mod q; the
+// accumulator is cleared for the next query of the slot.
+__global__ void k_giant_finish(const uint32_t* __restrict__ sout, unsigned long long* __restrict__ acc,
+                               uint32_t* __restrict__ result, int R, int N2, Batch bt) {
     const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= (long)R * 4 * kN) return;
+    sout = shifted(sout, ws_off(bt));
+    acc = shifted(acc, ws_off(bt));
+    result = shifted(result, ws_off(bt));
     const int k = (int)(idx % kN);
     const int cc_ = (int)((idx / kN) % 4);      // comp * 2 + ch
-    const long r = idx / (4 * kN);
+    const int r = (int)(idx / (4 * kN));
     const ChanConst q = c_dev.ch[cc_ & 1];
-    const uint64_t v = (uint64_t)sout[((size_t)r * N2 * 4 + cc_) * kN + k] + acc[idx];
+    const uint64_t v = (uint64_t)sout[sout_idx(r * N2, cc_, k, R * N2)] + acc[idx];
+    acc[idx] = 0;
     result[idx] = reduce64(v, q.q, q.barrett);
 }
 
@@ -207,9 +216,12 @@ template <int ELL>
 __global__ void __launch_bounds__(kNttThreads) k_pack_fused(const uint32_t* __restrict__ in,
                                                             uint32_t* __restrict__ out,
                                                             const uint32_t* __restrict__ key, int I, uint32_t ginv,
-                                                            NttTables tabs, GadgetB g) {
+                                                            NttTables tabs, GadgetB g, Batch bt) {
     static_assert(ELL + 1 <= kPackPolys, "shared-memory polynomials");
     extern __shared__ __align__(16) uint8_t smem_raw[];
+    in = shifted(in, ws_off(bt));
+    out = shifted(out, ws_off(bt));
+    key = shifted(key, key_off(bt));
     uint2* tws = reinterpret_cast<uint2*>(smem_raw);
     uint32_t* P = reinterpret_cast<uint32_t*>(smem_raw + kN * 8);   // [kPackPolys][N]
     const int j = blockIdx.x >> 1, ch = blockIdx.x & 1;
@@ -289,9 +301,14 @@ __global__ void __launch_bounds__(kNttThreads) k_ext_fused(const uint32_t* __res
                                                            const uint32_t* __restrict__ init,
                                                            uint32_t* __restrict__ ext,
                                                            uint32_t* __restrict__ coef_out, NttTables tabs,
-                                                           GadgetS g) {
+                                                           GadgetS g, Batch bt) {
     static_assert(2 * ELL <= kExtPolys, "shared-memory polynomials");
     extern __shared__ __align__(16) uint8_t smem_raw[];
+    first_dim = shifted(first_dim, ws_off(bt));
+    init = shifted(init, ws_off(bt));
+    ext = shifted(ext, ws_off(bt));
+    coef_out = shifted(coef_out, ws_off(bt));
+    rgsw = shifted(rgsw, key_off(bt));
     uint2* tws = reinterpret_cast<uint2*>(smem_raw);
     uint32_t* P = reinterpret_cast<uint32_t*>(smem_raw + kN * 8);   // [4][N]
     const int r = blockIdx.x >> 1, ch = blockIdx.x & 1;

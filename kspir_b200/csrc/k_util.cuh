@@ -4,6 +4,7 @@
 
 #include "common.cuh"
 #include "ntt.cuh"
+#include "pipeline.cuh"
 
 namespace kspir {
 
@@ -20,11 +21,13 @@ struct NttJob {
 constexpr int kNttJobSmem = kN * 4 + kN * 8;
 
 template <bool INVERSE>
-__global__ void __launch_bounds__(kNttThreads) k_ntt_jobs(const NttJob* __restrict__ jobs, NttTables tabs) {
+__global__ void __launch_bounds__(kNttThreads) k_ntt_jobs(const NttJob* __restrict__ jobs, NttTables tabs, Batch bt) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
     uint2* tws = reinterpret_cast<uint2*>(smem_raw);
     uint32_t* s = reinterpret_cast<uint32_t*>(smem_raw + kN * 8);
-    const NttJob jb = jobs[blockIdx.x];
+    NttJob jb = jobs[blockIdx.x];
+    jb.src = shifted(jb.src, ws_off(bt));   // job lists address workspace slot 0
+    jb.dst = shifted(jb.dst, ws_off(bt));
     stage_twiddles(tws, tabs, jb.ch, INVERSE ? NTT_INV : NTT_FWD);
     const uint4* src4 = reinterpret_cast<const uint4*>(jb.src);
     uint4* s4 = reinterpret_cast<uint4*>(s);
@@ -49,6 +52,16 @@ __global__ void k_compose_words(const uint32_t* __restrict__ res, uint64_t* __re
     int p = idx / kN, k = idx % kN;
     const uint32_t* r = res + (size_t)p * 2 * kN;
     words[idx] = crt_compose_res(r[k], r[kN + k]);
+}
+
+// Response words of every query of a batch: resp64 of its slot = canonical
+// words of the two residue polynomials `res` (a workspace pointer of slot 0).
+__global__ void k_compose_resp(const uint32_t* __restrict__ res, Workspace w, Batch bt) {
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= 2 * kN) return;
+    const uint32_t* r = shifted(res, ws_off(bt)) + (size_t)(idx / kN) * 2 * kN;
+    const int k = idx % kN;
+    w.resp64[(size_t)batch_slot(bt) * 2 * kN + idx] = crt_compose_res(r[k], r[kN + k]);
 }
 
 // res[p][ch][k] = words[p][k] mod q_ch (ch = q1, q2) for `polys` polynomials.

@@ -9,8 +9,10 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <mutex>
+#include <type_traits>
 #include <string>
 #include <vector>
 
@@ -20,6 +22,7 @@
 #include "k_baby.cuh"
 #include "k_query.cuh"
 #include "k_scan.cuh"
+#include "k_scan_mma.cuh"
 #include "k_second.cuh"
 #include "k_util.cuh"
 #include "ntt.cuh"
@@ -128,23 +131,31 @@ GadgetBsgs make_gadget_bsgs(int ell, uint64_t base, uint64_t bg) {
 
 size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
-// ---------------------------------------------------------------------------
+constexpr int kTimingRing = 512;   // event sets of recent launches kept for kspir_timing_summary
+constexpr int kMaxBatch = 256;     // queries per launch
 
-struct WsSlot {
-    Workspace ws{};
-    void* mem = nullptr;
-    uint32_t* stage32 = nullptr;   // scratch residues for the staged entry points
-    NttJob* jobs = nullptr;        // device job list
-    int seg_q = 0, n_q = 0, seg_inter = 0, seg_dig1 = 0;
+struct ClientList {
+    int n;
+    int id[kMaxBatch];
 };
 
-constexpr int kTimingRing = 512;   // per-answer event sets kept for kspir_timing_summary
+// client_of[slot0 + i] = key slot of query i of a launch (read by the kernels)
+__global__ void k_set_clients(int* client_of, int slot0, ClientList cl) {
+    const int i = threadIdx.x;
+    if (i < cl.n) client_of[slot0 + i] = cl.id[i];
+}
 
-struct ClientSlot {
-    bool loaded = false;
-    uint32_t* mem = nullptr;
-    ClientKeysDev keys{};
-};
+// scan-stage residues back to the [row][comp][ch][N] polynomial layout
+__global__ void k_unblock_sout(const uint32_t* __restrict__ sout, uint32_t* __restrict__ out, int rows) {
+    const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long)rows * 4 * kN) return;
+    const int z = (int)(idx % kN), cv = (int)((idx / kN) % 4), row = (int)(idx / (4 * kN));
+    out[idx] = sout[sout_idx(row, cv, z, rows)];
+}
+
+// database-scan variants (chosen per batch size by kspir_tune_batch)
+enum ScanKind { SCAN_CUDA = 0, SCAN_MMA4 = 1, SCAN_MMA8 = 2, SCAN_MMA16 = 3, SCAN_MMA32 = 4, SCAN_KINDS = 5 };
+int scan_bt(int kind) { return kind == SCAN_MMA4 ? 4 : kind == SCAN_MMA8 ? 8 : kind == SCAN_MMA16 ? 16 : 32; }
 
 }  // namespace
 
@@ -156,26 +167,48 @@ struct kspir_ctx {
     std::string err;
     uint64_t* db = nullptr;
     bool db_loaded = false;
+    bool mma = false;                 // batched tensor-core scan enabled (N1 = 128, several slots)
+    uint8_t* dbop = nullptr;          // its database operand [N][2][G] tiles
+    int G = 0;
+    uint8_t* qop = nullptr;           // its query operand of one launch
     int32_t* perms = nullptr;
     bool perms_loaded = false;
-    uint32_t* tw = nullptr;          // [3][4][N]
-    uint16_t* sigma_baby = nullptr;  // [N1/2][N]
-    uint16_t* sigma_giant = nullptr; // [N2-1][N]
+    uint32_t* tw = nullptr;           // [3][4][N]
+    uint16_t* sigma_baby = nullptr;   // [N1/2][N]
+    uint16_t* sigma_giant = nullptr;  // [N2-1][N]
     NttTables ntabs{};
     PathGadgets gad{};
     int nsm = 148;
-    std::vector<ClientSlot> clients;
-    std::vector<WsSlot> ws;
-    // CUDA graphs of the four non-scan phases, per (workspace, client)
-    struct PhaseGraphs { bool ready = false; cudaGraphExec_t g[4] = {nullptr, nullptr, nullptr, nullptr}; };
-    std::vector<PhaseGraphs> graphs;   // [ws * max_clients + client]
+    // workspaces: slot s is slot 0's layout shifted by s * ws_bytes
+    void* ws_mem = nullptr;
+    size_t ws_bytes = 0;
+    Workspace ws0{};
+    uint64_t* bq64 = nullptr;         // [slots][4][N] query words
+    uint64_t* bresp = nullptr;        // [slots][2][N] response words
+    int* errs = nullptr;              // [slots][kErrStride]
+    int* client_of = nullptr;         // [slots]
+    uint32_t* stage32 = nullptr;      // [r][4][N] residues for the staged entry points
+    NttJob* jobs = nullptr;           // transform job lists of slot 0
+    int seg_q = 0, n_q = 0, seg_inter = 0, seg_dig1 = 0;
+    // client keys: key slot k is slot 0's layout shifted by k * key_bytes
+    uint32_t* key_mem = nullptr;
+    size_t key_bytes = 0;
+    ClientKeysDev keys0{};
+    std::vector<char> key_loaded;
+    // CUDA graphs of the four non-scan phases per (slot0, queries)
+    struct PhaseGraphs { cudaGraphExec_t g[4] = {nullptr, nullptr, nullptr, nullptr}; };
+    std::map<std::pair<int, int>, PhaseGraphs> graphs;
     cudaStream_t capture = nullptr;
     bool use_graphs = true;
-    // phase events of recent answers: ring[i][0..5] brackets baby / scan / giant / ext / packing
+    std::map<int, int> scan_choice;   // queries per launch -> ScanKind
+    // events of recent launches: ring[i][0..5] brackets baby / scan / giant / ext / packing
     std::vector<std::array<cudaEvent_t, 6>> ring;
-    long answers = 0;          // answers enqueued since the last kspir_timing_reset
-    long launches = 0;         // kernels launched by those answers
+    std::vector<int> ring_nq;
+    long enqueues = 0;        // launches since the last kspir_timing_reset
+    long answers = 0;         // queries of those launches
+    long launches = 0;        // kernels launched by them
     int last_slot = -1;
+    std::mutex mu;            // serialises enqueues from several host threads
 };
 
 namespace {
@@ -211,6 +244,58 @@ int copy_sync(kspir_ctx* c, void* dst, const void* src, size_t bytes, cudaMemcpy
         int rc_ = copy_sync(ctx, dst, src, bytes, kind);         \
         if (rc_) return rc_;                                     \
     } while (0)
+
+template <class T>
+T* host_shift(T* p, size_t off) {
+    return p ? reinterpret_cast<T*>(reinterpret_cast<char*>(const_cast<typename std::remove_const<T>::type*>(p)) + off)
+             : p;
+}
+
+// host copy of ws_at: the buffers of workspace slot s
+Workspace ws_host(const kspir_ctx* c, int s) {
+    Workspace w = c->ws0;
+    const size_t off = (size_t)s * c->ws_bytes;
+    w.q64 += (size_t)s * 4 * kN;
+    w.resp64 += (size_t)s * 2 * kN;
+    w.dig0 = host_shift(w.dig0, off);
+    w.qbn = host_shift(w.qbn, off);
+    w.qbbs = host_shift(w.qbbs, off);
+    w.col0 = host_shift(w.col0, off);
+    w.interA = host_shift(w.interA, off);
+    w.interB = host_shift(w.interB, off);
+    w.inter_bs = host_shift(w.inter_bs, off);
+    w.inter_acoef = host_shift(w.inter_acoef, off);
+    w.dig1 = host_shift(w.dig1, off);
+    w.cipherbuf = host_shift(w.cipherbuf, off);
+    w.sout = host_shift(w.sout, off);
+    w.result = host_shift(w.result, off);
+    w.ecoef = host_shift(w.ecoef, off);
+    w.ext = host_shift(w.ext, off);
+    w.ext2 = host_shift(w.ext2, off);
+    w.gacc = host_shift(w.gacc, off);
+    w.err += (size_t)s * kErrStride;
+    return w;
+}
+
+ClientKeysDev keys_host(const kspir_ctx* c, int k) {
+    ClientKeysDev d = c->keys0;
+    const size_t off = (size_t)k * c->key_bytes;
+    d.baby_crt = host_shift(d.baby_crt, off);
+    d.baby_bs = host_shift(d.baby_bs, off);
+    d.giant = host_shift(d.giant, off);
+    d.packing = host_shift(d.packing, off);
+    d.rgsw = host_shift(d.rgsw, off);
+    return d;
+}
+
+Batch batch_of(const kspir_ctx* c, int slot0) {
+    Batch b;
+    b.ws_bytes = c->ws_bytes;
+    b.key_bytes = c->key_bytes;
+    b.client_of = c->client_of;
+    b.slot0 = slot0;
+    return b;
+}
 
 int init_constants(kspir_ctx* c) {
     DevConst dc{};
@@ -267,15 +352,15 @@ int init_constants(kspir_ctx* c) {
     return KSPIR_OK;
 }
 
-// Carves one workspace out of a single allocation and builds its job lists.
-int init_workspace(kspir_ctx* c, WsSlot& s) {
-    const int r = c->p.r, N2 = c->N2, N1 = c->N1;
+// Carves the workspace slots (slot 0's layout repeated at ws_bytes) and the
+// slot-indexed arrays, and builds slot 0's transform job lists.
+int init_workspaces(kspir_ctx* c) {
+    const int r = c->p.r, N2 = c->N2, N1 = c->N1, S = c->p.max_inflight;
     const size_t P = (size_t)kN * 4;   // bytes of one residue poly
     const int half = std::max(1, r / 2);
     struct Part { void** dst; size_t bytes; };
-    Workspace& w = s.ws;
+    Workspace& w = c->ws0;
     std::vector<Part> parts = {
-        {(void**)&w.q64, 4 * kN * 8},
         {(void**)&w.dig0, 9 * P},
         {(void**)&w.qbn, 2 * P},
         {(void**)&w.qbbs, P},
@@ -292,28 +377,35 @@ int init_workspace(kspir_ctx* c, WsSlot& s) {
         {(void**)&w.ext, (size_t)r * 4 * P},
         {(void**)&w.ext2, (size_t)half * 4 * P},
         {(void**)&w.gacc, (size_t)r * 4 * kN * 8},
-        {(void**)&w.resp64, 2 * kN * 8},
-        {(void**)&w.err, 256},
-        {(void**)&s.stage32, (size_t)r * 4 * P},
     };
     size_t total = 0;
     for (auto& pt : parts) total = align_up(total, 256) + pt.bytes;
-    KS_CUDA(c, cudaMalloc(&s.mem, total));
-    KS_CUDA(c, cudaMemsetAsync(s.mem, 0, total, c->stream));
-    KS_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->ws_bytes = align_up(total, 4096);
+    KS_CUDA(c, cudaMalloc(&c->ws_mem, c->ws_bytes * S));
+    KS_CUDA(c, cudaMemsetAsync(c->ws_mem, 0, c->ws_bytes * S, c->stream));
     size_t off = 0;
     for (auto& pt : parts) {
         off = align_up(off, 256);
-        *pt.dst = (char*)s.mem + off;
+        *pt.dst = (char*)c->ws_mem + off;
         off += pt.bytes;
     }
+    KS_CUDA(c, cudaMalloc(&c->bq64, (size_t)S * 4 * kN * 8));
+    KS_CUDA(c, cudaMalloc(&c->bresp, (size_t)S * 2 * kN * 8));
+    KS_CUDA(c, cudaMalloc(&c->errs, (size_t)S * kErrStride * 4));
+    KS_CUDA(c, cudaMemsetAsync(c->errs, 0, (size_t)S * kErrStride * 4, c->stream));
+    KS_CUDA(c, cudaMalloc(&c->client_of, (size_t)S * 4));
+    KS_CUDA(c, cudaMemsetAsync(c->client_of, 0, (size_t)S * 4, c->stream));
+    KS_CUDA(c, cudaMalloc(&c->stage32, (size_t)r * 4 * P));
+    w.q64 = c->bq64;
+    w.resp64 = c->bresp;
+    w.err = c->errs;
 
     std::vector<NttJob> jobs;
     auto add = [&](const uint32_t* src, uint32_t* dst, int ch, int stride) {
         NttJob j; j.src = src; j.dst = dst; j.ch = ch; j.dst_stride = stride; jobs.push_back(j);
     };
     // query: dig0 (9), query b crt (2), modswitched query -> cipherbuf column 0 (4)
-    s.seg_q = (int)jobs.size();
+    c->seg_q = (int)jobs.size();
     for (int j = 0; j < 3; j++)
         for (int ch = 0; ch < 3; ch++) add(w.dig0 + (j * 3 + ch) * kN, w.dig0 + (j * 3 + ch) * kN, ch, 1);
     for (int ch = 0; ch < 2; ch++) add(w.qbn + ch * kN, w.qbn + ch * kN, ch, 1);
@@ -321,154 +413,232 @@ int init_workspace(kspir_ctx* c, WsSlot& s) {
     for (int comp = 0; comp < 2; comp++)
         for (int ch = 0; ch < 2; ch++)
             add(w.col0 + (comp * 2 + ch) * kN, cb32 + 2 * comp + ch, ch, 4 * N1);
-    s.n_q = (int)jobs.size() - s.seg_q;
-    s.seg_inter = (int)jobs.size();
+    c->n_q = (int)jobs.size() - c->seg_q;
+    c->seg_inter = (int)jobs.size();
     for (int ch = 0; ch < 2; ch++) add(w.interA + ch * kN, w.inter_acoef + ch * kN, ch, 1);
-    s.seg_dig1 = (int)jobs.size();
+    c->seg_dig1 = (int)jobs.size();
     for (int j = 0; j < 3; j++)
         for (int ch = 0; ch < 3; ch++) add(w.dig1 + (j * 3 + ch) * kN, w.dig1 + (j * 3 + ch) * kN, ch, 1);
-    KS_CUDA(c, cudaMalloc(&s.jobs, jobs.size() * sizeof(NttJob)));
-    KS_COPY(c, s.jobs, jobs.data(), jobs.size() * sizeof(NttJob), cudaMemcpyHostToDevice);
+    KS_CUDA(c, cudaMalloc(&c->jobs, jobs.size() * sizeof(NttJob)));
+    KS_COPY(c, c->jobs, jobs.data(), jobs.size() * sizeof(NttJob), cudaMemcpyHostToDevice);
+    return KSPIR_OK;
+}
+
+// Key slot layout (u32 residue words) and the single allocation of all slots.
+int init_key_slots(kspir_ctx* c) {
+    const size_t P = (size_t)kN;
+    const size_t nb_poly = (size_t)c->N1h * 3 * 2;
+    const size_t ng_poly = (size_t)std::max(0, c->N2 - 1) * 2 * 2;
+    const size_t np_poly = (size_t)c->levels * 4 * 2;
+    const size_t nr_poly = 4 * 2;
+    const size_t n_baby_crt = nb_poly * 2 * P, n_baby_bs = nb_poly * P;
+    const size_t n_giant = ng_poly * 2 * P, n_pack = np_poly * 2 * P, n_rgsw = nr_poly * 2 * P;
+    const size_t words = n_baby_crt + n_baby_bs + n_giant + n_pack + n_rgsw;
+    c->key_bytes = align_up(words * 4, 4096);
+    KS_CUDA(c, cudaMalloc(&c->key_mem, c->key_bytes * c->p.max_clients));
+    uint32_t* base = c->key_mem;
+    c->keys0.baby_crt = base; base += n_baby_crt;
+    c->keys0.baby_bs = base; base += n_baby_bs;
+    c->keys0.giant = base; base += n_giant;
+    c->keys0.packing = base; base += n_pack;
+    c->keys0.rgsw = base;
+    c->key_loaded.assign(c->p.max_clients, 0);
     return KSPIR_OK;
 }
 
 inline int blocks_for(long n, int t) { return (int)((n + t - 1) / t); }
 
 // ---------------------------------------------------------------------------
-// launch sequence
+// launch sequence of `nq` queries in workspace slots slot0 .. slot0 + nq - 1
+// (blockIdx.y of every kernel is the query)
 
 // baby steps -> cipherbuf (reference evalAutoSRNSSmallKeys + reorientCipher)
-void enqueue_baby(kspir_ctx* c, WsSlot& s, const ClientKeysDev& keys, cudaStream_t st) {
-    Workspace& w = s.ws;
-    k_query_prep<<<kN / 256, 256, 0, st>>>(w, c->gad.baby);
-    k_ntt_jobs<false><<<s.n_q, kNttThreads, kNttJobSmem, st>>>(s.jobs + s.seg_q, c->ntabs);
+void enqueue_baby(kspir_ctx* c, int slot0, int nq, cudaStream_t st) {
+    const Workspace& w = c->ws0;
+    const Batch bt = batch_of(c, slot0);
+    k_query_prep<<<dim3(kN / 256, nq), 256, 0, st>>>(w, c->gad.baby, bt);
+    k_ntt_jobs<false><<<dim3(c->n_q, nq), kNttThreads, kNttJobSmem, st>>>(c->jobs + c->seg_q, c->ntabs, bt);
     BabyArgs a1{};
     a1.dig = w.dig0; a1.srcB = w.qbn; a1.srcBbs = w.qbbs; a1.perms = c->perms; a1.sigma = c->sigma_baby;
     a1.cipherbuf = w.cipherbuf; a1.interA = w.interA; a1.interB = w.interB; a1.inter_bs = w.inter_bs;
     a1.N1 = c->N1; a1.col_base = 1; a1.inter_idx = c->N1h - 2;
-    if (c->N1h - 1 > 0) k_baby_rot<3><<<(c->N1h - 1) * 4, kNttThreads, kBabySmem, st>>>(a1, keys, c->ntabs);
-    k_ntt_jobs<true><<<2, kNttThreads, kNttJobSmem, st>>>(s.jobs + s.seg_inter, c->ntabs);
-    k_inter_decomp<<<kN / 256, 256, 0, st>>>(w, c->gad.baby);
-    k_ntt_jobs<false><<<9, kNttThreads, kNttJobSmem, st>>>(s.jobs + s.seg_dig1, c->ntabs);
+    if (c->N1h - 1 > 0)
+        k_baby_rot<3><<<dim3((c->N1h - 1) * 4, nq), kNttThreads, kBabySmem, st>>>(a1, c->keys0, c->ntabs, bt);
+    k_ntt_jobs<true><<<dim3(2, nq), kNttThreads, kNttJobSmem, st>>>(c->jobs + c->seg_inter, c->ntabs, bt);
+    k_inter_decomp<<<dim3(kN / 256, nq), 256, 0, st>>>(w, c->gad.baby, bt);
+    k_ntt_jobs<false><<<dim3(9, nq), kNttThreads, kNttJobSmem, st>>>(c->jobs + c->seg_dig1, c->ntabs, bt);
     BabyArgs a2 = a1;
     a2.dig = w.dig1; a2.srcB = w.interB; a2.srcBbs = w.inter_bs + kN;
     a2.col_base = c->N1h; a2.inter_idx = -1;
-    k_baby_rot<3><<<c->N1h * 4, kNttThreads, kBabySmem, st>>>(a2, keys, c->ntabs);
+    k_baby_rot<3><<<dim3(c->N1h * 4, nq), kNttThreads, kBabySmem, st>>>(a2, c->keys0, c->ntabs, bt);
 }
 
-void enqueue_scan(kspir_ctx* c, WsSlot& s, cudaStream_t st) {
-    Workspace& w = s.ws;
+int scan_kind_for(kspir_ctx* c, int nq) {
+    if (!c->mma) return SCAN_CUDA;
+    auto it = c->scan_choice.find(nq);
+    if (it != c->scan_choice.end()) return it->second;
+    if (nq == 1) return SCAN_CUDA;
+    return nq >= 16 ? SCAN_MMA16 : nq >= 8 ? SCAN_MMA8 : SCAN_MMA4;
+}
+
+long scan_launches(const kspir_ctx* c, int kind, int nq) { return kind == SCAN_CUDA ? nq : 2; }
+
+template <int BT>
+void launch_scan_mma(kspir_ctx* c, int slot0, int nq, cudaStream_t st) {
+    using C = MmaCfg<BT>;
+    const int QT = (nq + BT - 1) / BT;
+    k_qop_split<BT><<<blocks_for((long)kN * QT * 2 * BT * 8, 256), 256, 0, st>>>(c->ws0.cipherbuf, c->ws_bytes, slot0,
+                                                                                  nq, QT, c->qop);
+    ScanMmaArgs a;
+    a.dbop = c->dbop;
+    a.qop = c->qop;
+    a.sout0 = c->ws0.sout;
+    a.ws_bytes = c->ws_bytes;
+    a.slot0 = slot0;
+    a.nq = nq;
+    a.QT = QT;
+    a.G = c->G;
+    a.rows = c->p.r * c->N2;
+    a.err = c->errs + (size_t)slot0 * kErrStride;
+    const int units = (kN / C::ZB) * 2 * QT;
+    k_scan_mma<BT><<<std::min(c->nsm, units), C::THREADS, C::SMEM, st>>>(a);
+}
+
+void enqueue_scan(kspir_ctx* c, int slot0, int nq, int kind, cudaStream_t st) {
     const int R = c->p.r;
-    switch (c->N1) {
-#define KS_SCAN(n) \
-    case n: k_scan<n><<<c->nsm, ScanCfg<n>::THREADS, ScanCfg<n>::SMEM, st>>>(c->db, w.cipherbuf, w.sout, R, w.err); break;
-        KS_SCAN(64) KS_SCAN(128) KS_SCAN(256)
+    if (kind == SCAN_CUDA) {
+        for (int q = 0; q < nq; q++) {
+            const Workspace w = ws_host(c, slot0 + q);
+            switch (c->N1) {
+#define KS_SCAN(n)                                                                                           \
+    case n:                                                                                                  \
+        k_scan<n><<<c->nsm, ScanCfg<n>::THREADS, ScanCfg<n>::SMEM, st>>>(c->db, w.cipherbuf, w.sout, R, w.err); \
+        break;
+                KS_SCAN(64) KS_SCAN(128) KS_SCAN(256)
 #undef KS_SCAN
+            }
+        }
+        return;
+    }
+    switch (scan_bt(kind)) {
+        case 4: launch_scan_mma<4>(c, slot0, nq, st); break;
+        case 8: launch_scan_mma<8>(c, slot0, nq, st); break;
+        case 16: launch_scan_mma<16>(c, slot0, nq, st); break;
+        default: launch_scan_mma<32>(c, slot0, nq, st); break;
     }
 }
 
-void enqueue_giant(kspir_ctx* c, WsSlot& s, const ClientKeysDev& keys, cudaStream_t st) {
-    Workspace& w = s.ws;
+void enqueue_giant(kspir_ctx* c, int slot0, int nq, cudaStream_t st) {
+    const Workspace& w = c->ws0;
+    const Batch bt = batch_of(c, slot0);
     const int R = c->p.r;
-    cudaMemsetAsync(w.gacc, 0, (size_t)R * 4 * kN * 8, st);
     if (c->N2 > 1)
-        k_giant_fused<2><<<R * (c->N2 - 1), kNttThreads, kGiantSmem, st>>>(w.sout, keys.giant, c->sigma_giant, w.gacc,
-                                                                          c->N1, c->ntabs, c->gad.giant);
-    k_giant_finish<<<blocks_for((long)R * 4 * kN, 256), 256, 0, st>>>(w.sout, w.gacc, w.result, R, c->N2);
+        k_giant_fused<2><<<dim3(R * (c->N2 - 1), nq), kNttThreads, kGiantSmem, st>>>(
+            w.sout, c->keys0.giant, c->sigma_giant, w.gacc, c->N1, c->ntabs, c->gad.giant, R, bt);
+    k_giant_finish<<<dim3(blocks_for((long)R * 4 * kN, 256), nq), 256, 0, st>>>(w.sout, w.gacc, w.result, R, c->N2, bt);
 }
 
 // external products of `count` first-dimension results (result -> ext);
-// `init` holds NTT-domain accumulators ([count][2][2][N]) or is null for zero;
-// coef_out (or null) receives the first-dimension results in coefficient form
-void enqueue_ext(kspir_ctx* c, WsSlot& s, const ClientKeysDev& keys, int count, const uint32_t* init,
-                 uint32_t* coef_out, cudaStream_t st) {
-    Workspace& w = s.ws;
-    k_ext_fused<2><<<count * 2, kNttThreads, kExtSmem, st>>>(w.result, keys.rgsw, init, w.ext, coef_out, c->ntabs,
-                                                              c->gad.ext);
+// `init` holds NTT-domain accumulators ([count][2][2][N], slot-0 workspace
+// address) or is null for zero; coef_out (or null) receives the
+// first-dimension results in coefficient form
+void enqueue_ext(kspir_ctx* c, int slot0, int nq, int count, const uint32_t* init, uint32_t* coef_out,
+                 cudaStream_t st) {
+    const Workspace& w = c->ws0;
+    k_ext_fused<2><<<dim3(count * 2, nq), kNttThreads, kExtSmem, st>>>(w.result, c->keys0.rgsw, init, w.ext, coef_out,
+                                                                        c->ntabs, c->gad.ext, batch_of(c, slot0));
 }
 
-void enqueue_packing(kspir_ctx* c, WsSlot& s, const ClientKeysDev& keys, cudaStream_t st) {
-    Workspace& w = s.ws;
+void enqueue_packing(kspir_ctx* c, int slot0, int nq, cudaStream_t st) {
+    const Workspace& w = c->ws0;
+    const Batch bt = batch_of(c, slot0);
     const int pe = c->gad.pack.ell;
     const uint32_t* cur = w.ext;
     for (int lv = c->levels - 1; lv >= 0; lv--) {
         const int I = 1 << lv;
         const uint32_t ginv = inv_mod_2n((uint32_t)(kN / I + 1));
         uint32_t* out = (cur == w.ext) ? w.ext2 : w.ext;
-        k_pack_fused<4><<<I * 2, kNttThreads, kPackSmem, st>>>(cur, out, keys.packing + (size_t)lv * pe * 4 * kN, I,
-                                                               ginv, c->ntabs, c->gad.pack);
+        k_pack_fused<4><<<dim3(I * 2, nq), kNttThreads, kPackSmem, st>>>(
+            cur, out, c->keys0.packing + (size_t)lv * pe * 4 * kN, I, ginv, c->ntabs, c->gad.pack, bt);
         cur = out;
     }
-    k_compose_words<<<2 * kN / 256, 256, 0, st>>>(cur, w.resp64, 2);
+    k_compose_resp<<<dim3(2 * kN / 256, nq), 256, 0, st>>>(cur, w, bt);
 }
 
 // kernels launched by one enqueue_answer
-long answer_launches(const kspir_ctx* c) {
-    // baby 7, scan 1, giant 2, external product 1, packing one per level + compose
-    return 7 + 1 + (c->N2 > 1 ? 2 : 1) + 1 + c->levels + 1;
+long answer_launches(const kspir_ctx* c, int kind, int nq) {
+    // clients 1, baby 7, scan, giant 2, external product 1, packing one per level + compose
+    return 1 + 7 + scan_launches(c, kind, nq) + (c->N2 > 1 ? 2 : 1) + 1 + c->levels + 1;
 }
 
-// Captures the four non-scan phases of one (workspace, client) pair as CUDA
-// graphs (the scan stays a direct launch so its duration is bracketed by the
-// per-answer events).  Pointers are fixed for the context's lifetime, so the
-// graphs stay valid when keys or the database are re-uploaded.
-int build_graphs(kspir_ctx* c, int wsi, int client) {
-    auto& pg = c->graphs[(size_t)wsi * c->p.max_clients + client];
-    if (pg.ready) return KSPIR_OK;
-    WsSlot& s = c->ws[wsi];
-    const ClientKeysDev keys = c->clients[client].keys;
+// Captures the four non-scan phases of (slot0, nq) as CUDA graphs (the scan
+// stays a direct launch so its duration is bracketed by the per-launch
+// events).  Pointers are fixed for the context's lifetime and the key slot of
+// each query is read from client_of at run time, so the graphs stay valid for
+// any clients and across key or database uploads.
+int build_graphs(kspir_ctx* c, int slot0, int nq, kspir_ctx::PhaseGraphs** out) {
+    auto key = std::make_pair(slot0, nq);
+    auto it = c->graphs.find(key);
+    if (it != c->graphs.end()) { *out = &it->second; return KSPIR_OK; }
+    kspir_ctx::PhaseGraphs pg;
     cudaStream_t cs = c->capture;
     for (int ph = 0; ph < 4; ph++) {
         cudaGraph_t g = nullptr;
         KS_CUDA(c, cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-        if (ph == 0) enqueue_baby(c, s, keys, cs);
-        else if (ph == 1) enqueue_giant(c, s, keys, cs);
-        else if (ph == 2) enqueue_ext(c, s, keys, c->p.r, nullptr, nullptr, cs);
-        else enqueue_packing(c, s, keys, cs);
+        if (ph == 0) enqueue_baby(c, slot0, nq, cs);
+        else if (ph == 1) enqueue_giant(c, slot0, nq, cs);
+        else if (ph == 2) enqueue_ext(c, slot0, nq, c->p.r, nullptr, nullptr, cs);
+        else enqueue_packing(c, slot0, nq, cs);
         KS_CUDA(c, cudaStreamEndCapture(cs, &g));
         cudaError_t e = cudaGraphInstantiate(&pg.g[ph], g, 0);
         cudaGraphDestroy(g);
         if (e != cudaSuccess) return set_err(c, KSPIR_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
     }
-    pg.ready = true;
+    auto res = c->graphs.emplace(key, pg);
+    *out = &res.first->second;
     return KSPIR_OK;
 }
 
-int enqueue_answer(kspir_ctx* c, int wsi, int client, cudaStream_t st) {
-    WsSlot& s = c->ws[wsi];
-    const ClientKeysDev& keys = c->clients[client].keys;
-    const int slot = (int)(c->answers % kTimingRing);
+int enqueue_answer(kspir_ctx* c, int slot0, int nq, const int* clients, cudaStream_t st) {
+    ClientList cl;
+    cl.n = nq;
+    for (int i = 0; i < nq; i++) cl.id[i] = clients[i];
+    k_set_clients<<<1, kMaxBatch, 0, st>>>(c->client_of, slot0, cl);
+    const int kind = scan_kind_for(c, nq);
+    const int slot = (int)(c->enqueues % kTimingRing);
     auto& ev = c->ring[slot];
     if (c->use_graphs) {
-        int rc = build_graphs(c, wsi, client);
+        kspir_ctx::PhaseGraphs* pg = nullptr;
+        int rc = build_graphs(c, slot0, nq, &pg);
         if (rc) return rc;
-        auto& pg = c->graphs[(size_t)wsi * c->p.max_clients + client];
         cudaEventRecord(ev[0], st);
-        KS_CUDA(c, cudaGraphLaunch(pg.g[0], st));
+        KS_CUDA(c, cudaGraphLaunch(pg->g[0], st));
         cudaEventRecord(ev[1], st);
-        enqueue_scan(c, s, st);
+        enqueue_scan(c, slot0, nq, kind, st);
         cudaEventRecord(ev[2], st);
-        KS_CUDA(c, cudaGraphLaunch(pg.g[1], st));
+        KS_CUDA(c, cudaGraphLaunch(pg->g[1], st));
         cudaEventRecord(ev[3], st);
-        KS_CUDA(c, cudaGraphLaunch(pg.g[2], st));
+        KS_CUDA(c, cudaGraphLaunch(pg->g[2], st));
         cudaEventRecord(ev[4], st);
-        KS_CUDA(c, cudaGraphLaunch(pg.g[3], st));
+        KS_CUDA(c, cudaGraphLaunch(pg->g[3], st));
         cudaEventRecord(ev[5], st);
     } else {
         cudaEventRecord(ev[0], st);
-        enqueue_baby(c, s, keys, st);
+        enqueue_baby(c, slot0, nq, st);
         cudaEventRecord(ev[1], st);
-        enqueue_scan(c, s, st);
+        enqueue_scan(c, slot0, nq, kind, st);
         cudaEventRecord(ev[2], st);
-        enqueue_giant(c, s, keys, st);
+        enqueue_giant(c, slot0, nq, st);
         cudaEventRecord(ev[3], st);
-        enqueue_ext(c, s, keys, c->p.r, nullptr, nullptr, st);
+        enqueue_ext(c, slot0, nq, c->p.r, nullptr, nullptr, st);
         cudaEventRecord(ev[4], st);
-        enqueue_packing(c, s, keys, st);
+        enqueue_packing(c, slot0, nq, st);
         cudaEventRecord(ev[5], st);
     }
-    c->answers++;
-    c->launches += answer_launches(c);
+    c->ring_nq[slot] = nq;
+    c->enqueues++;
+    c->answers += nq;
+    c->launches += answer_launches(c, kind, nq);
     c->last_slot = slot;
     return KSPIR_OK;
 }
@@ -479,24 +649,59 @@ bool canonical(const uint64_t* w, size_t n, uint64_t q) {
     return true;
 }
 
-int check_ready(kspir_ctx* c, int client) {
+int check_base(kspir_ctx* c) {
     if (!c) return KSPIR_ERR_INVALID_ARG;
-    if (client < 0 || client >= (int)c->clients.size()) return set_err(c, KSPIR_ERR_INVALID_ARG, "client slot out of range");
     if (!c->db_loaded) return set_err(c, KSPIR_ERR_NOT_READY, "database not uploaded");
     if (!c->perms_loaded) return set_err(c, KSPIR_ERR_NOT_READY, "permutations not uploaded");
-    if (!c->clients[client].loaded) return set_err(c, KSPIR_ERR_NOT_READY, "client keys not uploaded");
     return KSPIR_OK;
 }
 
-int finish(kspir_ctx* c, WsSlot& s) {
+int check_client(kspir_ctx* c, int client) {
+    if (client < 0 || client >= c->p.max_clients) return set_err(c, KSPIR_ERR_INVALID_ARG, "client slot out of range");
+    if (!c->key_loaded[client]) return set_err(c, KSPIR_ERR_NOT_READY, "client keys not uploaded");
+    return KSPIR_OK;
+}
+
+int check_ready(kspir_ctx* c, int client) {
+    int rc = check_base(c);
+    return rc ? rc : check_client(c, client);
+}
+
+// Waits for the context stream and reports (then clears) the error words of
+// slots [slot0, slot0 + nq).  After a timed-out launch the giant-step
+// accumulators of those slots are cleared too (a partial launch leaves them
+// dirty).
+int finish(kspir_ctx* c, int slot0, int nq) {
     KS_CUDA(c, cudaStreamSynchronize(c->stream));
+    std::vector<int> e((size_t)nq * kErrStride);
+    KS_COPY(c, e.data(), c->errs + (size_t)slot0 * kErrStride, e.size() * 4, cudaMemcpyDeviceToHost);
     int herr = 0;
-    KS_COPY(c, &herr, s.ws.err, sizeof(int), cudaMemcpyDeviceToHost);
+    for (int q = 0; q < nq; q++) herr |= e[(size_t)q * kErrStride];
     if (herr) {
-        cudaMemsetAsync(s.ws.err, 0, sizeof(int), c->stream);
+        cudaMemsetAsync(c->errs + (size_t)slot0 * kErrStride, 0, e.size() * 4, c->stream);
+        for (int q = 0; q < nq; q++)
+            cudaMemsetAsync(ws_host(c, slot0 + q).gacc, 0, (size_t)c->p.r * 4 * kN * 8, c->stream);
         cudaStreamSynchronize(c->stream);
         return set_err(c, KSPIR_ERR_TIMEOUT, "a bounded device wait gave up (code " + std::to_string(herr) + ")");
     }
+    return KSPIR_OK;
+}
+
+// the tensor-core database operand, rebuilt from the resident database
+int build_dbop(kspir_ctx* c) {
+    if (!c->mma) return KSPIR_OK;
+    const size_t bytes = (size_t)kN * 2 * c->G * kATile;
+    if (!c->dbop) KS_CUDA(c, cudaMalloc(&c->dbop, bytes));
+    k_dbop_build<<<blocks_for((long)kN * 2 * c->G * 128 * 8, 256), 256, 0, c->stream>>>(c->db, c->dbop, c->p.r, c->N2,
+                                                                                        c->G);
+    KS_CUDA(c, cudaGetLastError());
+    KS_CUDA(c, cudaStreamSynchronize(c->stream));
+    return KSPIR_OK;
+}
+
+template <int BT>
+int mma_attr(kspir_ctx* c) {
+    KS_CUDA(c, cudaFuncSetAttribute(k_scan_mma<BT>, cudaFuncAttributeMaxDynamicSharedMemorySize, MmaCfg<BT>::SMEM));
     return KSPIR_OK;
 }
 
@@ -527,8 +732,8 @@ int kspir_ctx_create(int device, const kspir_params* params, kspir_ctx** out) {
     const kspir_params p = *params;
     auto pow2 = [](int v) { return v > 0 && (v & (v - 1)) == 0; };
     if (!pow2(p.r) || p.r > 512 || !pow2(p.N1) || p.N1 < 64 || p.N1 > 256 || p.max_clients < 1 ||
-        p.max_inflight < 1)
-        return KSPIR_ERR_INVALID_ARG;
+        p.max_inflight < 1 || p.max_inflight > 4096)
+        return set_err(nullptr, KSPIR_ERR_INVALID_ARG, "invalid parameters");
     std::unique_ptr<kspir_ctx> c(new kspir_ctx());
     c->device = device;
     c->p = p;
@@ -536,6 +741,8 @@ int kspir_ctx_create(int device, const kspir_params* params, kspir_ctx** out) {
     c->N1h = p.N1 / 2;
     c->N2 = kN / 2 / p.N1;
     c->levels = ilog2i(p.r);
+    c->mma = (p.N1 == kMmaK && p.max_inflight >= 2);
+    c->G = (p.r * c->N2 + 31) / 32;
     KS_CUDA(c.get(), cudaSetDevice(device));
     KS_CUDA(c.get(), cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     KS_CUDA(c.get(), cudaStreamCreateWithFlags(&c->capture, cudaStreamNonBlocking));
@@ -548,19 +755,28 @@ int kspir_ctx_create(int device, const kspir_params* params, kspir_ctx** out) {
     KS_CUDA(c.get(), cudaFuncSetAttribute(k_scan<n>, cudaFuncAttributeMaxDynamicSharedMemorySize, ScanCfg<n>::SMEM));
     KS_ATTR(64) KS_ATTR(128) KS_ATTR(256)
 #undef KS_ATTR
-    int rc = init_constants(c.get());
+    int rc = KSPIR_OK;
+    if (c->mma) {
+        if (!rc) rc = mma_attr<4>(c.get());
+        if (!rc) rc = mma_attr<8>(c.get());
+        if (!rc) rc = mma_attr<16>(c.get());
+        if (!rc) rc = mma_attr<32>(c.get());
+        if (rc) return rc;
+        const size_t qslots = align_up((size_t)p.max_inflight, 32);
+        KS_CUDA(c.get(), cudaMalloc(&c->qop, (size_t)kN * 2 * qslots * 8 * kMmaK));
+    }
+    rc = init_constants(c.get());
     if (rc) return rc;
     KS_CUDA(c.get(), cudaMalloc(&c->perms, (size_t)p.N1 * kN * 4));
     c->ring.resize(kTimingRing);
+    c->ring_nq.assign(kTimingRing, 0);
     for (auto& evs : c->ring)
         for (auto& e : evs) KS_CUDA(c.get(), cudaEventCreate(&e));
-    c->clients.resize(p.max_clients);
-    c->ws.resize(p.max_inflight);
-    c->graphs.resize((size_t)p.max_inflight * p.max_clients);
-    for (auto& s : c->ws) {
-        rc = init_workspace(c.get(), s);
-        if (rc) return rc;
-    }
+    rc = init_key_slots(c.get());
+    if (rc) return rc;
+    rc = init_workspaces(c.get());
+    if (rc) return rc;
+    KS_CUDA(c.get(), cudaStreamSynchronize(c->stream));
     *out = c.release();
     return KSPIR_OK;
 }
@@ -569,17 +785,22 @@ int kspir_ctx_destroy(kspir_ctx* c) {
     if (!c) return KSPIR_ERR_INVALID_ARG;
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
-    for (auto& s : c->ws) {
-        cudaFree(s.mem);
-        cudaFree(s.jobs);
-    }
     for (auto& evs : c->ring)
         for (auto& e : evs) if (e) cudaEventDestroy(e);
-    for (auto& pg : c->graphs)
-        for (auto& g : pg.g) if (g) cudaGraphExecDestroy(g);
+    for (auto& kv : c->graphs)
+        for (auto& g : kv.second.g) if (g) cudaGraphExecDestroy(g);
     if (c->capture) cudaStreamDestroy(c->capture);
-    for (auto& cl : c->clients) cudaFree(cl.mem);
+    cudaFree(c->ws_mem);
+    cudaFree(c->jobs);
+    cudaFree(c->bq64);
+    cudaFree(c->bresp);
+    cudaFree(c->errs);
+    cudaFree(c->client_of);
+    cudaFree(c->stage32);
+    cudaFree(c->key_mem);
     cudaFree(c->db);
+    cudaFree(c->dbop);
+    cudaFree(c->qop);
     cudaFree(c->perms);
     cudaFree(c->tw);
     cudaFree(c->sigma_baby);
@@ -593,9 +814,12 @@ int kspir_db_upload(kspir_ctx* c, const uint64_t* datacrt, size_t words) {
     if (!c || !datacrt) return KSPIR_ERR_INVALID_ARG;
     const size_t need = (size_t)c->p.r * kN * (kN / 2);
     if (words != need) return set_err(c, KSPIR_ERR_INVALID_ARG, "database size must be r*N*N/2 words");
+    std::lock_guard<std::mutex> lk(c->mu);
     KS_CUDA(c, cudaSetDevice(c->device));
     if (!c->db) KS_CUDA(c, cudaMalloc(&c->db, need * 8));
     KS_COPY(c, c->db, datacrt, need * 8, cudaMemcpyHostToDevice);
+    int rc = build_dbop(c);
+    if (rc) return rc;
     c->db_loaded = true;
     return KSPIR_OK;
 }
@@ -605,6 +829,7 @@ int kspir_perms_upload(kspir_ctx* c, const int32_t* perms, size_t count) {
     if (count != (size_t)c->N1 * kN) return set_err(c, KSPIR_ERR_INVALID_ARG, "permutations must be N1*N entries");
     for (size_t i = 0; i < count; i++)
         if (perms[i] < 0 || perms[i] >= kN) return set_err(c, KSPIR_ERR_INVALID_ARG, "permutation entry out of range");
+    std::lock_guard<std::mutex> lk(c->mu);
     KS_CUDA(c, cudaSetDevice(c->device));
     KS_COPY(c, c->perms, perms, count * 4, cudaMemcpyHostToDevice);
     c->perms_loaded = true;
@@ -613,9 +838,10 @@ int kspir_perms_upload(kspir_ctx* c, const int32_t* perms, size_t count) {
 
 int kspir_client_keys_upload(kspir_ctx* c, int client, const uint64_t* baby, const uint64_t* giant,
                              const uint64_t* packing, const uint64_t* rgsw) {
-    if (!c || client < 0 || client >= (int)c->clients.size() || !baby || !rgsw) return KSPIR_ERR_INVALID_ARG;
+    if (!c || client < 0 || client >= c->p.max_clients || !baby || !rgsw) return KSPIR_ERR_INVALID_ARG;
     if (c->N2 > 1 && !giant) return KSPIR_ERR_INVALID_ARG;
     if (c->levels > 0 && !packing) return KSPIR_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(c->mu);
     KS_CUDA(c, cudaSetDevice(c->device));
     const size_t nb_poly = (size_t)c->N1h * 3 * 2;                 // crt rows and bs rows each
     const size_t ng_poly = (size_t)(c->N2 - 1) * 2 * 2;
@@ -636,42 +862,31 @@ int kspir_client_keys_upload(kspir_ctx* c, int client, const uint64_t* baby, con
         !canonical(rgsw, nr_poly * kN, kCrtMod))
         return set_err(c, KSPIR_ERR_INVALID_ARG, "key word not canonical");
 
-    ClientSlot& cl = c->clients[client];
-    const size_t P = (size_t)kN;   // u32 words per residue poly
-    const size_t n_baby_crt = nb_poly * 2 * P, n_baby_bs = nb_poly * P;
-    const size_t n_giant = ng_poly * 2 * P, n_pack = np_poly * 2 * P, n_rgsw = nr_poly * 2 * P;
-    const size_t total = n_baby_crt + n_baby_bs + n_giant + n_pack + n_rgsw;
-    if (!cl.mem) KS_CUDA(c, cudaMalloc(&cl.mem, total * 4));
-    uint32_t* base = cl.mem;
-    cl.keys.baby_crt = base; base += n_baby_crt;
-    cl.keys.baby_bs = base; base += n_baby_bs;
-    cl.keys.giant = base; base += n_giant;
-    cl.keys.packing = base; base += n_pack;
-    cl.keys.rgsw = base;
-
+    const ClientKeysDev keys = keys_host(c, client);
     const size_t stage_words = std::max({nb_poly, ng_poly, np_poly, nr_poly}) * kN;
     uint64_t* stage = nullptr;
     KS_CUDA(c, cudaMalloc(&stage, stage_words * 8));
-    auto split = [&](const uint64_t* h, size_t polys, uint32_t* dst) -> int {
+    auto split = [&](const uint64_t* h, size_t polys, const uint32_t* dst) -> int {
         if (!polys) return KSPIR_OK;
         KS_COPY(c, stage, h, polys * kN * 8, cudaMemcpyHostToDevice);
-        k_split_words<<<blocks_for((long)polys * kN, 256), 256, 0, c->stream>>>(stage, dst, (int)polys);
+        k_split_words<<<blocks_for((long)polys * kN, 256), 256, 0, c->stream>>>(stage, const_cast<uint32_t*>(dst),
+                                                                              (int)polys);
         KS_CUDA(c, cudaStreamSynchronize(c->stream));
         return KSPIR_OK;
     };
-    int rc = split(crt_rows.data(), nb_poly, const_cast<uint32_t*>(cl.keys.baby_crt));
-    if (!rc) rc = split(giant, ng_poly, const_cast<uint32_t*>(cl.keys.giant));
-    if (!rc) rc = split(packing, np_poly, const_cast<uint32_t*>(cl.keys.packing));
-    if (!rc) rc = split(rgsw, nr_poly, const_cast<uint32_t*>(cl.keys.rgsw));
+    c->key_loaded[client] = 0;
+    int rc = split(crt_rows.data(), nb_poly, keys.baby_crt);
+    if (!rc) rc = split(giant, ng_poly, keys.giant);
+    if (!rc) rc = split(packing, np_poly, keys.packing);
+    if (!rc) rc = split(rgsw, nr_poly, keys.rgsw);
     if (!rc) {
         std::vector<uint32_t> bs32(bs_rows.size());
         for (size_t i = 0; i < bs_rows.size(); i++) bs32[i] = (uint32_t)bs_rows[i];
-        rc = copy_sync(c, const_cast<uint32_t*>(cl.keys.baby_bs), bs32.data(), bs32.size() * 4,
-                       cudaMemcpyHostToDevice);
+        rc = copy_sync(c, const_cast<uint32_t*>(keys.baby_bs), bs32.data(), bs32.size() * 4, cudaMemcpyHostToDevice);
     }
     cudaFree(stage);
     if (rc) return rc;
-    cl.loaded = true;
+    c->key_loaded[client] = 1;
     return KSPIR_OK;
 }
 
@@ -679,13 +894,13 @@ int kspir_answer_device(kspir_ctx* c, int client, const uint64_t* d_query, uint6
     int rc = check_ready(c, client);
     if (rc) return rc;
     if (!d_query || !d_response) return KSPIR_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(c->mu);
     cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
-    WsSlot& s = c->ws[0];
     KS_CUDA(c, cudaSetDevice(c->device));
-    KS_CUDA(c, cudaMemcpyAsync(s.ws.q64, d_query, 4 * kN * 8, cudaMemcpyDeviceToDevice, st));
-    rc = enqueue_answer(c, 0, client, st);
+    KS_CUDA(c, cudaMemcpyAsync(c->bq64, d_query, 4 * kN * 8, cudaMemcpyDeviceToDevice, st));
+    rc = enqueue_answer(c, 0, 1, &client, st);
     if (rc) return rc;
-    KS_CUDA(c, cudaMemcpyAsync(d_response, s.ws.resp64, 2 * kN * 8, cudaMemcpyDeviceToDevice, st));
+    KS_CUDA(c, cudaMemcpyAsync(d_response, c->bresp, 2 * kN * 8, cudaMemcpyDeviceToDevice, st));
     KS_CUDA(c, cudaGetLastError());
     return KSPIR_OK;
 }
@@ -693,7 +908,7 @@ int kspir_answer_device(kspir_ctx* c, int client, const uint64_t* d_query, uint6
 int kspir_sync(kspir_ctx* c) {
     if (!c) return KSPIR_ERR_INVALID_ARG;
     KS_CUDA(c, cudaDeviceSynchronize());
-    return finish(c, c->ws[0]);
+    return finish(c, 0, c->p.max_inflight);
 }
 
 int kspir_answer(kspir_ctx* c, int client, const uint64_t* query, uint64_t* response) {
@@ -702,15 +917,102 @@ int kspir_answer(kspir_ctx* c, int client, const uint64_t* query, uint64_t* resp
     if (!query || !response) return KSPIR_ERR_INVALID_ARG;
     if (!canonical(query, 2 * kN, kCrtMod) || !canonical(query + 2 * kN, 2 * kN, kBsMod))
         return set_err(c, KSPIR_ERR_INVALID_ARG, "query word not canonical");
-    WsSlot& s = c->ws[0];
+    std::lock_guard<std::mutex> lk(c->mu);
     KS_CUDA(c, cudaSetDevice(c->device));
-    KS_CUDA(c, cudaMemcpyAsync(s.ws.q64, query, 4 * kN * 8, cudaMemcpyHostToDevice, c->stream));
-    rc = enqueue_answer(c, 0, client, c->stream);
+    KS_CUDA(c, cudaMemcpyAsync(c->bq64, query, 4 * kN * 8, cudaMemcpyHostToDevice, c->stream));
+    rc = enqueue_answer(c, 0, 1, &client, c->stream);
     if (rc) return rc;
     KS_CUDA(c, cudaGetLastError());
-    KS_CUDA(c, cudaMemcpyAsync(response, s.ws.resp64, 2 * kN * 8, cudaMemcpyDeviceToHost, c->stream));
-    return finish(c, s);
+    KS_CUDA(c, cudaMemcpyAsync(response, c->bresp, 2 * kN * 8, cudaMemcpyDeviceToHost, c->stream));
+    return finish(c, 0, 1);
 }
+
+int kspir_answer_batch_device(kspir_ctx* c, int n, const int32_t* clients, const uint64_t* d_queries,
+                              uint64_t* d_responses, void* stream) {
+    int rc = check_base(c);
+    if (rc) return rc;
+    if (n < 1 || n > c->p.max_inflight || n > kMaxBatch || !clients || !d_queries || !d_responses)
+        return set_err(c, KSPIR_ERR_INVALID_ARG, "batch size out of range or null pointer");
+    for (int i = 0; i < n; i++)
+        if ((rc = check_client(c, clients[i]))) return rc;
+    std::lock_guard<std::mutex> lk(c->mu);
+    cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+    KS_CUDA(c, cudaSetDevice(c->device));
+    KS_CUDA(c, cudaMemcpyAsync(c->bq64, d_queries, (size_t)n * 4 * kN * 8, cudaMemcpyDeviceToDevice, st));
+    rc = enqueue_answer(c, 0, n, clients, st);
+    if (rc) return rc;
+    KS_CUDA(c, cudaMemcpyAsync(d_responses, c->bresp, (size_t)n * 2 * kN * 8, cudaMemcpyDeviceToDevice, st));
+    KS_CUDA(c, cudaGetLastError());
+    return KSPIR_OK;
+}
+
+int kspir_answer_batch(kspir_ctx* c, int n, const int32_t* clients, const uint64_t* queries, uint64_t* responses) {
+    int rc = check_base(c);
+    if (rc) return rc;
+    if (n < 1 || n > c->p.max_inflight || n > kMaxBatch || !clients || !queries || !responses)
+        return set_err(c, KSPIR_ERR_INVALID_ARG, "batch size out of range or null pointer");
+    for (int i = 0; i < n; i++) {
+        if ((rc = check_client(c, clients[i]))) return rc;
+        const uint64_t* q = queries + (size_t)i * 4 * kN;
+        if (!canonical(q, 2 * kN, kCrtMod) || !canonical(q + 2 * kN, 2 * kN, kBsMod))
+            return set_err(c, KSPIR_ERR_INVALID_ARG, "query word not canonical");
+    }
+    std::lock_guard<std::mutex> lk(c->mu);
+    KS_CUDA(c, cudaSetDevice(c->device));
+    KS_CUDA(c, cudaMemcpyAsync(c->bq64, queries, (size_t)n * 4 * kN * 8, cudaMemcpyHostToDevice, c->stream));
+    rc = enqueue_answer(c, 0, n, clients, c->stream);
+    if (rc) return rc;
+    KS_CUDA(c, cudaGetLastError());
+    KS_CUDA(c, cudaMemcpyAsync(responses, c->bresp, (size_t)n * 2 * kN * 8, cudaMemcpyDeviceToHost, c->stream));
+    return finish(c, 0, n);
+}
+
+int kspir_tune_batch(kspir_ctx* c, int n, int* kind_out, float* ms_out) {
+    int rc = check_base(c);
+    if (rc) return rc;
+    if (n < 1 || n > c->p.max_inflight || n > kMaxBatch) return set_err(c, KSPIR_ERR_INVALID_ARG, "batch size");
+    std::lock_guard<std::mutex> lk(c->mu);
+    KS_CUDA(c, cudaSetDevice(c->device));
+    cudaEvent_t e0, e1;
+    KS_CUDA(c, cudaEventCreate(&e0));
+    KS_CUDA(c, cudaEventCreate(&e1));
+    int best = SCAN_CUDA;
+    float best_ms = 1e30f;
+    for (int kind = 0; kind < SCAN_KINDS; kind++) {
+        if (kind != SCAN_CUDA && !c->mma) continue;
+        if (kind != SCAN_CUDA && scan_bt(kind) > 4 && (n + 3) / 4 * 4 < scan_bt(kind) / 2) continue;   // mostly padding
+        float ms_min = 1e30f;
+        for (int rep = 0; rep < 4; rep++) {
+            cudaEventRecord(e0, c->stream);
+            enqueue_scan(c, 0, n, kind, c->stream);
+            cudaEventRecord(e1, c->stream);
+            KS_CUDA(c, cudaEventSynchronize(e1));
+            float ms = 0;
+            KS_CUDA(c, cudaEventElapsedTime(&ms, e0, e1));
+            if (rep > 0) ms_min = std::min(ms_min, ms);   // first run warms up
+        }
+        if (ms_min < best_ms) { best_ms = ms_min; best = kind; }
+        if (ms_out) ms_out[kind] = ms_min;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    rc = finish(c, 0, n);
+    if (rc) return rc;
+    c->scan_choice[n] = best;
+    if (kind_out) *kind_out = best;
+    return KSPIR_OK;
+}
+
+int kspir_set_scan_kind(kspir_ctx* c, int n, int kind) {
+    if (!c || n < 1 || kind < -1 || kind >= SCAN_KINDS) return KSPIR_ERR_INVALID_ARG;
+    if (kind > SCAN_CUDA && !c->mma) return set_err(c, KSPIR_ERR_INVALID_ARG, "tensor-core scan not enabled");
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (kind < 0) c->scan_choice.erase(n);
+    else c->scan_choice[n] = kind;
+    return KSPIR_OK;
+}
+
+int kspir_get_scan_kind(kspir_ctx* c, int n) { return c ? scan_kind_for(c, n) : KSPIR_ERR_INVALID_ARG; }
 
 int kspir_last_timing(kspir_ctx* c, float* total_ms, float* phase_ms) {
     if (!c || c->last_slot < 0) return KSPIR_ERR_NOT_READY;
@@ -726,6 +1028,7 @@ int kspir_last_timing(kspir_ctx* c, float* total_ms, float* phase_ms) {
 
 int kspir_timing_reset(kspir_ctx* c) {
     if (!c) return KSPIR_ERR_INVALID_ARG;
+    c->enqueues = 0;
     c->answers = 0;
     c->launches = 0;
     c->last_slot = -1;
@@ -734,20 +1037,22 @@ int kspir_timing_reset(kspir_ctx* c) {
 
 int kspir_timing_summary(kspir_ctx* c, int* answers, long* launches, float* total_ms, float* phase_ms) {
     if (!c) return KSPIR_ERR_INVALID_ARG;
-    const int n = (int)std::min<long>(c->answers, kTimingRing);
+    const int n = (int)std::min<long>(c->enqueues, kTimingRing);
     float tot = 0, ph[5] = {0, 0, 0, 0, 0};
+    int queries = 0;
     for (int k = 0; k < n; k++) {
         auto& ev = c->ring[k];
         KS_CUDA(c, cudaEventSynchronize(ev[5]));
         float t = 0;
         KS_CUDA(c, cudaEventElapsedTime(&t, ev[0], ev[5]));
         tot += t;
+        queries += c->ring_nq[k];
         for (int i = 0; i < 5; i++) {
             KS_CUDA(c, cudaEventElapsedTime(&t, ev[i], ev[i + 1]));
             ph[i] += t;
         }
     }
-    if (answers) *answers = n;
+    if (answers) *answers = queries;
     if (launches) *launches = c->launches;
     if (total_ms) *total_ms = tot;
     if (phase_ms)
@@ -761,23 +1066,24 @@ int kspir_matrix_vector_mul_bsgs_rns_crt_large(kspir_ctx* c, int client, uint64_
     if (!query_inout || !result) return KSPIR_ERR_INVALID_ARG;
     if (!canonical(query_inout, 2 * kN, kCrtMod) || !canonical(query_inout + 2 * kN, 2 * kN, kBsMod))
         return set_err(c, KSPIR_ERR_INVALID_ARG, "query word not canonical");
-    WsSlot& s = c->ws[0];
-    const ClientKeysDev& keys = c->clients[client].keys;
+    std::lock_guard<std::mutex> lk(c->mu);
+    const Workspace w = ws_host(c, 0);
     cudaStream_t st = c->stream;
     KS_CUDA(c, cudaSetDevice(c->device));
-    KS_CUDA(c, cudaMemcpyAsync(s.ws.q64, query_inout, 4 * kN * 8, cudaMemcpyHostToDevice, st));
-    enqueue_baby(c, s, keys, st);
-    enqueue_scan(c, s, st);
-    enqueue_giant(c, s, keys, st);
+    KS_CUDA(c, cudaMemcpyAsync(c->bq64, query_inout, 4 * kN * 8, cudaMemcpyHostToDevice, st));
+    k_set_clients<<<1, 32, 0, st>>>(c->client_of, 0, ClientList{1, {client}});
+    enqueue_baby(c, 0, 1, st);
+    enqueue_scan(c, 0, 1, SCAN_CUDA, st);
+    enqueue_giant(c, 0, 1, st);
     // result words, and the modswitched query (cipherbuf column 0) back into query1[0]
-    uint64_t* words = reinterpret_cast<uint64_t*>(s.stage32);
-    k_compose_words<<<blocks_for((long)c->p.r * 2 * kN, 256), 256, 0, st>>>(s.ws.result, words, c->p.r * 2);
+    uint64_t* words = reinterpret_cast<uint64_t*>(c->stage32);
+    k_compose_words<<<blocks_for((long)c->p.r * 2 * kN, 256), 256, 0, st>>>(w.result, words, c->p.r * 2);
     KS_CUDA(c, cudaGetLastError());
     KS_CUDA(c, cudaMemcpyAsync(result, words, (size_t)c->p.r * 2 * kN * 8, cudaMemcpyDeviceToHost, st));
-    rc = finish(c, s);
+    rc = finish(c, 0, 1);
     if (rc) return rc;
     std::vector<uint64_t> cb((size_t)kN * c->N1 * 2);
-    KS_COPY(c, cb.data(), s.ws.cipherbuf, cb.size() * 8, cudaMemcpyDeviceToHost);
+    KS_COPY(c, cb.data(), w.cipherbuf, cb.size() * 8, cudaMemcpyDeviceToHost);
     for (int comp = 0; comp < 2; comp++)
         for (int k = 0; k < kN; k++) {
             const uint64_t wv = cb[(size_t)k * c->N1 * 2 + comp];
@@ -791,52 +1097,55 @@ int kspir_matrix_vector_mul_bsgs_rns_crt_large(kspir_ctx* c, int client, uint64_
 
 int kspir_external_product(kspir_ctx* c, int client, uint64_t* result, uint64_t* first_dim, int count) {
     if (!c) return KSPIR_ERR_INVALID_ARG;
-    if (client < 0 || client >= (int)c->clients.size() || !c->clients[client].loaded)
-        return set_err(c, KSPIR_ERR_NOT_READY, "client keys not uploaded");
+    int rc = check_client(c, client);
+    if (rc) return rc;
     if (!result || !first_dim || count < 1 || count > c->p.r) return KSPIR_ERR_INVALID_ARG;
     const size_t n = (size_t)count * 2 * kN;
     if (!canonical(result, n, kCrtMod) || !canonical(first_dim, n, kCrtMod))
         return set_err(c, KSPIR_ERR_INVALID_ARG, "ciphertext word not canonical");
-    WsSlot& s = c->ws[0];
-    const ClientKeysDev& keys = c->clients[client].keys;
+    std::lock_guard<std::mutex> lk(c->mu);
+    const Workspace w = ws_host(c, 0);
     cudaStream_t st = c->stream;
     KS_CUDA(c, cudaSetDevice(c->device));
-    uint64_t* words = reinterpret_cast<uint64_t*>(s.stage32);     // r*2*N u64 fit in r*4*N u32
+    k_set_clients<<<1, 32, 0, st>>>(c->client_of, 0, ClientList{1, {client}});
+    uint64_t* words = reinterpret_cast<uint64_t*>(c->stage32);     // r*2*N u64 fit in r*4*N u32
     // first_dim -> ws.result residues; the caller's accumulators (NTT domain) -> ws.sout residues
     KS_CUDA(c, cudaMemcpyAsync(words, first_dim, n * 8, cudaMemcpyHostToDevice, st));
-    k_split_words<<<blocks_for((long)n, 256), 256, 0, st>>>(words, s.ws.result, count * 2);
-    uint32_t* acc = s.ws.sout;   // r*N2*4*N >= count*4*N residues
+    k_split_words<<<blocks_for((long)n, 256), 256, 0, st>>>(words, w.result, count * 2);
+    uint32_t* acc = w.sout;   // r*N2*4*N >= count*4*N residues
     KS_CUDA(c, cudaMemcpyAsync(words, result, n * 8, cudaMemcpyHostToDevice, st));
     k_split_words<<<blocks_for((long)n, 256), 256, 0, st>>>(words, acc, count * 2);
-    enqueue_ext(c, s, keys, count, acc, s.ws.ecoef, st);
-    k_compose_words<<<blocks_for((long)n, 256), 256, 0, st>>>(s.ws.ext, words, count * 2);
+    enqueue_ext(c, 0, 1, count, acc, w.ecoef, st);
+    k_compose_words<<<blocks_for((long)n, 256), 256, 0, st>>>(w.ext, words, count * 2);
     KS_CUDA(c, cudaGetLastError());
     KS_CUDA(c, cudaMemcpyAsync(result, words, n * 8, cudaMemcpyDeviceToHost, st));
-    int rc = finish(c, s);
+    rc = finish(c, 0, 1);
     if (rc) return rc;
-    k_compose_words<<<blocks_for((long)n, 256), 256, 0, st>>>(s.ws.ecoef, words, count * 2);
+    k_compose_words<<<blocks_for((long)n, 256), 256, 0, st>>>(w.ecoef, words, count * 2);
     KS_CUDA(c, cudaGetLastError());
     KS_CUDA(c, cudaMemcpyAsync(first_dim, words, n * 8, cudaMemcpyDeviceToHost, st));
-    return finish(c, s);
+    return finish(c, 0, 1);
 }
 
 int kspir_packing_rlwes(kspir_ctx* c, int client, const uint64_t* rlwes, uint64_t* response) {
     if (!c) return KSPIR_ERR_INVALID_ARG;
-    if (client < 0 || client >= (int)c->clients.size() || !c->clients[client].loaded)
-        return set_err(c, KSPIR_ERR_NOT_READY, "client keys not uploaded");
+    int rc = check_client(c, client);
+    if (rc) return rc;
     if (!rlwes || !response) return KSPIR_ERR_INVALID_ARG;
     const size_t n = (size_t)c->p.r * 2 * kN;
     if (!canonical(rlwes, n, kCrtMod)) return set_err(c, KSPIR_ERR_INVALID_ARG, "ciphertext word not canonical");
-    WsSlot& s = c->ws[0];
+    std::lock_guard<std::mutex> lk(c->mu);
+    const Workspace w = ws_host(c, 0);
     cudaStream_t st = c->stream;
     KS_CUDA(c, cudaSetDevice(c->device));
-    uint64_t* words = reinterpret_cast<uint64_t*>(s.stage32);
+    k_set_clients<<<1, 32, 0, st>>>(c->client_of, 0, ClientList{1, {client}});
+    uint64_t* words = reinterpret_cast<uint64_t*>(c->stage32);
     KS_CUDA(c, cudaMemcpyAsync(words, rlwes, n * 8, cudaMemcpyHostToDevice, st));
-    k_split_words<<<blocks_for((long)n, 256), 256, 0, st>>>(words, s.ws.ext, c->p.r * 2);
-    enqueue_packing(c, s, c->clients[client].keys, st);
+    k_split_words<<<blocks_for((long)n, 256), 256, 0, st>>>(words, w.ext, c->p.r * 2);
+    enqueue_packing(c, 0, 1, st);
     KS_CUDA(c, cudaGetLastError());
-    KS_CUDA(c, cudaMemcpyAsync(response, s.ws.resp64, 2 * kN * 8, cudaMemcpyDeviceToHost, st));
-    return finish(c, s);
+    KS_CUDA(c, cudaMemcpyAsync(response, c->bresp, 2 * kN * 8, cudaMemcpyDeviceToHost, st));
+    return finish(c, 0, 1);
 }
 
 int kspir_permutation_matrix(int32_t* perms, int N1) {
@@ -849,9 +1158,10 @@ int kspir_permutation_matrix(int32_t* perms, int N1) {
     return KSPIR_OK;
 }
 
-int kspir_fetch_stage(kspir_ctx* c, int stage, uint64_t* out, size_t words) {
-    if (!c || !out) return KSPIR_ERR_INVALID_ARG;
-    WsSlot& s = c->ws[0];
+int kspir_fetch_stage_slot(kspir_ctx* c, int slot, int stage, uint64_t* out, size_t words) {
+    if (!c || !out || slot < 0 || slot >= c->p.max_inflight) return KSPIR_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(c->mu);
+    const Workspace w = ws_host(c, slot);
     const int R = c->p.r;
     cudaStream_t st = c->stream;
     KS_CUDA(c, cudaSetDevice(c->device));
@@ -859,24 +1169,40 @@ int kspir_fetch_stage(kspir_ctx* c, int stage, uint64_t* out, size_t words) {
     if (stage == KSPIR_STAGE_CIPHERBUF) {
         const size_t n = (size_t)kN * c->N1 * 2;
         if (words != n) return set_err(c, KSPIR_ERR_INVALID_ARG, "size mismatch");
-        KS_COPY(c, out, s.ws.cipherbuf, n * 8, cudaMemcpyDeviceToHost);
+        KS_COPY(c, out, w.cipherbuf, n * 8, cudaMemcpyDeviceToHost);
         return KSPIR_OK;
     }
     const uint32_t* src = nullptr;
     size_t polys = 0;
-    if (stage == KSPIR_STAGE_SCAN) { src = s.ws.sout; polys = (size_t)R * c->N2 * 2; }
-    else if (stage == KSPIR_STAGE_RESULT) { src = s.ws.result; polys = (size_t)R * 2; }
-    else if (stage == KSPIR_STAGE_EXT) { src = s.ws.ext; polys = (size_t)R * 2; }
+    if (stage == KSPIR_STAGE_SCAN) { src = w.sout; polys = (size_t)R * c->N2 * 2; }
+    else if (stage == KSPIR_STAGE_RESULT) { src = w.result; polys = (size_t)R * 2; }
+    else if (stage == KSPIR_STAGE_EXT) { src = w.ext; polys = (size_t)R * 2; }
     else return set_err(c, KSPIR_ERR_INVALID_ARG, "unknown stage");
     if (words != polys * kN) return set_err(c, KSPIR_ERR_INVALID_ARG, "size mismatch");
     uint64_t* tmp = nullptr;
+    uint32_t* flat = nullptr;
     KS_CUDA(c, cudaMalloc(&tmp, words * 8));
-    k_compose_words<<<blocks_for((long)words, 256), 256, 0, st>>>(src, tmp, (int)polys);
-    cudaError_t e = cudaMemcpyAsync(out, tmp, words * 8, cudaMemcpyDeviceToHost, st);
+    cudaError_t e = cudaSuccess;
+    if (stage == KSPIR_STAGE_SCAN) {
+        e = cudaMalloc(&flat, words * 8);
+        if (e == cudaSuccess) {
+            k_unblock_sout<<<blocks_for((long)R * c->N2 * 4 * kN, 256), 256, 0, st>>>(src, flat, R * c->N2);
+            src = flat;
+        }
+    }
+    if (e == cudaSuccess) {
+        k_compose_words<<<blocks_for((long)words, 256), 256, 0, st>>>(src, tmp, (int)polys);
+        e = cudaMemcpyAsync(out, tmp, words * 8, cudaMemcpyDeviceToHost, st);
+    }
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     cudaFree(tmp);
+    cudaFree(flat);
     if (e != cudaSuccess) return set_err(c, KSPIR_ERR_CUDA, cudaGetErrorString(e));
     return KSPIR_OK;
+}
+
+int kspir_fetch_stage(kspir_ctx* c, int stage, uint64_t* out, size_t words) {
+    return kspir_fetch_stage_slot(c, 0, stage, out, words);
 }
 
 }  // extern "C"
@@ -1046,9 +1372,9 @@ extern "C" int kspir_external_product_noalloc(int device, const uint64_t* d_rgsw
         k_split_words<<<blocks_for((long)n, 256), 256, 0, st>>>(d_first_dim, L.fd_res, count * 2);
         k_split_words<<<blocks_for((long)n, 256), 256, 0, st>>>(d_result, L.acc_res, count * 2);
         k_split_words<<<blocks_for(8L * kN, 256), 256, 0, st>>>(d_rgsw, L.rgsw, 8);
-        k_ntt_jobs<true><<<count * 4, kNttThreads, kNttJobSmem, st>>>(L.jobs, tabs);
+        k_ntt_jobs<true><<<count * 4, kNttThreads, kNttJobSmem, st>>>(L.jobs, tabs, Batch{});
         k_ext_decomp<<<blocks_for((long)count * kN, 256), 256, 0, st>>>(L.ecoef, L.edig, count, g);
-        k_ntt_jobs<false><<<count * 8, kNttThreads, kNttJobSmem, st>>>(L.jobs + kNoAllocMaxCount * 4, tabs);
+        k_ntt_jobs<false><<<count * 8, kNttThreads, kNttJobSmem, st>>>(L.jobs + kNoAllocMaxCount * 4, tabs, Batch{});
         k_ext_mac_intt<<<count * 4, kNttThreads, kMacSmem, st>>>(L.edig, L.rgsw, L.acc_res, L.ext, 4, tabs);
         int flag = 0;
         if (cudaGetLastError() != cudaSuccess ||

@@ -5,6 +5,8 @@
 // lives in one Workspace so several queries can be in flight at once.
 #pragma once
 
+#include <type_traits>
+
 #include "common.cuh"
 #include "gadget.cuh"
 
@@ -24,6 +26,14 @@ struct ClientKeysDev {
     const uint32_t* rgsw;
 };
 
+// Database-scan output layout: z-blocked so that eight consecutive NTT slots of
+// one polynomial share a 32-byte sector (the batched scan writes whole sectors):
+//   sout[z / 8][row = r * N2 + i][comp * 2 + ch][z % 8]
+constexpr int kZBlock = 8;
+__host__ __device__ __forceinline__ size_t sout_idx(int row, int cv, int z, int rows) {
+    return (((size_t)(z >> 3) * rows + row) * 4 + cv) * kZBlock + (z & 7);
+}
+
 struct Workspace {
     uint64_t* q64;          // [4][N] query words: crt a, crt b, bs a, bs b (coefficient form)
     uint32_t* dig0;         // [3][3 ch][N] decompose_bsgs(query a) digits -> NTT form
@@ -36,15 +46,77 @@ struct Workspace {
     uint32_t* inter_acoef;  // [2 ch][N] interA, coefficient form
     uint32_t* dig1;         // [3][3 ch][N] digits of the intermediate -> NTT form
     uint64_t* cipherbuf;    // [N][N1][2] reference reorientCipher layout (twosteps.cpp:1386)
-    uint32_t* sout;         // [r][N2][2 comp][2 ch][N] DB-scan outputs, NTT form
+    uint32_t* sout;         // DB-scan outputs, NTT form, layout of sout_idx (r * N2 rows)
     uint32_t* result;       // [r][2 comp][2 ch][N] first-dimension results, NTT form
     uint32_t* ecoef;        // [r][2 comp][2 ch][N] result, coefficient form
     uint32_t* ext;          // [r][2 comp][2 ch][N] external products, coefficient form
     uint32_t* ext2;         // [r/2][2 comp][2 ch][N] packing levels ping-pong with ext
     unsigned long long* gacc;  // [r][2 comp][2 ch][N] giant-step accumulators
     uint64_t* resp64;       // [2][N] response words
-    int* err;               // device error word (bounded waits)
+    int* err;               // device error word (bounded waits), slot-indexed array
 };
+constexpr int kErrStride = 64;   // ints between the error words of two slots
+
+// Batch addressing.  Query q of a launch (blockIdx.y) runs in workspace slot
+// slot0 + q.  Every workspace slot is a copy of slot 0's layout at a fixed byte
+// stride, every client key slot a copy of slot 0's at another, so a kernel
+// reaches its query's buffers by shifting slot-0 pointers.  The query words,
+// response words and error words live in slot-indexed arrays (one host copy
+// per batch).
+struct Batch {
+    size_t ws_bytes;        // stride between workspace slots
+    size_t key_bytes;       // stride between client key slots
+    const int* client_of;   // [slots] client key slot serving each workspace slot
+    int slot0;
+};
+
+template <class T>
+__device__ __forceinline__ T* shifted(T* p, size_t off) {
+    return p ? reinterpret_cast<T*>(reinterpret_cast<char*>(const_cast<typename std::remove_const<T>::type*>(p)) + off)
+             : p;
+}
+
+__device__ __forceinline__ int batch_slot(const Batch& b) { return b.slot0 + (int)blockIdx.y; }
+
+__device__ __forceinline__ Workspace ws_at(Workspace w, const Batch& b) {
+    const int s = batch_slot(b);
+    const size_t off = (size_t)s * b.ws_bytes;
+    w.q64 += (size_t)s * 4 * kN;
+    w.resp64 += (size_t)s * 2 * kN;
+    w.dig0 = shifted(w.dig0, off);
+    w.qbn = shifted(w.qbn, off);
+    w.qbbs = shifted(w.qbbs, off);
+    w.col0 = shifted(w.col0, off);
+    w.interA = shifted(w.interA, off);
+    w.interB = shifted(w.interB, off);
+    w.inter_bs = shifted(w.inter_bs, off);
+    w.inter_acoef = shifted(w.inter_acoef, off);
+    w.dig1 = shifted(w.dig1, off);
+    w.cipherbuf = shifted(w.cipherbuf, off);
+    w.sout = shifted(w.sout, off);
+    w.result = shifted(w.result, off);
+    w.ecoef = shifted(w.ecoef, off);
+    w.ext = shifted(w.ext, off);
+    w.ext2 = shifted(w.ext2, off);
+    w.gacc = shifted(w.gacc, off);
+    w.err += (size_t)s * kErrStride;
+    return w;
+}
+
+__device__ __forceinline__ size_t ws_off(const Batch& b) { return (size_t)batch_slot(b) * b.ws_bytes; }
+__device__ __forceinline__ size_t key_off(const Batch& b) {
+    return (size_t)__ldg(b.client_of + batch_slot(b)) * b.key_bytes;
+}
+
+__device__ __forceinline__ ClientKeysDev keys_at(ClientKeysDev k, const Batch& b) {
+    const size_t off = key_off(b);
+    k.baby_crt = shifted(k.baby_crt, off);
+    k.baby_bs = shifted(k.baby_bs, off);
+    k.giant = shifted(k.giant, off);
+    k.packing = shifted(k.packing, off);
+    k.rgsw = shifted(k.rgsw, off);
+    return k;
+}
 
 // Gadget parameters of the path (reference defaults; lwe.h:391-404, test-pir.cpp:71, :88).
 struct PathGadgets {

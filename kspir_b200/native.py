@@ -55,7 +55,22 @@ SIGNATURES = {
     "kspir_external_product_noalloc": (_i, [_i, _vp, _vp, _vp, _i, _vp]),
     "kspir_timing_reset": (_i, [_vp]),
     "kspir_timing_summary": (_i, [_vp, _vp, _vp, _vp, _vp]),
+    "kspir_answer_batch": (_i, [_vp, _i, _vp, _vp, _vp]),
+    "kspir_answer_batch_device": (_i, [_vp, _i, _vp, _vp, _vp, _vp]),
+    "kspir_tune_batch": (_i, [_vp, _i, _vp, _vp]),
+    "kspir_set_scan_kind": (_i, [_vp, _i, _i]),
+    "kspir_get_scan_kind": (_i, [_vp, _i]),
+    "kspir_fetch_stage_slot": (_i, [_vp, _i, _i, _vp, _sz]),
 }
+
+# database-scan variants of kspir_tune_batch / kspir_set_scan_kind
+SCAN_CUDA = 0
+SCAN_MMA4 = 1
+SCAN_MMA8 = 2
+SCAN_MMA16 = 3
+SCAN_MMA32 = 4
+SCAN_NAMES = {SCAN_CUDA: "cuda-core", SCAN_MMA4: "tcgen05-bt4", SCAN_MMA8: "tcgen05-bt8",
+              SCAN_MMA16: "tcgen05-bt16", SCAN_MMA32: "tcgen05-bt32"}
 
 
 class Params(ctypes.Structure):
@@ -177,6 +192,37 @@ class Context:
     def sync(self):
         self._check(self.lib.kspir_sync(self._h))
 
+    def answer_batch(self, clients, queries, out: np.ndarray | None = None) -> np.ndarray:
+        """Responses [n][2][N] of n queries ([n][2][2][N]) of the given client slots."""
+        cl = np.ascontiguousarray(clients, dtype=np.int32).reshape(-1)
+        q = _u64(queries).reshape(-1)
+        n = cl.size
+        if q.size != n * 4 * N:
+            raise ValueError("queries must be [n][2][2][N]")
+        if out is None:
+            out = np.empty((n, 2 * N), dtype=np.uint64)
+        self._check(self.lib.kspir_answer_batch(self._h, n, ptr(cl), ptr(q), ptr(out)))
+        return out
+
+    def answer_batch_device(self, clients, d_queries: int, d_responses: int, stream: int | None = None):
+        cl = np.ascontiguousarray(clients, dtype=np.int32).reshape(-1)
+        self._check(self.lib.kspir_answer_batch_device(self._h, cl.size, ptr(cl), ctypes.c_void_p(d_queries),
+                                                       ctypes.c_void_p(d_responses),
+                                                       ctypes.c_void_p(stream) if stream else None))
+
+    def tune_batch(self, n: int):
+        """Times every scan variant for batches of n; returns (chosen kind, {kind: ms})."""
+        kind = ctypes.c_int()
+        ms = (ctypes.c_float * 5)()
+        self._check(self.lib.kspir_tune_batch(self._h, n, ctypes.byref(kind), ms))
+        return kind.value, {k: ms[k] for k in range(5) if ms[k] < 1e29}
+
+    def set_scan_kind(self, n: int, kind: int):
+        self._check(self.lib.kspir_set_scan_kind(self._h, n, kind))
+
+    def scan_kind(self, n: int) -> int:
+        return self.lib.kspir_get_scan_kind(self._h, n)
+
     def last_timing(self):
         tot = ctypes.c_float()
         ph = (ctypes.c_float * 5)()
@@ -215,9 +261,9 @@ class Context:
         self._check(self.lib.kspir_packing_rlwes(self._h, client, ptr(rl), ptr(out)))
         return out
 
-    def fetch_stage(self, stage: int) -> np.ndarray:
+    def fetch_stage(self, stage: int, slot: int = 0) -> np.ndarray:
         sizes = {STAGE_CIPHERBUF: N * self.N1 * 2, STAGE_SCAN: self.r * self.N2 * 2 * N,
                  STAGE_RESULT: self.r * 2 * N, STAGE_EXT: self.r * 2 * N}
         out = np.empty(sizes[stage], dtype=np.uint64)
-        self._check(self.lib.kspir_fetch_stage(self._h, stage, ptr(out), out.size))
+        self._check(self.lib.kspir_fetch_stage_slot(self._h, slot, stage, ptr(out), out.size))
         return out
