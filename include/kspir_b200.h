@@ -185,6 +185,9 @@ int kspir_timing_summary(kspir_ctx* ctx, int* answers, long* launches, float* to
  * as reference words (host buffer of exactly the stated size):
  *   KSPIR_STAGE_CIPHERBUF [N][N1][2]  reorientCipher output (twosteps.cpp:1386-1403)
  *   KSPIR_STAGE_SCAN      [r][N2][2][N] fastMultiplyQueryByDatabaseDim1InvCRT outputs
+ *                         (recomputed from the slot's reorientCipher output by
+ *                         the scan variant of the last launch: the giant steps
+ *                         reuse the scan output in place)
  *   KSPIR_STAGE_RESULT    [r][2][N]   first-dimension results (NTT form)
  *   KSPIR_STAGE_EXT       [r][2][N]   external products (coefficient form) */
 #define KSPIR_STAGE_CIPHERBUF 0

@@ -51,13 +51,15 @@ __device__ __forceinline__ uint32_t pow5_mod2n(uint32_t e) {
     return r;
 }
 
-constexpr int kBabySmem = kN * 8 + kN * 4;   // twiddles + one polynomial
+constexpr int kBabySmem = kN * 8 + kPadN * 4;       // twiddles + one padded polynomial
 constexpr int kPerThread = kN / kNttThreads; // 8 coefficients per thread
 
 // One CTA per (rotation, component, crt prime): blockIdx.x = 4*ki + 2*comp + ch;
-// blockIdx.y = query of the batch.
-// Each CTA recomputes the bsMod part of its component (one inverse transform)
-// so the four CTAs of a rotation run in parallel.
+// blockIdx.y = query of the batch.  Each CTA recomputes the bsMod part of its
+// component (one inverse transform) so the four CTAs of a rotation run in
+// parallel.  (One CTA per (rotation, component) doing both primes saves two
+// of the eight transforms per rotation but measured slower on B200 even for
+// batches of 64: these CTAs are latency-bound, not issue-bound.)
 template <int ELL>
 __global__ void __launch_bounds__(kNttThreads) k_baby_rot(BabyArgs a, ClientKeysDev keys, NttTables tabs, Batch bt) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
@@ -107,7 +109,7 @@ __global__ void __launch_bounds__(kNttThreads) k_baby_rot(BabyArgs a, ClientKeys
         }
 #pragma unroll
         for (int it = 0; it < kPerThread; it++)
-            S[tid + it * kNttThreads] = negmod(reduce64(acc[it], cb.q, cb.barrett), cb.q);
+            S[pidx(tid) + it * kPadStep] = negmod(reduce64(acc[it], cb.q, cb.barrett), cb.q);
     }
     cta_ntt_inverse(S, tws, CH_BS);
 
@@ -118,26 +120,29 @@ __global__ void __launch_bounds__(kNttThreads) k_baby_rot(BabyArgs a, ClientKeys
 #pragma unroll
         for (int it = 0; it < kPerThread; it++) {
             const int k = tid + it * kNttThreads;
+            const int pk2 = pidx(tid) + it * kPadStep;
             bool neg;
             const int src = auto_src(k, ginv, &neg);
             uint32_t v = __ldg(a.srcBbs + src);
             if (neg) v = negmod(v, qb);
-            S[k] = addmod(S[k], v, qb);
+            S[pk2] = addmod(S[pk2], v, qb);
         }
     }
     if (inter && ch == 0) {
 #pragma unroll
         for (int it = 0; it < kPerThread; it++) {
             const int k = tid + it * kNttThreads;
-            a.inter_bs[comp * kN + k] = S[k];
+            a.inter_bs[comp * kN + k] = S[pidx(tid) + it * kPadStep];
         }
     }
-    __syncthreads();   // S complete and the inverse twiddles no longer read
+    const uint16_t* __restrict__ sig = a.sigma + (size_t)ki * kN;
+    uint32_t* cb32 = reinterpret_cast<uint32_t*>(a.cipherbuf);
+    uint32_t* inter_out = comp == 0 ? a.interA : a.interB;
+    __syncthreads();   // x2 complete and the inverse twiddles no longer read
     stage_twiddles(tws, tabs, ch, NTT_FWD);
     cta_ntt_forward(S, tws, ch);   // NTT_ch(x2), x2 < bsMod < q
 
     const ChanConst cc = c_dev.ch[ch];
-    const uint16_t* __restrict__ sig = a.sigma + (size_t)ki * kN;
     uint64_t acc[kPerThread];
 #pragma unroll
     for (int it = 0; it < kPerThread; it++) acc[it] = 0;
@@ -149,15 +154,13 @@ __global__ void __launch_bounds__(kNttThreads) k_baby_rot(BabyArgs a, ClientKeys
         for (int it = 0; it < kPerThread; it++)
             acc[it] += (uint64_t)__ldg(d + pk[it]) * __ldg(kk + tid + it * kNttThreads);
     }
-    uint32_t* cb32 = reinterpret_cast<uint32_t*>(a.cipherbuf);
-    uint32_t* inter_out = comp == 0 ? a.interA : a.interB;
 #pragma unroll
     for (int it = 0; it < kPerThread; it++) {
         const int k = tid + it * kNttThreads;
         uint32_t A = negmod(reduce64(acc[it], cc.q, cc.barrett), cc.q);
         if (comp == 1) A = addmod(A, __ldg(a.srcB + ch * kN + sig[k]), cc.q);
         if (inter) inter_out[ch * kN + k] = A;
-        const uint32_t r = shoup_mul(submod(A, S[k], cc.q), cc.bsinv, cc.bsinv_p, cc.q);
+        const uint32_t r = shoup_mul(submod(A, S[pidx(tid) + it * kPadStep], cc.q), cc.bsinv, cc.bsinv_p, cc.q);
         cb32[(((size_t)k * a.N1 + col) * 2 + comp) * 2 + ch] = r;
     }
 }

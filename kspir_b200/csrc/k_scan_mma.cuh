@@ -70,6 +70,7 @@ struct MmaCfg {
     static constexpr int CHUNKS = N / 16;             // 16-column chunks = 4 query groups each
     static constexpr int PARTS = CHUNKS < 4 ? CHUNKS : 4;   // epilogue warps per TMEM quarter
     static constexpr int CPW = CHUNKS / PARTS;        // chunks (outputs per lane) per epilogue warp
+    static constexpr int LDB = CPW < 2 ? CPW : 2;     // outputs whose TMEM loads share one wait
     static constexpr int EPI = 4 * PARTS;             // epilogue warps
     static constexpr int THREADS = 32 * (2 + EPI);
     static_assert(NA >= 2 && SMEM <= kMmaSmemLimit, "shared memory budget");
@@ -285,25 +286,34 @@ __global__ void __launch_bounds__(MmaCfg<BT>::THREADS, 1) k_scan_mma(ScanMmaArgs
                     }
                     tc_fence_after();
 #pragma unroll
-                    for (int c = 0; c < C::CPW; c++) {
-                        uint32_t lo[8], hi[8];   // limbs la 0,1 and la 2,3
-                        const uint32_t col = tq + tb * C::N + c * 16;
-                        tmem_ld_16x256b_x2(col, lo);
-                        tmem_ld_16x256b_x2(col + (16u << 16), hi);
+                    for (int c0 = 0; c0 < C::CPW; c0 += C::LDB) {
+                        // LDB outputs per wait: their loads overlap
+                        uint32_t lo[C::LDB][8], hi[C::LDB][8];   // limbs la 0,1 and la 2,3
+#pragma unroll
+                        for (int c1 = 0; c1 < C::LDB; c1++) {
+                            const uint32_t col = tq + tb * C::N + (c0 + c1) * 16;
+                            tmem_ld_16x256b_x2(col, lo[c1]);
+                            tmem_ld_16x256b_x2(col + (16u << 16), hi[c1]);
+                        }
                         tmem_wait_ld();
-                        // v[la][lb]: lo = {00, 01, 10, 11, 02, 03, 12, 13}, hi likewise for la + 2
-                        const uint32_t t1 = lo[1] + lo[2];
-                        const uint32_t t2 = lo[4] + lo[3] + hi[0];
-                        const uint32_t t3 = lo[5] + lo[6] + hi[1] + hi[2];
-                        const uint32_t t4 = lo[7] + hi[4] + hi[3];
-                        const uint32_t t5 = hi[5] + hi[6];
-                        uint64_t x = lo[0];
-                        mad_wide(x, t1, 1u << 8);
-                        mad_wide(x, t2, 1u << 16);
-                        mad_wide(x, t3, 1u << 24);
-                        const uint32_t xh = t4 + (t5 << 8) + (hi[7] << 16);   // weights 2^32.. (mod 2^64)
-                        x += (uint64_t)xh << 32;
-                        ob[zi][c] = mod28(x, q, mu1, c32, mu2);
+#pragma unroll
+                        for (int c1 = 0; c1 < C::LDB; c1++) {
+                            const uint32_t* L = lo[c1];
+                            const uint32_t* H = hi[c1];
+                            // v[la][lb]: L = {00, 01, 10, 11, 02, 03, 12, 13}, H likewise for la + 2
+                            const uint32_t t1 = L[1] + L[2];
+                            const uint32_t t2 = L[4] + L[3] + H[0];
+                            const uint32_t t3 = L[5] + L[6] + H[1] + H[2];
+                            const uint32_t t4 = L[7] + H[4] + H[3];
+                            const uint32_t t5 = H[5] + H[6];
+                            uint64_t x = L[0];
+                            mad_wide(x, t1, 1u << 8);
+                            mad_wide(x, t2, 1u << 16);
+                            mad_wide(x, t3, 1u << 24);
+                            const uint32_t xh = t4 + (t5 << 8) + (H[7] << 16);   // weights 2^32.. (mod 2^64)
+                            x += (uint64_t)xh << 32;
+                            ob[zi][c0 + c1] = mod28(x, q, mu1, c32, mu2);
+                        }
                     }
                     tc_fence_before();
                     __syncwarp();
@@ -344,49 +354,54 @@ __global__ void __launch_bounds__(MmaCfg<BT>::THREADS, 1) k_scan_mma(ScanMmaArgs
 // Query operand of a batch: qop[z][ch][qt] tiles of 8 BT rows
 // n = mma_brow(comp * BT + b, lb), byte k = limb lb of the prime-ch residue of
 // cipherbuf[z][k][comp] of query qt * BT + b (workspace slot slot0 + that);
-// queries past nq are zero.  One thread per (z, qt, comp, b, 16-byte chunk).
+// queries past nq are zero.  One thread per (z, qt, b, 16-byte chunk): it reads
+// the 16 cipherbuf entries of its chunk (256 contiguous bytes: both components
+// and both primes) and writes 16 chunks of 16 bytes.
 template <int BT>
 __global__ void k_qop_split(const uint64_t* __restrict__ cb0, size_t ws_bytes, int slot0, int nq, int QT,
                             uint8_t* __restrict__ qop) {
     using C = MmaCfg<BT>;
     const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long total = (long)kN * QT * 2 * BT * 8;
+    const long total = (long)kN * QT * BT * 8;
     if (idx >= total) return;
     const int c = (int)(idx & 7);
     const int b = (int)((idx >> 3) % BT);
-    const int comp = (int)((idx >> 3) / BT % 2);
-    const long zq = (idx >> 3) / BT / 2;        // z * QT + qt
+    const long zq = (idx >> 3) / BT;            // z * QT + qt
     const int qt = (int)(zq % QT), z = (int)(zq / QT);
     const int bq = qt * BT + b;
-    uint32_t w[2][16];
+    uint4 w[16];   // entry k = 16 c + j: (comp 0 ch 0, comp 0 ch 1, comp 1 ch 0, comp 1 ch 1)
     if (bq < nq) {
-        const uint32_t* cb = reinterpret_cast<const uint32_t*>(
-            reinterpret_cast<const char*>(cb0) + (size_t)(slot0 + bq) * ws_bytes);
+        const uint4* cb = reinterpret_cast<const uint4*>(reinterpret_cast<const char*>(cb0) +
+                                                         (size_t)(slot0 + bq) * ws_bytes) +
+                          (size_t)z * kMmaK + 16 * c;
 #pragma unroll
-        for (int j = 0; j < 16; j++) {
-            const uint2 v = __ldg(reinterpret_cast<const uint2*>(cb + (((size_t)z * kMmaK + 16 * c + j) * 2 + comp) * 2));
-            w[0][j] = v.x;
-            w[1][j] = v.y;
-        }
+        for (int j = 0; j < 16; j++) w[j] = __ldg(cb + j);
     } else {
 #pragma unroll
-        for (int j = 0; j < 16; j++) w[0][j] = w[1][j] = 0;
+        for (int j = 0; j < 16; j++) w[j] = make_uint4(0, 0, 0, 0);
     }
 #pragma unroll
     for (int ch = 0; ch < 2; ch++) {
         uint8_t* tile = qop + (((size_t)z * 2 + ch) * QT + qt) * C::BTILE;
 #pragma unroll
-        for (int lb = 0; lb < 4; lb++) {
-            uint32_t pk[4];
+        for (int comp = 0; comp < 2; comp++) {
 #pragma unroll
-            for (int q4 = 0; q4 < 4; q4++) {
-                uint32_t x = 0;
+            for (int lb = 0; lb < 4; lb++) {
+                uint32_t pk[4];
 #pragma unroll
-                for (int t = 0; t < 4; t++) x |= ((w[ch][4 * q4 + t] >> (8 * lb)) & 255u) << (8 * t);
-                pk[q4] = x;
+                for (int q4 = 0; q4 < 4; q4++) {
+                    uint32_t x = 0;
+#pragma unroll
+                    for (int t = 0; t < 4; t++) {
+                        const uint4 e = w[4 * q4 + t];
+                        const uint32_t v = comp == 0 ? (ch == 0 ? e.x : e.y) : (ch == 0 ? e.z : e.w);
+                        x |= ((v >> (8 * lb)) & 255u) << (8 * t);
+                    }
+                    pk[q4] = x;
+                }
+                const int n = mma_brow(comp * BT + b, lb);
+                *reinterpret_cast<uint4*>(tile + sw128_off(n, 16 * c)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
             }
-            const int n = mma_brow(comp * BT + b, lb);
-            *reinterpret_cast<uint4*>(tile + sw128_off(n, 16 * c)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
         }
     }
 }

@@ -44,7 +44,7 @@ __global__ void k_ext_decomp(const uint32_t* __restrict__ ecoef, uint32_t* __res
 }
 
 // dynamic shared memory of the fused multiply-accumulate + inverse-transform kernels
-constexpr int kMacSmem = kN * 8 + kN * 4;
+constexpr int kMacSmem = kN * 8 + kPadN * 4;
 
 // One CTA per (r, comp, ch): ext = INTT( init + sum_row digit_row * rgsw[row].comp ),
 // init being the caller's NTT-domain accumulator (zero on the answer path,
@@ -67,12 +67,12 @@ __global__ void __launch_bounds__(kNttThreads) k_ext_mac_intt(const uint32_t* __
         for (int row = 0; row < rows; row++)
             acc += (uint64_t)d[(row * 2 + ch) * kN + k] * rgsw[((row * 2 + comp) * 2 + ch) * kN + k];
         const uint32_t m = reduce64(acc, cc.q, cc.barrett);
-        s[k] = init ? addmod(init[((size_t)r * 4 + comp * 2 + ch) * kN + k], m, cc.q) : m;
+        s[pidx(k)] = init ? addmod(init[((size_t)r * 4 + comp * 2 + ch) * kN + k], m, cc.q) : m;
     }
     cta_ntt_inverse(s, tws, ch);
     uint32_t* o = ext + ((size_t)r * 4 + comp * 2 + ch) * kN;
 #pragma unroll
-    for (int k = threadIdx.x; k < kN; k += T) o[k] = s[k];
+    for (int k = threadIdx.x; k < kN; k += T) o[k] = s[pidx(k)];
 }
 
 }  // namespace kspir
@@ -84,18 +84,19 @@ namespace kspir {
 // evalAutoRNSCRT for output[c] (twosteps.cpp:612-672) in shared memory:
 //   INTT(a) per prime -> compose -> X -> X^g -> decompose (ell digits)
 //   -> digit transforms -> -sum_j d_j * key[j]  and  b[sigma_g] - sum_j d_j * key[j]
-// and adds both into a 64-bit accumulator of sub-database r (atomics; the
-// canonical contributions of N2-1 giant steps cannot overflow it).
+// and writes both, canonical, over its own input row (r, c) of the scan
+// output: the a part once the inverse transforms have read it, the b part
+// after a barrier that ends every gather of it.  k_giant_finish then sums the
+// N2 rows of each sub-database (no atomics: the 15 giant steps of one
+// sub-database would all hit the same words at the same time).
 
 constexpr int kGiantPolys = 4;   // two primes x two digits (ell = 2)
 constexpr int kPerThreadG = kN / kNttThreads;
-constexpr int kGiantSmem = kN * 8 + kGiantPolys * kN * 4;
+constexpr int kGiantSmem = kN * 8 + kGiantPolys * kPadN * 4;
 
 template <int ELL>
-__global__ void __launch_bounds__(kNttThreads) k_giant_fused(const uint32_t* __restrict__ sout,
-                                                             const uint32_t* __restrict__ gkeys,
-                                                             const uint16_t* __restrict__ gsigma,
-                                                             unsigned long long* __restrict__ acc, int N1,
+__global__ void __launch_bounds__(kNttThreads) k_giant_fused(uint32_t* sout, const uint32_t* __restrict__ gkeys,
+                                                             const uint16_t* __restrict__ gsigma, int N1,
                                                              NttTables tabs, GadgetB g, int R, Batch bt) {
     static_assert(2 * ELL <= kGiantPolys, "shared-memory polynomials");
     extern __shared__ __align__(16) uint8_t smem_raw[];
@@ -108,18 +109,17 @@ __global__ void __launch_bounds__(kNttThreads) k_giant_fused(const uint32_t* __r
     const int row = r * N2 + c;
     const int tid = threadIdx.x;
     sout = shifted(sout, ws_off(bt));
-    acc = shifted(acc, ws_off(bt));
     gkeys = shifted(gkeys, key_off(bt));
 
     // a of output[c], both primes, to coefficient form
 #pragma unroll
     for (int ch = 0; ch < 2; ch++) {
         stage_twiddles(tws, tabs, ch, NTT_INV);
-        uint4* dst = reinterpret_cast<uint4*>(P + ch * kN);
 #pragma unroll
         for (int k = tid; k < kN / 4; k += kNttThreads)
-            dst[k] = __ldg(reinterpret_cast<const uint4*>(sout + sout_idx(row, 0 * 2 + ch, 4 * k, rows)));
-        cta_ntt_inverse(P + ch * kN, tws, ch);
+            *reinterpret_cast<uint4*>(P + ch * kPadN + pidx(4 * k)) =
+                *reinterpret_cast<const uint4*>(sout + sout_idx(row, 0 * 2 + ch, 4 * k, rows));
+        cta_ntt_inverse(P + ch * kPadN, tws, ch);
     }
     // X -> X^g, g = 5^(N1 c), then the digits (registers first: P is overwritten)
     const uint32_t e = (uint32_t)(N1 * c) & 2047u;
@@ -131,7 +131,7 @@ __global__ void __launch_bounds__(kNttThreads) k_giant_fused(const uint32_t* __r
         const int k = tid + it * kNttThreads;
         bool neg;
         const int src = auto_src(k, ginv, &neg);
-        uint64_t v = crt_compose_res(P[src], P[kN + src]);
+        uint64_t v = crt_compose_res(P[pidx(src)], P[kPadN + pidx(src)]);
         if (neg && v) v = kCrtMod - v;
         int32_t dig[kMaxEll];
         decompose_b(v, kCrtMod, g, dig);
@@ -147,7 +147,7 @@ __global__ void __launch_bounds__(kNttThreads) k_giant_fused(const uint32_t* __r
 #pragma unroll
         for (int j = 0; j < ELL; j++)
 #pragma unroll
-            for (int ch = 0; ch < 2; ch++) P[(j * 2 + ch) * kN + tid + it * kNttThreads] = dres[it][j][ch];
+            for (int ch = 0; ch < 2; ch++) P[(j * 2 + ch) * kPadN + pidx(tid) + it * kPadStep] = dres[it][j][ch];
     // digit transforms and the key multiply-accumulate, prime by prime
     const uint32_t* key = gkeys + (size_t)(c - 1) * ELL * 2 * 2 * kN;   // [ELL][2 comp][2 ch][N]
     const uint16_t* sig = gsigma + (size_t)(c - 1) * kN;
@@ -155,44 +155,43 @@ __global__ void __launch_bounds__(kNttThreads) k_giant_fused(const uint32_t* __r
     for (int ch = 0; ch < 2; ch++) {
         __syncthreads();
         stage_twiddles(tws, tabs, ch, NTT_FWD);
-        cta_ntt_forward_m<ELL>(P + ch * kN, 2 * kN, tws, ch);   // digits j of this prime: P[j*2+ch]
+        cta_ntt_forward_m<ELL>(P + ch * kPadN, 2 * kPadN, tws, ch);   // digits j of this prime: P[j*2+ch]
         const ChanConst cc = c_dev.ch[ch];
-        unsigned long long* acc_a = acc + ((size_t)(r * 2 + 0) * 2 + ch) * kN;
-        unsigned long long* acc_b = acc + ((size_t)(r * 2 + 1) * 2 + ch) * kN;
+        uint32_t cbv[kPerThreadG];
 #pragma unroll
         for (int it = 0; it < kPerThreadG; it++) {
             const int k = tid + it * kNttThreads;
             uint64_t sa = 0, sb = 0;
 #pragma unroll
             for (int j = 0; j < ELL; j++) {
-                const uint32_t d = P[(j * 2 + ch) * kN + k];
+                const uint32_t d = P[(j * 2 + ch) * kPadN + pidx(tid) + it * kPadStep];
                 mad_wide(sa, d, __ldg(key + ((j * 2 + 0) * 2 + ch) * kN + k));
                 mad_wide(sb, d, __ldg(key + ((j * 2 + 1) * 2 + ch) * kN + k));
             }
-            const uint32_t ca = negmod(reduce64(sa, cc.q, cc.barrett), cc.q);
-            const uint32_t bv = __ldg(sout + sout_idx(row, 1 * 2 + ch, sig[k], rows));
-            const uint32_t cb = addmod(bv, negmod(reduce64(sb, cc.q, cc.barrett), cc.q), cc.q);
-            atomicAdd(acc_a + k, (unsigned long long)ca);
-            atomicAdd(acc_b + k, (unsigned long long)cb);
+            const uint32_t bv = sout[sout_idx(row, 1 * 2 + ch, sig[k], rows)];
+            cbv[it] = addmod(bv, negmod(reduce64(sb, cc.q, cc.barrett), cc.q), cc.q);
+            sout[sout_idx(row, 0 * 2 + ch, k, rows)] = negmod(reduce64(sa, cc.q, cc.barrett), cc.q);
         }
+        __syncthreads();   // every gather of this prime's b part is done
+#pragma unroll
+        for (int it = 0; it < kPerThreadG; it++) sout[sout_idx(row, 1 * 2 + ch, tid + it * kNttThreads, rows)] = cbv[it];
     }
 }
 
-// result[r][comp][ch][k] = (output[0] + accumulated giant steps) mod q; the
-// accumulator is cleared for the next query of the slot.
-__global__ void k_giant_finish(const uint32_t* __restrict__ sout, unsigned long long* __restrict__ acc,
-                               uint32_t* __restrict__ result, int R, int N2, Batch bt) {
+// result[r][comp][ch][k] = (output[0] + the N2 - 1 giant-step contributions)
+// mod q: the sum of the N2 rows of sub-database r after k_giant_fused.
+__global__ void k_giant_finish(const uint32_t* __restrict__ sout, uint32_t* __restrict__ result, int R, int N2,
+                               Batch bt) {
     const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= (long)R * 4 * kN) return;
     sout = shifted(sout, ws_off(bt));
-    acc = shifted(acc, ws_off(bt));
     result = shifted(result, ws_off(bt));
     const int k = (int)(idx % kN);
     const int cc_ = (int)((idx / kN) % 4);      // comp * 2 + ch
     const int r = (int)(idx / (4 * kN));
     const ChanConst q = c_dev.ch[cc_ & 1];
-    const uint64_t v = (uint64_t)sout[sout_idx(r * N2, cc_, k, R * N2)] + acc[idx];
-    acc[idx] = 0;
+    uint64_t v = 0;
+    for (int c = 0; c < N2; c++) v += sout[sout_idx(r * N2 + c, cc_, k, R * N2)];
     result[idx] = reduce64(v, q.q, q.barrett);
 }
 
@@ -210,7 +209,7 @@ namespace kspir {
 //   a' = -sum_d dig_d * key[d].a,  b' = NTT(temp.b) - sum_d dig_d * key[d].b
 //   out[j] = INTT(a', b') + c2
 constexpr int kPackPolys = 5;    // ell = 4 digits + temp.b
-constexpr int kPackSmem = kN * 8 + kPackPolys * kN * 4;
+constexpr int kPackSmem = kN * 8 + kPackPolys * kPadN * 4;
 
 template <int ELL>
 __global__ void __launch_bounds__(kNttThreads) k_pack_fused(const uint32_t* __restrict__ in,
@@ -231,7 +230,7 @@ __global__ void __launch_bounds__(kNttThreads) k_pack_fused(const uint32_t* __re
     const uint32_t q = c_dev.ch[ch].q;
     stage_twiddles(tws, tabs, ch, NTT_FWD);
     // X^I c at position p of polynomial (comp, prime)
-    auto shifted = [&](int comp, int pch, int p) -> uint32_t {
+    auto cshift = [&](int comp, int pch, int p) -> uint32_t {
         const int s = p - I;
         const uint32_t qq = pch ? kQ2 : kQ1;
         return s >= 0 ? __ldg(cc + (comp * 2 + pch) * kN + s) : negmod(__ldg(cc + (comp * 2 + pch) * kN + s + kN), qq);
@@ -242,24 +241,25 @@ __global__ void __launch_bounds__(kNttThreads) k_pack_fused(const uint32_t* __re
         const int k = tid + it * kNttThreads;
 #pragma unroll
         for (int comp = 0; comp < 2; comp++)
-            c2v[it][comp] = addmod(shifted(comp, ch, k), __ldg(r0 + (comp * 2 + ch) * kN + k), q);
+            c2v[it][comp] = addmod(cshift(comp, ch, k), __ldg(r0 + (comp * 2 + ch) * kN + k), q);
         bool neg;
         const int src = auto_src(k, ginv, &neg);
         uint32_t ra[2];
 #pragma unroll
         for (int pch = 0; pch < 2; pch++) {
             const uint32_t qq = pch ? kQ2 : kQ1;
-            const uint32_t v = submod(__ldg(r0 + (0 * 2 + pch) * kN + src), shifted(0, pch, src), qq);
+            const uint32_t v = submod(__ldg(r0 + (0 * 2 + pch) * kN + src), cshift(0, pch, src), qq);
             ra[pch] = neg ? negmod(v, qq) : v;
         }
         int32_t dig[kMaxEll];
         decompose_b(crt_compose_res(ra[0], ra[1]), kCrtMod, g, dig);
+        const int pk = pidx(tid) + it * kPadStep;
 #pragma unroll
-        for (int d = 0; d < ELL; d++) P[d * kN + k] = signed_to_res(dig[d], q);
-        const uint32_t vb = submod(__ldg(r0 + (1 * 2 + ch) * kN + src), shifted(1, ch, src), q);
-        P[ELL * kN + k] = neg ? negmod(vb, q) : vb;
+        for (int d = 0; d < ELL; d++) P[d * kPadN + pk] = signed_to_res(dig[d], q);
+        const uint32_t vb = submod(__ldg(r0 + (1 * 2 + ch) * kN + src), cshift(1, ch, src), q);
+        P[ELL * kPadN + pk] = neg ? negmod(vb, q) : vb;
     }
-    cta_ntt_forward_m<ELL + 1>(P, kN, tws, ch);
+    cta_ntt_forward_m<ELL + 1>(P, kPadN, tws, ch);
     const ChanConst cq = c_dev.ch[ch];
 #pragma unroll
     for (int it = 0; it < kPerThreadG; it++) {
@@ -267,23 +267,24 @@ __global__ void __launch_bounds__(kNttThreads) k_pack_fused(const uint32_t* __re
         uint64_t sa = 0, sb = 0;
 #pragma unroll
         for (int d = 0; d < ELL; d++) {
-            const uint32_t dv = P[d * kN + k];
+            const uint32_t dv = P[d * kPadN + pidx(tid) + it * kPadStep];
             mad_wide(sa, dv, __ldg(key + ((d * 2 + 0) * 2 + ch) * kN + k));
             mad_wide(sb, dv, __ldg(key + ((d * 2 + 1) * 2 + ch) * kN + k));
         }
         const uint32_t a2 = negmod(reduce64(sa, cq.q, cq.barrett), q);
-        const uint32_t b2 = submod(P[ELL * kN + k], reduce64(sb, cq.q, cq.barrett), q);
-        P[k] = a2;            // only this thread reads index k of these rows
-        P[kN + k] = b2;
+        const int pk = pidx(tid) + it * kPadStep;
+        const uint32_t b2 = submod(P[ELL * kPadN + pk], reduce64(sb, cq.q, cq.barrett), q);
+        P[pk] = a2;            // only this thread reads index k of these rows
+        P[kPadN + pk] = b2;
     }
     stage_twiddles(tws, tabs, ch, NTT_INV);   // the forward transforms ended with a barrier
-    cta_ntt_inverse_m<2>(P, kN, tws, ch);
+    cta_ntt_inverse_m<2>(P, kPadN, tws, ch);
 #pragma unroll
     for (int it = 0; it < kPerThreadG; it++) {
         const int k = tid + it * kNttThreads;
 #pragma unroll
         for (int comp = 0; comp < 2; comp++)
-            out[((size_t)j * 4 + comp * 2 + ch) * kN + k] = addmod(P[comp * kN + k], c2v[it][comp], q);
+            out[((size_t)j * 4 + comp * 2 + ch) * kN + k] = addmod(P[comp * kPadN + pidx(tid) + it * kPadStep], c2v[it][comp], q);
     }
 }
 
@@ -293,7 +294,7 @@ __global__ void __launch_bounds__(kNttThreads) k_pack_fused(const uint32_t* __re
 //   INTT(first_dim) (both primes, to compose) -> decompose_rlwe (2 ell rows)
 //   -> row transforms -> init + sum_row row * rgsw[row] -> INTT
 constexpr int kExtPolys = 4;
-constexpr int kExtSmem = kN * 8 + kExtPolys * kN * 4;
+constexpr int kExtSmem = kN * 8 + kExtPolys * kPadN * 4;
 
 template <int ELL>
 __global__ void __launch_bounds__(kNttThreads) k_ext_fused(const uint32_t* __restrict__ first_dim,
@@ -321,28 +322,24 @@ __global__ void __launch_bounds__(kNttThreads) k_ext_fused(const uint32_t* __res
         stage_twiddles(tws, tabs, pch, NTT_INV);
 #pragma unroll
         for (int comp = 0; comp < 2; comp++) {
-            const uint4* src = reinterpret_cast<const uint4*>(fd + (comp * 2 + pch) * kN);
-            uint4* dst = reinterpret_cast<uint4*>(P + (comp * 2 + pch) * kN);
-#pragma unroll
-            for (int k = tid; k < kN / 4; k += kNttThreads) dst[k] = __ldg(src + k);
+            poly_to_smem(P + (comp * 2 + pch) * kPadN, fd + (comp * 2 + pch) * kN);
         }
-        cta_ntt_inverse_m<2>(P + pch * kN, 2 * kN, tws, pch);   // a and b of this prime
+        cta_ntt_inverse_m<2>(P + pch * kPadN, 2 * kPadN, tws, pch);   // a and b of this prime
     }
     if (coef_out && ch == 0) {
-        uint4* dst = reinterpret_cast<uint4*>(coef_out + (size_t)r * 4 * kN);
-        const uint4* src = reinterpret_cast<const uint4*>(P);
 #pragma unroll
-        for (int k = tid; k < kN; k += kNttThreads) dst[k] = src[k];
+        for (int i = 0; i < 4; i++) poly_from_smem(coef_out + ((size_t)r * 4 + i) * kN, P + i * kPadN);
     }
     // signed digits of a and b (rows comp * ELL + t), residues of this prime
     uint32_t dres[kPerThreadG][2 * ELL];
 #pragma unroll
     for (int it = 0; it < kPerThreadG; it++) {
-        const int k = tid + it * kNttThreads;
 #pragma unroll
         for (int comp = 0; comp < 2; comp++) {
             int32_t dig[kMaxEll];
-            decompose_signed(crt_compose_res(P[(comp * 2 + 0) * kN + k], P[(comp * 2 + 1) * kN + k]), kCrtMod, g, dig);
+            const int pk = pidx(tid) + it * kPadStep;
+            decompose_signed(crt_compose_res(P[(comp * 2 + 0) * kPadN + pk], P[(comp * 2 + 1) * kPadN + pk]), kCrtMod, g,
+                             dig);
 #pragma unroll
             for (int t = 0; t < ELL; t++) dres[it][comp * ELL + t] = signed_to_res(dig[t], ch ? kQ2 : kQ1);
         }
@@ -351,9 +348,9 @@ __global__ void __launch_bounds__(kNttThreads) k_ext_fused(const uint32_t* __res
 #pragma unroll
     for (int it = 0; it < kPerThreadG; it++)
 #pragma unroll
-        for (int row = 0; row < 2 * ELL; row++) P[row * kN + tid + it * kNttThreads] = dres[it][row];
+        for (int row = 0; row < 2 * ELL; row++) P[row * kPadN + pidx(tid) + it * kPadStep] = dres[it][row];
     stage_twiddles(tws, tabs, ch, NTT_FWD);
-    cta_ntt_forward_m<2 * ELL>(P, kN, tws, ch);
+    cta_ntt_forward_m<2 * ELL>(P, kPadN, tws, ch);
     const ChanConst cq = c_dev.ch[ch];
     uint32_t outv[kPerThreadG][2];
 #pragma unroll
@@ -364,24 +361,25 @@ __global__ void __launch_bounds__(kNttThreads) k_ext_fused(const uint32_t* __res
             uint64_t s = 0;
 #pragma unroll
             for (int row = 0; row < 2 * ELL; row++)
-                mad_wide(s, P[row * kN + k], __ldg(rgsw + ((row * 2 + comp) * 2 + ch) * kN + k));
+                mad_wide(s, P[row * kPadN + pidx(tid) + it * kPadStep], __ldg(rgsw + ((row * 2 + comp) * 2 + ch) * kN + k));
             const uint32_t m = reduce64(s, cq.q, cq.barrett);
             outv[it][comp] = init ? addmod(__ldg(init + ((size_t)r * 4 + comp * 2 + ch) * kN + k), m, cq.q) : m;
         }
     }
 #pragma unroll
     for (int it = 0; it < kPerThreadG; it++) {
-        const int k = tid + it * kNttThreads;
-        P[k] = outv[it][0];        // only this thread reads index k of rows 0, 1
-        P[kN + k] = outv[it][1];
+        const int pk = pidx(tid) + it * kPadStep;
+        P[pk] = outv[it][0];        // only this thread reads this slot of rows 0, 1
+        P[kPadN + pk] = outv[it][1];
     }
     stage_twiddles(tws, tabs, ch, NTT_INV);   // the forward transforms ended with a barrier
-    cta_ntt_inverse_m<2>(P, kN, tws, ch);
+    cta_ntt_inverse_m<2>(P, kPadN, tws, ch);
 #pragma unroll
     for (int it = 0; it < kPerThreadG; it++) {
         const int k = tid + it * kNttThreads;
 #pragma unroll
-        for (int comp = 0; comp < 2; comp++) ext[((size_t)r * 4 + comp * 2 + ch) * kN + k] = P[comp * kN + k];
+        for (int comp = 0; comp < 2; comp++)
+            ext[((size_t)r * 4 + comp * 2 + ch) * kN + k] = P[comp * kPadN + pidx(tid) + it * kPadStep];
     }
 }
 

@@ -17,8 +17,8 @@ struct NttJob {
     int32_t dst_stride;
 };
 
-// dynamic shared memory: 16 KiB polynomial + 32 KiB twiddles
-constexpr int kNttJobSmem = kN * 4 + kN * 8;
+// dynamic shared memory: 32 KiB twiddles + one padded polynomial
+constexpr int kNttJobSmem = kN * 8 + kPadN * 4;
 
 template <bool INVERSE>
 __global__ void __launch_bounds__(kNttThreads) k_ntt_jobs(const NttJob* __restrict__ jobs, NttTables tabs, Batch bt) {
@@ -29,18 +29,13 @@ __global__ void __launch_bounds__(kNttThreads) k_ntt_jobs(const NttJob* __restri
     jb.src = shifted(jb.src, ws_off(bt));   // job lists address workspace slot 0
     jb.dst = shifted(jb.dst, ws_off(bt));
     stage_twiddles(tws, tabs, jb.ch, INVERSE ? NTT_INV : NTT_FWD);
-    const uint4* src4 = reinterpret_cast<const uint4*>(jb.src);
-    uint4* s4 = reinterpret_cast<uint4*>(s);
-#pragma unroll
-    for (int k = threadIdx.x; k < kN / 4; k += kNttThreads) s4[k] = src4[k];
+    poly_to_smem(s, jb.src);
     if (INVERSE) cta_ntt_inverse(s, tws, jb.ch);
     else cta_ntt_forward(s, tws, jb.ch);
     if (jb.dst_stride == 1) {
-        uint4* dst4 = reinterpret_cast<uint4*>(jb.dst);
-#pragma unroll
-        for (int k = threadIdx.x; k < kN / 4; k += kNttThreads) dst4[k] = s4[k];
+        poly_from_smem(jb.dst, s);
     } else {
-        for (int k = threadIdx.x; k < kN; k += kNttThreads) jb.dst[(size_t)k * jb.dst_stride] = s[k];
+        for (int k = threadIdx.x; k < kN; k += kNttThreads) jb.dst[(size_t)k * jb.dst_stride] = s[pidx(k)];
     }
 }
 

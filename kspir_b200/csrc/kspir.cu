@@ -201,6 +201,7 @@ struct kspir_ctx {
     cudaStream_t capture = nullptr;
     bool use_graphs = true;
     std::map<int, int> scan_choice;   // queries per launch -> ScanKind
+    int last_kind = 0;                // scan variant of the last answer launch
     // events of recent launches: ring[i][0..5] brackets baby / scan / giant / ext / packing
     std::vector<std::array<cudaEvent_t, 6>> ring;
     std::vector<int> ring_nq;
@@ -272,7 +273,6 @@ Workspace ws_host(const kspir_ctx* c, int s) {
     w.ecoef = host_shift(w.ecoef, off);
     w.ext = host_shift(w.ext, off);
     w.ext2 = host_shift(w.ext2, off);
-    w.gacc = host_shift(w.gacc, off);
     w.err += (size_t)s * kErrStride;
     return w;
 }
@@ -319,7 +319,7 @@ int init_constants(kspir_ctx* c) {
     // per prime; bsMod uses HEXL's minimal primitive root
     const uint64_t root_crt = 3375402822066082ull;
     const uint64_t roots[3] = {root_crt % kQ1, root_crt % kQ2, h_min_root(kBsMod)};
-    // per channel uint2 [2][N]: {psi^brv(k), Shoup} then {psi^-brv(k), Shoup}
+    // per channel uint2 [2][N]: {psi^brv(k), Shoup} then {psi^-brv(k), Shoup}, k-major order
     std::vector<uint32_t> tw(3 * 4 * kN);
     for (int ch = 0; ch < 3; ch++) {
         const uint64_t q = qs[ch], psi = roots[ch], pinv = h_invmod(psi, q);
@@ -327,10 +327,11 @@ int init_constants(kspir_ctx* c) {
         for (int k = 0; k < kN; k++) {
             uint32_t e = h_bitrev12(k);
             const uint32_t w = (uint32_t)h_powmod(psi, e, q), iw = (uint32_t)h_powmod(pinv, e, q);
-            t[2 * k] = w;
-            t[2 * k + 1] = shoup32(w, (uint32_t)q);
-            t[2 * kN + 2 * k] = iw;
-            t[2 * kN + 2 * k + 1] = shoup32(iw, (uint32_t)q);
+            const int pos = tw_layout_pos(k);   // the transforms read the k-major layout
+            t[2 * pos] = w;
+            t[2 * pos + 1] = shoup32(w, (uint32_t)q);
+            t[2 * kN + 2 * pos] = iw;
+            t[2 * kN + 2 * pos + 1] = shoup32(iw, (uint32_t)q);
         }
     }
     KS_CUDA(c, cudaMalloc(&c->tw, tw.size() * 4));
@@ -376,7 +377,6 @@ int init_workspaces(kspir_ctx* c) {
         {(void**)&w.ecoef, (size_t)r * 4 * P},
         {(void**)&w.ext, (size_t)r * 4 * P},
         {(void**)&w.ext2, (size_t)half * 4 * P},
-        {(void**)&w.gacc, (size_t)r * 4 * kN * 8},
     };
     size_t total = 0;
     for (auto& pt : parts) total = align_up(total, 256) + pt.bytes;
@@ -462,15 +462,17 @@ void enqueue_baby(kspir_ctx* c, int slot0, int nq, cudaStream_t st) {
     a1.dig = w.dig0; a1.srcB = w.qbn; a1.srcBbs = w.qbbs; a1.perms = c->perms; a1.sigma = c->sigma_baby;
     a1.cipherbuf = w.cipherbuf; a1.interA = w.interA; a1.interB = w.interB; a1.inter_bs = w.inter_bs;
     a1.N1 = c->N1; a1.col_base = 1; a1.inter_idx = c->N1h - 2;
-    if (c->N1h - 1 > 0)
-        k_baby_rot<3><<<dim3((c->N1h - 1) * 4, nq), kNttThreads, kBabySmem, st>>>(a1, c->keys0, c->ntabs, bt);
+    auto rot = [&](const BabyArgs& args, int nrot) {
+        if (nrot > 0) k_baby_rot<3><<<dim3(nrot * 4, nq), kNttThreads, kBabySmem, st>>>(args, c->keys0, c->ntabs, bt);
+    };
+    rot(a1, c->N1h - 1);
     k_ntt_jobs<true><<<dim3(2, nq), kNttThreads, kNttJobSmem, st>>>(c->jobs + c->seg_inter, c->ntabs, bt);
     k_inter_decomp<<<dim3(kN / 256, nq), 256, 0, st>>>(w, c->gad.baby, bt);
     k_ntt_jobs<false><<<dim3(9, nq), kNttThreads, kNttJobSmem, st>>>(c->jobs + c->seg_dig1, c->ntabs, bt);
     BabyArgs a2 = a1;
     a2.dig = w.dig1; a2.srcB = w.interB; a2.srcBbs = w.inter_bs + kN;
     a2.col_base = c->N1h; a2.inter_idx = -1;
-    k_baby_rot<3><<<dim3(c->N1h * 4, nq), kNttThreads, kBabySmem, st>>>(a2, c->keys0, c->ntabs, bt);
+    rot(a2, c->N1h);
 }
 
 int scan_kind_for(kspir_ctx* c, int nq) {
@@ -487,8 +489,8 @@ template <int BT>
 void launch_scan_mma(kspir_ctx* c, int slot0, int nq, cudaStream_t st) {
     using C = MmaCfg<BT>;
     const int QT = (nq + BT - 1) / BT;
-    k_qop_split<BT><<<blocks_for((long)kN * QT * 2 * BT * 8, 256), 256, 0, st>>>(c->ws0.cipherbuf, c->ws_bytes, slot0,
-                                                                                  nq, QT, c->qop);
+    k_qop_split<BT><<<blocks_for((long)kN * QT * BT * 8, 256), 256, 0, st>>>(c->ws0.cipherbuf, c->ws_bytes, slot0, nq,
+                                                                              QT, c->qop);
     ScanMmaArgs a;
     a.dbop = c->dbop;
     a.qop = c->qop;
@@ -534,8 +536,8 @@ void enqueue_giant(kspir_ctx* c, int slot0, int nq, cudaStream_t st) {
     const int R = c->p.r;
     if (c->N2 > 1)
         k_giant_fused<2><<<dim3(R * (c->N2 - 1), nq), kNttThreads, kGiantSmem, st>>>(
-            w.sout, c->keys0.giant, c->sigma_giant, w.gacc, c->N1, c->ntabs, c->gad.giant, R, bt);
-    k_giant_finish<<<dim3(blocks_for((long)R * 4 * kN, 256), nq), 256, 0, st>>>(w.sout, w.gacc, w.result, R, c->N2, bt);
+            w.sout, c->keys0.giant, c->sigma_giant, c->N1, c->ntabs, c->gad.giant, R, bt);
+    k_giant_finish<<<dim3(blocks_for((long)R * 4 * kN, 256), nq), 256, 0, st>>>(w.sout, w.result, R, c->N2, bt);
 }
 
 // external products of `count` first-dimension results (result -> ext);
@@ -605,6 +607,7 @@ int enqueue_answer(kspir_ctx* c, int slot0, int nq, const int* clients, cudaStre
     for (int i = 0; i < nq; i++) cl.id[i] = clients[i];
     k_set_clients<<<1, kMaxBatch, 0, st>>>(c->client_of, slot0, cl);
     const int kind = scan_kind_for(c, nq);
+    c->last_kind = kind;
     const int slot = (int)(c->enqueues % kTimingRing);
     auto& ev = c->ring[slot];
     if (c->use_graphs) {
@@ -668,9 +671,7 @@ int check_ready(kspir_ctx* c, int client) {
 }
 
 // Waits for the context stream and reports (then clears) the error words of
-// slots [slot0, slot0 + nq).  After a timed-out launch the giant-step
-// accumulators of those slots are cleared too (a partial launch leaves them
-// dirty).
+// slots [slot0, slot0 + nq).
 int finish(kspir_ctx* c, int slot0, int nq) {
     KS_CUDA(c, cudaStreamSynchronize(c->stream));
     std::vector<int> e((size_t)nq * kErrStride);
@@ -679,8 +680,6 @@ int finish(kspir_ctx* c, int slot0, int nq) {
     for (int q = 0; q < nq; q++) herr |= e[(size_t)q * kErrStride];
     if (herr) {
         cudaMemsetAsync(c->errs + (size_t)slot0 * kErrStride, 0, e.size() * 4, c->stream);
-        for (int q = 0; q < nq; q++)
-            cudaMemsetAsync(ws_host(c, slot0 + q).gacc, 0, (size_t)c->p.r * 4 * kN * 8, c->stream);
         cudaStreamSynchronize(c->stream);
         return set_err(c, KSPIR_ERR_TIMEOUT, "a bounded device wait gave up (code " + std::to_string(herr) + ")");
     }
@@ -748,6 +747,9 @@ int kspir_ctx_create(int device, const kspir_params* params, kspir_ctx** out) {
     KS_CUDA(c.get(), cudaStreamCreateWithFlags(&c->capture, cudaStreamNonBlocking));
     if (const char* e = getenv("KSPIR_NO_GRAPHS")) c->use_graphs = !(e[0] == '1');
     KS_CUDA(c.get(), cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device));
+    KS_CUDA(c.get(), cudaFuncSetAttribute(k_baby_rot<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBabySmem));
+    KS_CUDA(c.get(), cudaFuncSetAttribute(k_ntt_jobs<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kNttJobSmem));
+    KS_CUDA(c.get(), cudaFuncSetAttribute(k_ntt_jobs<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kNttJobSmem));
     KS_CUDA(c.get(), cudaFuncSetAttribute(k_giant_fused<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGiantSmem));
     KS_CUDA(c.get(), cudaFuncSetAttribute(k_ext_fused<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kExtSmem));
     KS_CUDA(c.get(), cudaFuncSetAttribute(k_pack_fused<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, kPackSmem));
@@ -1181,6 +1183,14 @@ int kspir_fetch_stage_slot(kspir_ctx* c, int slot, int stage, uint64_t* out, siz
     if (words != polys * kN) return set_err(c, KSPIR_ERR_INVALID_ARG, "size mismatch");
     uint64_t* tmp = nullptr;
     uint32_t* flat = nullptr;
+    if (stage == KSPIR_STAGE_SCAN) {
+        // the giant steps overwrite rows c >= 1 of the scan output: scan the
+        // slot's rotations again, with the variant the last launch used
+        enqueue_scan(c, slot, 1, c->last_kind, st);
+        KS_CUDA(c, cudaGetLastError());
+        int rc = finish(c, slot, 1);
+        if (rc) return rc;
+    }
     KS_CUDA(c, cudaMalloc(&tmp, words * 8));
     cudaError_t e = cudaSuccess;
     if (stage == KSPIR_STAGE_SCAN) {
@@ -1264,11 +1274,12 @@ __global__ void k_na_twiddles(uint32_t* tw, uint32_t q0, uint32_t q1, uint32_t q
         };
         uint32_t w = pw(e);
         uint32_t iw = pw((2 * kN - e) % (2 * kN));   // psi^(2N) = 1
-        uint32_t* t = tw + (size_t)ch * 4 * kN;   // uint2 [2][N]
-        t[2 * k] = w;
-        t[2 * k + 1] = (uint32_t)(((uint64_t)w << 32) / q);
-        t[2 * kN + 2 * k] = iw;
-        t[2 * kN + 2 * k + 1] = (uint32_t)(((uint64_t)iw << 32) / q);
+        uint32_t* t = tw + (size_t)ch * 4 * kN;   // uint2 [2][N], k-major layout
+        const int pos = tw_layout_pos(k);
+        t[2 * pos] = w;
+        t[2 * pos + 1] = (uint32_t)(((uint64_t)w << 32) / q);
+        t[2 * kN + 2 * pos] = iw;
+        t[2 * kN + 2 * pos + 1] = (uint32_t)(((uint64_t)iw << 32) / q);
     }
 }
 
@@ -1316,6 +1327,10 @@ int na_setup(int device, cudaStream_t st) {
     if (d.ready) return KSPIR_OK;
     if (cudaGetSymbolAddress((void**)&d.scratch, g_na_scratch) != cudaSuccess) return KSPIR_ERR_CUDA;
     if (cudaGetSymbolAddress((void**)&d.tw, g_na_tw) != cudaSuccess) return KSPIR_ERR_CUDA;
+    if (cudaFuncSetAttribute(k_ntt_jobs<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kNttJobSmem) != cudaSuccess ||
+        cudaFuncSetAttribute(k_ntt_jobs<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kNttJobSmem) != cudaSuccess ||
+        cudaFuncSetAttribute(k_ext_mac_intt, cudaFuncAttributeMaxDynamicSharedMemorySize, kMacSmem) != cudaSuccess)
+        return KSPIR_ERR_CUDA;
     DevConst dc{};
     const uint32_t qs[3] = {kQ1, kQ2, kBsMod};
     for (int ch = 0; ch < 3; ch++) {

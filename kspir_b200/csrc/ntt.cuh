@@ -13,8 +13,19 @@
 // twiddles.  The twiddles of one direction of one channel are staged into
 // shared memory first (stage_twiddles) as uint2 {w, floor(w 2^32 / q)}.
 //
-// Device table layout per channel: uint2 tw[2][N]; tw[0][k] = psi^brv(k),
-// tw[1][k] = psi^-brv(k), each with its Shoup companion.
+// Shared-memory layout.  A polynomial occupies kPadN words: coefficient (or
+// slot) i sits at pidx(i) = i + 4 (i / 32).  With that padding the element
+// pattern of every pass (strides 512, 64 and 8 words, then eight contiguous
+// words read as two 16-byte vectors) hits 32 distinct banks per warp access,
+// and the position of element t of a thread's unit is pidx(base) plus a
+// compile-time offset, so the padding costs no address arithmetic.
+//
+// Device table layout per channel: uint2 tw[2][N] (forward, inverse), entry
+// m + i of level m = 2^l (root^brv(m + i) and its Shoup companion) stored
+// "k-major" within its pass: for the pass p = l / 3 with unit count
+// m0 = 8^p, level 2 m0 index 2 i0 + k sits at 2 m0 + k m0 + i0 and level 4 m0
+// index 4 i0 + k at 4 m0 + k m0 + i0, so the twiddles a warp reads in one
+// load are consecutive (tw_layout_pos gives the position).
 #pragma once
 
 #include "common.cuh"
@@ -22,6 +33,21 @@
 namespace kspir {
 
 constexpr int kNttThreads = 512;
+constexpr int kPadN = kN + kN / 8;      // padded length of a polynomial in shared memory
+constexpr int kPadStep = 576;           // pidx(i + 512) - pidx(i)
+
+__host__ __device__ __forceinline__ int pidx(int i) { return i + ((i >> 5) << 2); }
+
+// position of twiddle-table index idx (1 <= idx < N) in the k-major layout
+__host__ __device__ inline int tw_layout_pos(int idx) {
+    if (idx <= 0) return 0;
+    int l = 0;
+    while ((2 << l) <= idx) l++;
+    const int m = 1 << l, i = idx - m, r = l % 3, m0 = 1 << (3 * (l / 3));
+    if (r == 0) return idx;
+    if (r == 1) return m + (i & 1) * m0 + (i >> 1);
+    return m + (i & 3) * m0 + (i >> 2);
+}
 
 struct NttTables {
     const uint2* tw[CH_COUNT];   // [2][N] per channel
@@ -38,25 +64,32 @@ __device__ __forceinline__ void stage_twiddles(uint2* tws, const NttTables& tabs
     for (int k = threadIdx.x; k < kN / 2; k += kNttThreads) s[k] = __ldg(g + k);
 }
 
-// the 8 elements of a radix-8 unit; contiguous (one 32-byte run) when q8 == 1
-__device__ __forceinline__ void load8(const uint32_t* s, int base, int q8, uint32_t* x) {
-    if (q8 == 1) {
-        const uint4 a = *reinterpret_cast<const uint4*>(s + base);
-        const uint4 b = *reinterpret_cast<const uint4*>(s + base + 4);
-        x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w; x[4] = b.x; x[5] = b.y; x[6] = b.z; x[7] = b.w;
+// offset of element t of a radix-8 unit from pidx(unit base), pass P
+template <int P>
+__device__ __forceinline__ constexpr int unit_off(int t) {
+    return P == 0 ? 576 * t : P == 1 ? 72 * t : P == 2 ? 8 * t + 4 * (t >> 2) : t;
+}
+
+template <int P>
+__device__ __forceinline__ void unit_load(const uint32_t* s, int b, uint32_t* x) {
+    if (P == 3) {
+        const uint4 a = *reinterpret_cast<const uint4*>(s + b);
+        const uint4 c = *reinterpret_cast<const uint4*>(s + b + 4);
+        x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w; x[4] = c.x; x[5] = c.y; x[6] = c.z; x[7] = c.w;
     } else {
 #pragma unroll
-        for (int t = 0; t < 8; t++) x[t] = s[base + t * q8];
+        for (int t = 0; t < 8; t++) x[t] = s[b + unit_off<P>(t)];
     }
 }
 
-__device__ __forceinline__ void store8(uint32_t* s, int base, int q8, const uint32_t* x) {
-    if (q8 == 1) {
-        *reinterpret_cast<uint4*>(s + base) = make_uint4(x[0], x[1], x[2], x[3]);
-        *reinterpret_cast<uint4*>(s + base + 4) = make_uint4(x[4], x[5], x[6], x[7]);
+template <int P>
+__device__ __forceinline__ void unit_store(uint32_t* s, int b, const uint32_t* x) {
+    if (P == 3) {
+        *reinterpret_cast<uint4*>(s + b) = make_uint4(x[0], x[1], x[2], x[3]);
+        *reinterpret_cast<uint4*>(s + b + 4) = make_uint4(x[4], x[5], x[6], x[7]);
     } else {
 #pragma unroll
-        for (int t = 0; t < 8; t++) s[base + t * q8] = x[t];
+        for (int t = 0; t < 8; t++) s[b + unit_off<P>(t)] = x[t];
     }
 }
 
@@ -75,178 +108,131 @@ __device__ __forceinline__ void inv_bfly(uint32_t& X, uint32_t& Y, uint2 w, uint
     Y = d;
 }
 
-// Forward transform of s[0..N) in place; input in [0, 4q) (canonical inputs are
-// fine), output canonical.  tws holds the forward twiddles of `ch`.
-__device__ __forceinline__ void cta_ntt_forward(uint32_t* s, const uint2* tws, int ch) {
-    const uint32_t q = c_dev.ch[ch].q, q2 = c_dev.ch[ch].two_q;
-    const int u = threadIdx.x;
-    __syncthreads();
+// One forward pass over M polynomials (s + m * stride): thread u's radix-8 unit
+// of each, three butterfly layers, no barrier inside (units are disjoint).
+template <int P, int M>
+__device__ __forceinline__ void fwd_pass(uint32_t* s, int stride, const uint2* tws, uint32_t q, uint32_t q2, int u) {
+    constexpr int lq = 9 - 3 * P, q8 = 1 << lq, m0 = 1 << (3 * P);
+    const int i0 = u >> lq, j = u & (q8 - 1);
+    const int b = pidx(i0 * 8 * q8 + j);
+    const uint2 wa = tws[m0 + i0];
+    const uint2 wb0 = tws[2 * m0 + i0], wb1 = tws[3 * m0 + i0];
+    const uint2 wc0 = tws[4 * m0 + i0], wc1 = tws[5 * m0 + i0], wc2 = tws[6 * m0 + i0], wc3 = tws[7 * m0 + i0];
+    uint32_t x[M][8];
 #pragma unroll
-    for (int p = 0; p < 4; p++) {
-        const int lq = 9 - 3 * p;             // log2 of the element stride within a unit
-        const int q8 = 1 << lq;
-        const int m0 = 1 << (3 * p);
-        const int i0 = u >> lq, j = u & (q8 - 1);
-        const int base = i0 * 8 * q8 + j;
-        uint32_t x[8];
-        load8(s, base, q8, x);
-        const uint2 wa = tws[m0 + i0];
-        const uint2 wb0 = tws[2 * m0 + 2 * i0], wb1 = tws[2 * m0 + 2 * i0 + 1];
-        const uint2 wc0 = tws[4 * m0 + 4 * i0], wc1 = tws[4 * m0 + 4 * i0 + 1];
-        const uint2 wc2 = tws[4 * m0 + 4 * i0 + 2], wc3 = tws[4 * m0 + 4 * i0 + 3];
+    for (int m = 0; m < M; m++) unit_load<P>(s + m * stride, b, x[m]);
 #pragma unroll
-        for (int t = 0; t < 4; t++) fwd_bfly(x[t], x[t + 4], wa, q, q2);
-        fwd_bfly(x[0], x[2], wb0, q, q2);
-        fwd_bfly(x[1], x[3], wb0, q, q2);
-        fwd_bfly(x[4], x[6], wb1, q, q2);
-        fwd_bfly(x[5], x[7], wb1, q, q2);
-        fwd_bfly(x[0], x[1], wc0, q, q2);
-        fwd_bfly(x[2], x[3], wc1, q, q2);
-        fwd_bfly(x[4], x[5], wc2, q, q2);
-        fwd_bfly(x[6], x[7], wc3, q, q2);
-        if (p == 3) {
+    for (int m = 0; m < M; m++) {
+#pragma unroll
+        for (int t = 0; t < 4; t++) fwd_bfly(x[m][t], x[m][t + 4], wa, q, q2);
+        fwd_bfly(x[m][0], x[m][2], wb0, q, q2);
+        fwd_bfly(x[m][1], x[m][3], wb0, q, q2);
+        fwd_bfly(x[m][4], x[m][6], wb1, q, q2);
+        fwd_bfly(x[m][5], x[m][7], wb1, q, q2);
+        fwd_bfly(x[m][0], x[m][1], wc0, q, q2);
+        fwd_bfly(x[m][2], x[m][3], wc1, q, q2);
+        fwd_bfly(x[m][4], x[m][5], wc2, q, q2);
+        fwd_bfly(x[m][6], x[m][7], wc3, q, q2);
+        if (P == 3) {
 #pragma unroll
             for (int t = 0; t < 8; t++) {
-                uint32_t v = x[t] >= q2 ? x[t] - q2 : x[t];
-                x[t] = v >= q ? v - q : v;
+                uint32_t v = x[m][t] >= q2 ? x[m][t] - q2 : x[m][t];
+                x[m][t] = v >= q ? v - q : v;
             }
         }
-        // the units of one pass are disjoint: write back without a barrier
-        store8(s, base, q8, x);
-        __syncthreads();
     }
+#pragma unroll
+    for (int m = 0; m < M; m++) unit_store<P>(s + m * stride, b, x[m]);
 }
 
-// Inverse transform of s[0..N) in place (includes N^-1); input in [0, 2q)
-// (canonical inputs are fine), output canonical.  tws holds the inverse
-// twiddles of `ch`.
-__device__ __forceinline__ void cta_ntt_inverse(uint32_t* s, const uint2* tws, int ch) {
-    const uint32_t q = c_dev.ch[ch].q, q2 = c_dev.ch[ch].two_q;
-    const uint32_t ni = c_dev.ch[ch].ninv, nip = c_dev.ch[ch].ninv_p;
-    const int u = threadIdx.x;
-    __syncthreads();
+template <int P, int M>
+__device__ __forceinline__ void inv_pass(uint32_t* s, int stride, const uint2* tws, uint32_t q, uint32_t q2,
+                                         uint32_t ni, uint32_t nip, int u) {
+    constexpr int lq = 9 - 3 * P, q8 = 1 << lq, m0 = 1 << (3 * P);
+    const int i0 = u >> lq, j = u & (q8 - 1);
+    const int b = pidx(i0 * 8 * q8 + j);
+    const uint2 wa = tws[m0 + i0];
+    const uint2 wb0 = tws[2 * m0 + i0], wb1 = tws[3 * m0 + i0];
+    const uint2 wc0 = tws[4 * m0 + i0], wc1 = tws[5 * m0 + i0], wc2 = tws[6 * m0 + i0], wc3 = tws[7 * m0 + i0];
+    uint32_t x[M][8];
 #pragma unroll
-    for (int p = 3; p >= 0; p--) {
-        const int lq = 9 - 3 * p;
-        const int q8 = 1 << lq;
-        const int m0 = 1 << (3 * p);
-        const int i0 = u >> lq, j = u & (q8 - 1);
-        const int base = i0 * 8 * q8 + j;
-        uint32_t x[8];
-        load8(s, base, q8, x);
-        const uint2 wa = tws[m0 + i0];
-        const uint2 wb0 = tws[2 * m0 + 2 * i0], wb1 = tws[2 * m0 + 2 * i0 + 1];
-        const uint2 wc0 = tws[4 * m0 + 4 * i0], wc1 = tws[4 * m0 + 4 * i0 + 1];
-        const uint2 wc2 = tws[4 * m0 + 4 * i0 + 2], wc3 = tws[4 * m0 + 4 * i0 + 3];
-        inv_bfly(x[0], x[1], wc0, q, q2);
-        inv_bfly(x[2], x[3], wc1, q, q2);
-        inv_bfly(x[4], x[5], wc2, q, q2);
-        inv_bfly(x[6], x[7], wc3, q, q2);
-        inv_bfly(x[0], x[2], wb0, q, q2);
-        inv_bfly(x[1], x[3], wb0, q, q2);
-        inv_bfly(x[4], x[6], wb1, q, q2);
-        inv_bfly(x[5], x[7], wb1, q, q2);
+    for (int m = 0; m < M; m++) unit_load<P>(s + m * stride, b, x[m]);
 #pragma unroll
-        for (int t = 0; t < 4; t++) inv_bfly(x[t], x[t + 4], wa, q, q2);
-        if (p == 0) {
+    for (int m = 0; m < M; m++) {
+        inv_bfly(x[m][0], x[m][1], wc0, q, q2);
+        inv_bfly(x[m][2], x[m][3], wc1, q, q2);
+        inv_bfly(x[m][4], x[m][5], wc2, q, q2);
+        inv_bfly(x[m][6], x[m][7], wc3, q, q2);
+        inv_bfly(x[m][0], x[m][2], wb0, q, q2);
+        inv_bfly(x[m][1], x[m][3], wb0, q, q2);
+        inv_bfly(x[m][4], x[m][6], wb1, q, q2);
+        inv_bfly(x[m][5], x[m][7], wb1, q, q2);
 #pragma unroll
-            for (int t = 0; t < 8; t++) x[t] = shoup_mul(x[t], ni, nip, q);
+        for (int t = 0; t < 4; t++) inv_bfly(x[m][t], x[m][t + 4], wa, q, q2);
+        if (P == 0) {
+#pragma unroll
+            for (int t = 0; t < 8; t++) x[m][t] = shoup_mul(x[m][t], ni, nip, q);
         }
-        store8(s, base, q8, x);
-        __syncthreads();
     }
+#pragma unroll
+    for (int m = 0; m < M; m++) unit_store<P>(s + m * stride, b, x[m]);
 }
 
-// M polynomials of the same channel, s + m * stride (m < M), transformed in
-// lockstep: one barrier per pass for all of them and M independent radix-8
-// units per thread, which hides the butterfly and shared-memory latencies a
-// single transform exposes.
+// Forward transforms of M padded polynomials s + m * stride of channel ch in
+// lockstep (one barrier per pass for all of them); input in [0, 4q)
+// (canonical inputs are fine), output canonical.  tws holds the forward
+// twiddles of ch.
 template <int M>
 __device__ __forceinline__ void cta_ntt_forward_m(uint32_t* s, int stride, const uint2* tws, int ch) {
     const uint32_t q = c_dev.ch[ch].q, q2 = c_dev.ch[ch].two_q;
     const int u = threadIdx.x;
     __syncthreads();
-#pragma unroll
-    for (int p = 0; p < 4; p++) {
-        const int lq = 9 - 3 * p;
-        const int q8 = 1 << lq;
-        const int m0 = 1 << (3 * p);
-        const int i0 = u >> lq, j = u & (q8 - 1);
-        const int base = i0 * 8 * q8 + j;
-        const uint2 wa = tws[m0 + i0];
-        const uint2 wb0 = tws[2 * m0 + 2 * i0], wb1 = tws[2 * m0 + 2 * i0 + 1];
-        const uint2 wc0 = tws[4 * m0 + 4 * i0], wc1 = tws[4 * m0 + 4 * i0 + 1];
-        const uint2 wc2 = tws[4 * m0 + 4 * i0 + 2], wc3 = tws[4 * m0 + 4 * i0 + 3];
-        uint32_t x[M][8];
-#pragma unroll
-        for (int m = 0; m < M; m++) load8(s + m * stride, base, q8, x[m]);
-#pragma unroll
-        for (int m = 0; m < M; m++) {
-#pragma unroll
-            for (int t = 0; t < 4; t++) fwd_bfly(x[m][t], x[m][t + 4], wa, q, q2);
-            fwd_bfly(x[m][0], x[m][2], wb0, q, q2);
-            fwd_bfly(x[m][1], x[m][3], wb0, q, q2);
-            fwd_bfly(x[m][4], x[m][6], wb1, q, q2);
-            fwd_bfly(x[m][5], x[m][7], wb1, q, q2);
-            fwd_bfly(x[m][0], x[m][1], wc0, q, q2);
-            fwd_bfly(x[m][2], x[m][3], wc1, q, q2);
-            fwd_bfly(x[m][4], x[m][5], wc2, q, q2);
-            fwd_bfly(x[m][6], x[m][7], wc3, q, q2);
-            if (p == 3) {
-#pragma unroll
-                for (int t = 0; t < 8; t++) {
-                    uint32_t v = x[m][t] >= q2 ? x[m][t] - q2 : x[m][t];
-                    x[m][t] = v >= q ? v - q : v;
-                }
-            }
-        }
-#pragma unroll
-        for (int m = 0; m < M; m++) store8(s + m * stride, base, q8, x[m]);
-        __syncthreads();
-    }
+    fwd_pass<0, M>(s, stride, tws, q, q2, u);
+    __syncthreads();
+    fwd_pass<1, M>(s, stride, tws, q, q2, u);
+    __syncthreads();
+    fwd_pass<2, M>(s, stride, tws, q, q2, u);
+    __syncthreads();
+    fwd_pass<3, M>(s, stride, tws, q, q2, u);
+    __syncthreads();
 }
 
+// Inverse transforms (include N^-1); input in [0, 2q) (canonical inputs are
+// fine), output canonical.  tws holds the inverse twiddles of ch.
 template <int M>
 __device__ __forceinline__ void cta_ntt_inverse_m(uint32_t* s, int stride, const uint2* tws, int ch) {
     const uint32_t q = c_dev.ch[ch].q, q2 = c_dev.ch[ch].two_q;
     const uint32_t ni = c_dev.ch[ch].ninv, nip = c_dev.ch[ch].ninv_p;
     const int u = threadIdx.x;
     __syncthreads();
+    inv_pass<3, M>(s, stride, tws, q, q2, ni, nip, u);
+    __syncthreads();
+    inv_pass<2, M>(s, stride, tws, q, q2, ni, nip, u);
+    __syncthreads();
+    inv_pass<1, M>(s, stride, tws, q, q2, ni, nip, u);
+    __syncthreads();
+    inv_pass<0, M>(s, stride, tws, q, q2, ni, nip, u);
+    __syncthreads();
+}
+
+__device__ __forceinline__ void cta_ntt_forward(uint32_t* s, const uint2* tws, int ch) {
+    cta_ntt_forward_m<1>(s, kPadN, tws, ch);
+}
+__device__ __forceinline__ void cta_ntt_inverse(uint32_t* s, const uint2* tws, int ch) {
+    cta_ntt_inverse_m<1>(s, kPadN, tws, ch);
+}
+
+// Copies of whole polynomials between global memory (natural order) and a
+// padded shared-memory polynomial; 16-byte vectors.
+__device__ __forceinline__ void poly_to_smem(uint32_t* s, const uint32_t* __restrict__ g) {
+    const uint4* g4 = reinterpret_cast<const uint4*>(g);
 #pragma unroll
-    for (int p = 3; p >= 0; p--) {
-        const int lq = 9 - 3 * p;
-        const int q8 = 1 << lq;
-        const int m0 = 1 << (3 * p);
-        const int i0 = u >> lq, j = u & (q8 - 1);
-        const int base = i0 * 8 * q8 + j;
-        const uint2 wa = tws[m0 + i0];
-        const uint2 wb0 = tws[2 * m0 + 2 * i0], wb1 = tws[2 * m0 + 2 * i0 + 1];
-        const uint2 wc0 = tws[4 * m0 + 4 * i0], wc1 = tws[4 * m0 + 4 * i0 + 1];
-        const uint2 wc2 = tws[4 * m0 + 4 * i0 + 2], wc3 = tws[4 * m0 + 4 * i0 + 3];
-        uint32_t x[M][8];
+    for (int k = threadIdx.x; k < kN / 4; k += kNttThreads) *reinterpret_cast<uint4*>(s + pidx(4 * k)) = __ldg(g4 + k);
+}
+__device__ __forceinline__ void poly_from_smem(uint32_t* __restrict__ g, const uint32_t* s) {
+    uint4* g4 = reinterpret_cast<uint4*>(g);
 #pragma unroll
-        for (int m = 0; m < M; m++) load8(s + m * stride, base, q8, x[m]);
-#pragma unroll
-        for (int m = 0; m < M; m++) {
-            inv_bfly(x[m][0], x[m][1], wc0, q, q2);
-            inv_bfly(x[m][2], x[m][3], wc1, q, q2);
-            inv_bfly(x[m][4], x[m][5], wc2, q, q2);
-            inv_bfly(x[m][6], x[m][7], wc3, q, q2);
-            inv_bfly(x[m][0], x[m][2], wb0, q, q2);
-            inv_bfly(x[m][1], x[m][3], wb0, q, q2);
-            inv_bfly(x[m][4], x[m][6], wb1, q, q2);
-            inv_bfly(x[m][5], x[m][7], wb1, q, q2);
-#pragma unroll
-            for (int t = 0; t < 4; t++) inv_bfly(x[m][t], x[m][t + 4], wa, q, q2);
-            if (p == 0) {
-#pragma unroll
-                for (int t = 0; t < 8; t++) x[m][t] = shoup_mul(x[m][t], ni, nip, q);
-            }
-        }
-#pragma unroll
-        for (int m = 0; m < M; m++) store8(s + m * stride, base, q8, x[m]);
-        __syncthreads();
-    }
+    for (int k = threadIdx.x; k < kN / 4; k += kNttThreads) g4[k] = *reinterpret_cast<const uint4*>(s + pidx(4 * k));
 }
 
 }  // namespace kspir
