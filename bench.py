@@ -8,12 +8,19 @@ with N = 4096, N1 = 128, N2 = 16 (reference tests/test-pir.cpp:14-29).
 Synthetic, seeded inputs of that shape (kspir_b200.synth).
 
 Reported (one JSON line on rank 0):
-  value      whole-job queries/s, inputs resident in HBM, device-timed with
-             CUDA events on the launching stream (max over ranks)
+  value      whole-job queries/s of the plain single-query answer, inputs
+             resident in HBM, device-timed with CUDA events on the launching
+             stream (max over ranks)
   e2e        queries/s through the public C ABI (kspir_answer) with the
              query in pinned host memory and the response read back, per step
   roofline   the dominant kernel (the database scan): algorithmic bytes per
              launch (r * N * N/2 * 8 = 1 GiB) / its mean CUDA-event duration
+  batched    the batched answer (kspir_answer_batch) at B = 1, 8, 32, 64, 128
+             queries of distinct clients: device-timed and end-to-end
+             queries/s, the scan variant the autotuner picked, per-phase
+             times, and the tensor roofline of the batched scan (int8 limb
+             products: 2 comp x 2 primes x 16 limb pairs per database word
+             and query)
   cpu_baseline  the reference's CPU answer (oracle/_ref, or the C port)
              on the host cores, on a bounded sample
 
@@ -52,6 +59,8 @@ def parse():
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batches", default="1,8,32,64,128", help="batch sizes of the batched sweep ('' = none)")
+    ap.add_argument("--clients", type=int, default=128, help="distinct client key sets of the batched sweep")
     return ap.parse_args()
 
 
@@ -183,6 +192,16 @@ def read_peaks():
     return 6650.0, "fallback (6.65 TB/s, earlier measurement on this pool)"
 
 
+def read_int8_peak():
+    """Dense int8 tensor peak, TOP/s: twice the measured bf16 burst (B200 issues
+    twice as many int8 as bf16 MMA operations per cycle: ncu peak_sustained
+    16384 vs 8192 per SM)."""
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        return 2 * float(json.load(open(p))["bf16_tflops"]), "2 x measured bf16 burst (MEASURED_PEAKS.json)"
+    return 2 * 1590.0, "2 x fallback bf16 1.59 PFLOP/s"
+
+
 def read_traffic(r):
     """DRAM bytes per scan launch from the committed ncu summary, if any."""
     p = os.path.join(ROOT, "profiles", "k_scan_256mb.md")
@@ -212,10 +231,13 @@ def run_gpu(args, rank, world, local_rank):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
     r, N1 = args.r, args.N1
+    batches = [int(x) for x in args.batches.split(",") if x.strip()]
+    bmax = max(batches) if batches else 1
+    nclients = max(1, min(args.clients, bmax))
     db = synth.gen_db(args.seed, r, N1)
     cl = synth.gen_client(args.seed + rank, r, N1)
     perms = kb.permutation_matrix(N1)
-    ctx = kb.Context(r, N1, device=local_rank)
+    ctx = kb.Context(r, N1, device=local_rank, max_clients=nclients, max_inflight=bmax)
     ctx.upload_db(db)
     ctx.upload_perms(perms)
     ctx.upload_client(0, cl["baby"], cl["giant"], cl["packing"], cl["rgsw"])
@@ -275,6 +297,8 @@ def run_gpu(args, rank, world, local_rank):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms, e2e_s = float(t[0]), float(t[1])
 
+    batched = run_batched(args, ctx, batches, nclients, rank, dist, torch) if batches else None
+
     if rank == 0:
         db_bytes = r * N * N // 2 * 8
         scan_ms = phases[1] / max(answers, 1)
@@ -305,6 +329,8 @@ def run_gpu(args, rank, world, local_rank):
             "gpu_launches": int(launches) * world,
             "clocks": clocks.summary(),
         }
+        if batched:
+            out["batched"] = batched
         if world == 1 and not args.no_cpu_baseline:
             threads = host_threads()
             rate, kind, n, th = cpu_answer_rate(db, cl, perms, r, N1, args.cpu_seconds, threads)
@@ -315,6 +341,93 @@ def run_gpu(args, rank, world, local_rank):
     ctx.close()
     if dist:
         dist.destroy_process_group()
+
+
+def run_batched(args, ctx, batches, nclients, rank, dist, torch):
+    """Batched answers of distinct clients at each batch size (the answer of
+    every query equals its single-query answer; tests/test_gpu_batch.py)."""
+    import kspir_b200 as kb
+    from kspir_b200 import synth
+    r, N1 = args.r, args.N1
+    for i in range(1, nclients):
+        c = synth.gen_client(args.seed + 1000 * (rank + 1) + i, r, N1)
+        ctx.upload_client(i, c["baby"], c["giant"], c["packing"], c["rgsw"])
+    rng = np.random.default_rng(args.seed + 77 + rank)
+    bmax = max(batches)
+    qall = np.empty((bmax, 4 * N), np.uint64)
+    qall[:, :2 * N] = rng.integers(0, kb.CRTMOD, size=(bmax, 2 * N), dtype=np.uint64)
+    qall[:, 2 * N:] = rng.integers(0, kb.BSMOD, size=(bmax, 2 * N), dtype=np.uint64)
+    dq = torch.from_numpy(qall.view(np.int64).copy()).cuda()
+    dr = torch.empty((bmax, 2 * N), dtype=torch.int64, device="cuda")
+    qh = torch.from_numpy(qall.view(np.int64).copy()).pin_memory()
+    rh = torch.empty((bmax, 2 * N), dtype=torch.int64).pin_memory()
+    stream = torch.cuda.Stream()
+    db_words = r * N * N // 2
+    int8_ops_per_query = db_words * 2 * 2 * 16 * 2
+    peak8, peak8_src = read_int8_peak()
+    res = {}
+    for B in batches:
+        cl = (np.arange(B, dtype=np.int32) % nclients)
+        kind, tried = ctx.tune_batch(B)
+        reps = max(5, min(args.steps, 2048 // B))
+
+        def step():
+            ctx.answer_batch_device(cl, dq.data_ptr(), dr.data_ptr(), stream.cuda_stream)
+        for _ in range(max(args.warmup, 3)):
+            step()
+        torch.cuda.synchronize()
+        ctx.timing_reset()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(reps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        nq, launches, tot, ph = ctx.timing_summary()
+        ctx.sync()
+        # end to end: pinned host queries in, responses out, through kspir_answer_batch
+        qv = qh.numpy().view(np.uint64)[:B]
+        rv = rh.numpy().view(np.uint64)[:B]
+        ctx.answer_batch(cl, qv, out=rv)
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            ctx.answer_batch(cl, qv, out=rv)
+        e2e_s = time.perf_counter() - t0
+        if not np.array_equal(rv, dr.cpu().numpy().view(np.uint64)[:B]):
+            raise RuntimeError(f"batch {B}: host-path and device-path responses differ")
+        if dist:
+            t = torch.tensor([ms, e2e_s], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms, e2e_s = float(t[0]), float(t[1])
+        world = dist.get_world_size() if dist else 1
+        scan_ms = ph[1] / reps
+        entry = {
+            "queries_per_s": world * B * reps / (ms * 1e-3),
+            "ms_per_batch": ms / reps,
+            "e2e_queries_per_s": world * B * reps / e2e_s,
+            "scan_kind": kb.SCAN_NAMES[kind],
+            "tuned_scan_ms": {kb.SCAN_NAMES[k]: v for k, v in tried.items()},
+            "phases_ms_per_batch": {"baby_steps": ph[0] / reps, "db_scan": scan_ms, "giant_steps": ph[2] / reps,
+                                    "external_products": ph[3] / reps, "packing": ph[4] / reps},
+            "launches_per_batch": launches / reps,
+        }
+        if kind != kb.SCAN_CUDA:
+            ach = int8_ops_per_query * B / (scan_ms * 1e-3) / 1e12
+            entry["roofline_scan"] = {"bound": "tensor", "achieved": ach, "peak": peak8, "unit": "TOP/s (int8)",
+                                      "frac": ach / peak8, "peak_source": peak8_src,
+                                      "algorithmic_ops_per_launch": int8_ops_per_query * B,
+                                      "note": "scan phase = query limb split + tcgen05 scan"}
+        res[str(B)] = entry
+    if "1" in res:
+        base = res["1"]["queries_per_s"]
+        for k, v in res.items():
+            v["speedup_vs_batch1"] = v["queries_per_s"] / base
+    return res
 
 
 def run_reference(args, rank, world):

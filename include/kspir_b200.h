@@ -199,6 +199,65 @@ int kspir_fetch_stage(kspir_ctx* ctx, int stage, uint64_t* out, size_t words);
  * batch ran in slot i). */
 int kspir_fetch_stage_slot(kspir_ctx* ctx, int slot, int stage, uint64_t* out, size_t words);
 
+/* Bytes of one client's keys in a device key slot (for sizing max_clients
+ * from an HBM budget). */
+size_t kspir_client_key_bytes(const kspir_ctx* ctx);
+
+/* ------------------------------------------------------------------------
+ * Serving loop (no counterpart in the reference): continuous batching of
+ * online answers on one context.
+ *
+ * A worker thread runs `lanes` lanes of `lane_size` workspace slots each
+ * (the context needs max_inflight >= lanes * lane_size, with lane_size
+ * rounded up to a multiple of 32 when the tensor-core scan is enabled).
+ * Whenever a lane is free, the waiting requests (up to lane_size) are
+ * admitted as one batch on it while the other lanes' batches still run.
+ * Client keys live in caller memory (registered once, kept valid by the
+ * caller until the server is destroyed or the client re-registered) and are
+ * cached in device key slots: at most key_budget_bytes of them (0 = all the
+ * context's slots), least recently used idle clients evicted first.  Each
+ * response equals kspir_answer on the same client and query.
+ * ------------------------------------------------------------------------ */
+typedef struct kspir_server kspir_server;
+
+typedef struct kspir_server_params {
+    int32_t lanes;             /* batches in flight at once */
+    int32_t lane_size;         /* largest batch (1..256) */
+    int64_t key_budget_bytes;  /* HBM for cached client keys; 0 = every key slot of the context */
+} kspir_server_params;
+
+typedef struct kspir_server_stats {
+    long served;               /* responses delivered since the last reset */
+    long batches;              /* batches launched */
+    double mean_batch;         /* queries per batch */
+    double p50_us, p95_us, p99_us, max_us;   /* submit -> response latency */
+    double queries_per_s;      /* served / seconds since the last reset */
+    long key_uploads;          /* client key sets brought into device slots */
+    long evictions;            /* resident key sets evicted for others */
+    int32_t key_slots;         /* device key slots the server may use */
+    int32_t max_running_lanes; /* most batches seen running at once */
+} kspir_server_stats;
+
+int kspir_server_create(kspir_ctx* ctx, const kspir_server_params* params, kspir_server** out);
+int kspir_server_destroy(kspir_server* srv);   /* finishes every submitted request first */
+int kspir_server_register_client(kspir_server* srv, int64_t client, const uint64_t* baby, const uint64_t* giant,
+                                 const uint64_t* packing, const uint64_t* rgsw);
+/* Queues one answer (query [2][2][N] and response [2][N] host buffers, both
+ * kept valid until the request completes); *ticket identifies it. */
+int kspir_server_submit(kspir_server* srv, int64_t client, const uint64_t* query, uint64_t* response,
+                        uint64_t* ticket);
+/* 1 = done (the ticket is released), 0 = still running, < 0 = the request
+ * failed with that error (released).  kspir_server_wait blocks up to
+ * timeout_ms. */
+int kspir_server_poll(kspir_server* srv, uint64_t ticket);
+int kspir_server_wait(kspir_server* srv, uint64_t ticket, int timeout_ms);
+int kspir_server_get_stats(kspir_server* srv, kspir_server_stats* out);
+int kspir_server_reset_stats(kspir_server* srv);
+/* Submit-to-response latencies (microseconds) of the requests served since
+ * the last reset, in completion order: *count receives how many there are,
+ * out (or NULL) the first min(capacity, count). */
+int kspir_server_latencies(kspir_server* srv, double* out, size_t capacity, size_t* count);
+
 #ifdef __cplusplus
 }
 #endif

@@ -4,7 +4,10 @@ The product is the CUDA library ``libkspir_b200.so`` behind the C ABI of
 ``include/kspir_b200.h``.  This package is its Python host binding:
 
 * :class:`Context` -- the device context (resident database, permutations,
-  per-client keys, query workspaces) and the C-ABI calls;
+  per-client keys, query workspaces) and the C-ABI calls, including the
+  batched answer;
+* :class:`Server` -- the serving loop (continuous batching, key admission by
+  HBM budget, p50/p95/p99 latency);
 * a mirror of the reference's own answer interface, with the reference's
   names, argument meaning and in-place effects, over numpy arrays laid out
   like the reference objects (an ``RlweCiphertext`` is a ``[2][N]`` u64 array
@@ -21,11 +24,11 @@ from dataclasses import dataclass
 import numpy as np
 
 from .native import (BSMOD, CRTMOD, N, Q1, Q2, SCAN_CUDA, SCAN_MMA4, SCAN_MMA8, SCAN_MMA16, SCAN_MMA32, SCAN_NAMES,
-                     Context, KspirError, LIB_PATH, STAGE_CIPHERBUF, STAGE_EXT, STAGE_RESULT, STAGE_SCAN, load,
+                     Context, KspirError, LIB_PATH, STAGE_CIPHERBUF, STAGE_EXT, STAGE_RESULT, STAGE_SCAN, Server, load,
                      permutation_matrix)
 
 __all__ = [
-    "N", "Q1", "Q2", "CRTMOD", "BSMOD", "Context", "KspirError", "load", "LIB_PATH", "permutation_matrix",
+    "N", "Q1", "Q2", "CRTMOD", "BSMOD", "Context", "Server", "KspirError", "load", "LIB_PATH", "permutation_matrix",
     "STAGE_CIPHERBUF", "STAGE_SCAN", "STAGE_RESULT", "STAGE_EXT",
     "SCAN_CUDA", "SCAN_MMA4", "SCAN_MMA8", "SCAN_MMA16", "SCAN_MMA32", "SCAN_NAMES",
     "AutoKeyBSGSRNS", "AutoKey", "RGSWCiphertext",

@@ -170,7 +170,7 @@ struct kspir_ctx {
     bool mma = false;                 // batched tensor-core scan enabled (N1 = 128, several slots)
     uint8_t* dbop = nullptr;          // its database operand [N][2][G] tiles
     int G = 0;
-    uint8_t* qop = nullptr;           // its query operand of one launch
+    uint8_t* qop = nullptr;           // its query operand: launch at slot0 uses qop_at(slot0)
     int32_t* perms = nullptr;
     bool perms_loaded = false;
     uint32_t* tw = nullptr;           // [3][4][N]
@@ -485,15 +485,21 @@ int scan_kind_for(kspir_ctx* c, int nq) {
 
 long scan_launches(const kspir_ctx* c, int kind, int nq) { return kind == SCAN_CUDA ? nq : 2; }
 
+// Query-operand region of a launch starting at workspace slot slot0: 8 MiB per
+// slot, so launches on disjoint 32-aligned slot ranges (serving lanes) never
+// share it.
+uint8_t* qop_at(kspir_ctx* c, int slot0) { return c->qop + (size_t)slot0 * kN * 2 * 8 * kMmaK; }
+
 template <int BT>
 void launch_scan_mma(kspir_ctx* c, int slot0, int nq, cudaStream_t st) {
     using C = MmaCfg<BT>;
     const int QT = (nq + BT - 1) / BT;
+    uint8_t* qop = qop_at(c, slot0);
     k_qop_split<BT><<<blocks_for((long)kN * QT * BT * 8, 256), 256, 0, st>>>(c->ws0.cipherbuf, c->ws_bytes, slot0, nq,
-                                                                              QT, c->qop);
+                                                                              QT, qop);
     ScanMmaArgs a;
     a.dbop = c->dbop;
-    a.qop = c->qop;
+    a.qop = qop;
     a.sout0 = c->ws0.sout;
     a.ws_bytes = c->ws_bytes;
     a.slot0 = slot0;
@@ -764,7 +770,7 @@ int kspir_ctx_create(int device, const kspir_params* params, kspir_ctx** out) {
         if (!rc) rc = mma_attr<16>(c.get());
         if (!rc) rc = mma_attr<32>(c.get());
         if (rc) return rc;
-        const size_t qslots = align_up((size_t)p.max_inflight, 32);
+        const size_t qslots = align_up((size_t)p.max_inflight, 32) + 32;   // a launch may round up by a tile
         KS_CUDA(c.get(), cudaMalloc(&c->qop, (size_t)kN * 2 * qslots * 8 * kMmaK));
     }
     rc = init_constants(c.get());
@@ -1216,6 +1222,8 @@ int kspir_fetch_stage(kspir_ctx* c, int stage, uint64_t* out, size_t words) {
 }
 
 }  // extern "C"
+
+#include "server.cuh"
 
 // ===========================================================================
 // External product without any allocation (kspir_external_product_noalloc).

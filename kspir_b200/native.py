@@ -61,6 +61,16 @@ SIGNATURES = {
     "kspir_set_scan_kind": (_i, [_vp, _i, _i]),
     "kspir_get_scan_kind": (_i, [_vp, _i]),
     "kspir_fetch_stage_slot": (_i, [_vp, _i, _i, _vp, _sz]),
+    "kspir_client_key_bytes": (_sz, [_vp]),
+    "kspir_server_create": (_i, [_vp, _vp, _vp]),
+    "kspir_server_destroy": (_i, [_vp]),
+    "kspir_server_register_client": (_i, [_vp, ctypes.c_int64, _vp, _vp, _vp, _vp]),
+    "kspir_server_submit": (_i, [_vp, ctypes.c_int64, _vp, _vp, _vp]),
+    "kspir_server_poll": (_i, [_vp, ctypes.c_uint64]),
+    "kspir_server_wait": (_i, [_vp, ctypes.c_uint64, _i]),
+    "kspir_server_get_stats": (_i, [_vp, _vp]),
+    "kspir_server_reset_stats": (_i, [_vp]),
+    "kspir_server_latencies": (_i, [_vp, _vp, _sz, _vp]),
 }
 
 # database-scan variants of kspir_tune_batch / kspir_set_scan_kind
@@ -76,6 +86,20 @@ SCAN_NAMES = {SCAN_CUDA: "cuda-core", SCAN_MMA4: "tcgen05-bt4", SCAN_MMA8: "tcge
 class Params(ctypes.Structure):
     _fields_ = [("r", ctypes.c_int32), ("N1", ctypes.c_int32),
                 ("max_clients", ctypes.c_int32), ("max_inflight", ctypes.c_int32)]
+
+
+class ServerParams(ctypes.Structure):
+    _fields_ = [("lanes", ctypes.c_int32), ("lane_size", ctypes.c_int32), ("key_budget_bytes", ctypes.c_int64)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("served", ctypes.c_long), ("batches", ctypes.c_long), ("mean_batch", ctypes.c_double),
+                ("p50_us", ctypes.c_double), ("p95_us", ctypes.c_double), ("p99_us", ctypes.c_double),
+                ("max_us", ctypes.c_double), ("queries_per_s", ctypes.c_double), ("key_uploads", ctypes.c_long),
+                ("evictions", ctypes.c_long), ("key_slots", ctypes.c_int32), ("max_running_lanes", ctypes.c_int32)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
 
 
 _lib = None
@@ -267,3 +291,82 @@ class Context:
         out = np.empty(sizes[stage], dtype=np.uint64)
         self._check(self.lib.kspir_fetch_stage_slot(self._h, slot, stage, ptr(out), out.size))
         return out
+
+
+class Server:
+    """Serving loop over a Context (kspir_server_* of include/kspir_b200.h):
+    continuous batching on `lanes` lanes of up to `lane_size` queries, client
+    keys cached in device key slots within `key_budget_bytes`."""
+
+    def __init__(self, ctx: Context, lanes: int = 2, lane_size: int = 64, key_budget_bytes: int = 0):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        self._h = ctypes.c_void_p()
+        self._keep = {}      # caller-owned key arrays must outlive the server
+        self._inflight = {}  # ticket -> (query, response) buffers
+        p = ServerParams(lanes, lane_size, key_budget_bytes)
+        self._check(self.lib.kspir_server_create(ctx.handle, ctypes.byref(p), ctypes.byref(self._h)))
+
+    def _check(self, rc):
+        if rc < 0:
+            raise KspirError(rc, self.lib.kspir_last_error(self.ctx.handle).decode() or
+                             self.lib.kspir_strerror(rc).decode())
+        return rc
+
+    def register(self, client: int, baby, giant, packing, rgsw):
+        arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.uint64).reshape(-1)
+                for a in (baby, giant, packing, rgsw)]
+        self._keep[client] = arrs
+        self._check(self.lib.kspir_server_register_client(self._h, client, *[ptr(a) for a in arrs]))
+
+    def submit(self, client: int, query, out: np.ndarray | None = None) -> int:
+        q = np.ascontiguousarray(query, dtype=np.uint64).reshape(-1)
+        if out is None:
+            out = np.empty(2 * N, dtype=np.uint64)
+        t = ctypes.c_uint64()
+        self._check(self.lib.kspir_server_submit(self._h, client, ptr(q), ptr(out), ctypes.byref(t)))
+        self._inflight[t.value] = (q, out)
+        return t.value
+
+    def poll(self, ticket: int):
+        """The response when done, else None."""
+        rc = self._check(self.lib.kspir_server_poll(self._h, ticket))
+        return self._inflight.pop(ticket)[1] if rc == 1 else None
+
+    def wait(self, ticket: int, timeout_ms: int = 60000) -> np.ndarray:
+        rc = self._check(self.lib.kspir_server_wait(self._h, ticket, timeout_ms))
+        if rc != 1:
+            raise TimeoutError(f"request {ticket} not done after {timeout_ms} ms")
+        return self._inflight.pop(ticket)[1]
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        self._check(self.lib.kspir_server_get_stats(self._h, ctypes.byref(st)))
+        return st.as_dict()
+
+    def reset_stats(self):
+        self._check(self.lib.kspir_server_reset_stats(self._h))
+
+    def latencies_us(self) -> np.ndarray:
+        n = ctypes.c_size_t()
+        self._check(self.lib.kspir_server_latencies(self._h, None, 0, ctypes.byref(n)))
+        out = np.empty(n.value, dtype=np.float64)
+        self._check(self.lib.kspir_server_latencies(self._h, ptr(out), out.size, ctypes.byref(n)))
+        return out[:min(out.size, n.value)]
+
+    def close(self):
+        if self._h:
+            self.lib.kspir_server_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
