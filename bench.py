@@ -77,7 +77,7 @@ def workload_config(args):
 # clocks during the timed region (NVML reads only)
 
 class ClockSampler:
-    def __init__(self, index: int, period: float = 0.05):
+    def __init__(self, index: int, period: float = 0.005):
         self.samples = []
         self.max_mhz = None
         self.reasons = set()

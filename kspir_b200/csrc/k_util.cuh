@@ -70,6 +70,44 @@ __global__ void k_split_words(const uint64_t* __restrict__ words, uint32_t* __re
     r[kN + k] = mod_q2(v);
 }
 
+// Client keys from reference words (layouts of include/kspir_b200.h) into a
+// key slot's residues: baby rows 0-2 mod crtMod -> baby_crt (both primes),
+// rows 3-5 mod bsMod -> baby_bs; giant, packing and RGSW -> both primes.  The
+// words were checked canonical when they were registered.
+__global__ void k_keys_from_words(const uint64_t* __restrict__ baby, const uint64_t* __restrict__ giant,
+                                  const uint64_t* __restrict__ packing, const uint64_t* __restrict__ rgsw,
+                                  uint32_t* __restrict__ baby_crt, uint32_t* __restrict__ baby_bs,
+                                  uint32_t* __restrict__ giant_res, uint32_t* __restrict__ packing_res,
+                                  uint32_t* __restrict__ rgsw_res, int nbaby, int ngiant, int npack) {
+    // polynomial index over [baby: nbaby * 6 * 2][giant: ngiant][packing: npack][rgsw: 8]
+    const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long nb = (long)nbaby * 12, total = nb + ngiant + npack + 8;
+    if (idx >= total * kN) return;
+    const int k = (int)(idx % kN);
+    long p = idx / kN;
+    if (p < nb) {
+        const long i = p / 12, j = (p / 2) % 6, comp = p % 2;
+        const uint64_t v = baby[p * kN + k];
+        if (j < 3) {
+            uint32_t* d = baby_crt + (((i * 3 + j) * 2 + comp) * 2) * kN;
+            d[k] = mod_q1(v);
+            d[kN + k] = mod_q2(v);
+        } else {
+            baby_bs[((i * 3 + j - 3) * 2 + comp) * kN + k] = (uint32_t)v;
+        }
+        return;
+    }
+    p -= nb;
+    const uint64_t* src;
+    uint32_t* dst;
+    if (p < ngiant) { src = giant; dst = giant_res; }
+    else if ((p -= ngiant) < npack) { src = packing; dst = packing_res; }
+    else { p -= npack; src = rgsw; dst = rgsw_res; }
+    const uint64_t v = src[p * kN + k];
+    dst[(p * 2) * kN + k] = mod_q1(v);
+    dst[(p * 2 + 1) * kN + k] = mod_q2(v);
+}
+
 // Validation of caller words: flags[0] |= 1 when some word is >= its modulus.
 __global__ void k_check_canonical(const uint64_t* __restrict__ words, size_t n, uint64_t modulus,
                                   int* __restrict__ flag) {

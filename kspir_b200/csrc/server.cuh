@@ -13,7 +13,11 @@
 // keys are resident or can be made resident, evicting the least recently used
 // client that has no queued or running request.  The number of key slots the
 // server may use follows from its HBM budget (key_budget_bytes / key slot
-// size, at most the context's max_clients).
+// size, at most the context's max_clients).  Keys are checked canonical and
+// page-locked once, at registration; admission then copies the raw words
+// asynchronously on the lane's stream into a per-lane staging buffer and a
+// kernel converts them into the slot, so the copy overlaps the other lanes'
+// batches; a per-slot event orders every later use of the slot after it.
 //
 // Each response equals kspir_answer on the same client and query: a batch
 // runs the same kernels on disjoint workspace slots, and no kernel reads
@@ -43,12 +47,15 @@ struct kspir_server {
         cudaEvent_t done = nullptr;
         uint64_t* hq = nullptr;   // pinned [lane_size][4][N]
         uint64_t* hr = nullptr;   // pinned [lane_size][2][N]
+        uint64_t* kstage = nullptr;   // device staging of one client's key words
         std::vector<Req*> reqs;
         bool busy = false;
     };
     struct Client {
         const uint64_t *baby = nullptr, *giant = nullptr, *packing = nullptr, *rgsw = nullptr;
+        std::vector<const void*> pinned;   // caller ranges page-locked at registration
         int slot = -1;
+        bool fresh = false;       // slot assigned, words not yet copied
         int active = 0;           // requests queued or running
         uint64_t last_use = 0;
     };
@@ -59,6 +66,8 @@ struct kspir_server {
     std::vector<Lane> lanes;
     std::unordered_map<int64_t, Client> clients;
     std::vector<int64_t> slot_owner;   // key slot -> client id, -1 free
+    std::vector<cudaEvent_t> slot_ready;   // recorded after each upload into the slot
+    size_t kw_baby = 0, kw_giant = 0, kw_pack = 0, kw_rgsw = 0;   // raw key words per client
     std::deque<Req*> pending;
     std::unordered_map<uint64_t, Req*> reqs;
     std::mutex mu;
@@ -78,9 +87,10 @@ namespace {
 
 using Srv = kspir_server;
 
-// keys of `id` resident (caller holds s.mu); false when every slot is held by
-// a client with requests in flight
-bool srv_make_resident(Srv& s, int64_t id, int* rc) {
+// a key slot for `id` (caller holds s.mu); false when every slot is held by a
+// client with requests in flight.  A newly assigned slot is marked fresh: its
+// words are copied by the batch that admitted the client (srv_upload).
+bool srv_make_resident(Srv& s, int64_t id) {
     Srv::Client& cl = s.clients[id];
     if (cl.slot >= 0) return true;
     int slot = -1;
@@ -96,12 +106,36 @@ bool srv_make_resident(Srv& s, int64_t id, int* rc) {
         s.clients[s.slot_owner[slot]].slot = -1;
         s.evictions++;
     }
-    *rc = kspir_client_keys_upload(s.c, slot, cl.baby, cl.giant, cl.packing, cl.rgsw);
-    if (*rc) return false;
     s.slot_owner[slot] = id;
     cl.slot = slot;
+    cl.fresh = true;
     s.key_uploads++;
     return true;
+}
+
+// enqueues the copy of a fresh client's key words into its slot on lane L
+int srv_upload(Srv& s, Srv::Lane& L, Srv::Client& cl) {
+    kspir_ctx* c = s.c;
+    uint64_t* b = L.kstage;
+    uint64_t* g = b + s.kw_baby;
+    uint64_t* pk = g + s.kw_giant;
+    uint64_t* rg = pk + s.kw_pack;
+    if (cudaMemcpyAsync(b, cl.baby, s.kw_baby * 8, cudaMemcpyHostToDevice, L.st) != cudaSuccess) return KSPIR_ERR_CUDA;
+    if (s.kw_giant && cudaMemcpyAsync(g, cl.giant, s.kw_giant * 8, cudaMemcpyHostToDevice, L.st) != cudaSuccess)
+        return KSPIR_ERR_CUDA;
+    if (s.kw_pack && cudaMemcpyAsync(pk, cl.packing, s.kw_pack * 8, cudaMemcpyHostToDevice, L.st) != cudaSuccess)
+        return KSPIR_ERR_CUDA;
+    if (cudaMemcpyAsync(rg, cl.rgsw, s.kw_rgsw * 8, cudaMemcpyHostToDevice, L.st) != cudaSuccess) return KSPIR_ERR_CUDA;
+    const ClientKeysDev d = keys_host(c, cl.slot);
+    const long polys = (long)(s.kw_baby + s.kw_giant + s.kw_pack + s.kw_rgsw) / kN;
+    k_keys_from_words<<<blocks_for(polys * kN, 256), 256, 0, L.st>>>(
+        b, g, pk, rg, const_cast<uint32_t*>(d.baby_crt), const_cast<uint32_t*>(d.baby_bs),
+        const_cast<uint32_t*>(d.giant), const_cast<uint32_t*>(d.packing), const_cast<uint32_t*>(d.rgsw), c->N1h,
+        (int)(s.kw_giant / kN), (int)(s.kw_pack / kN));
+    if (cudaGetLastError() != cudaSuccess) return KSPIR_ERR_CUDA;
+    if (cudaEventRecord(s.slot_ready[cl.slot], L.st) != cudaSuccess) return KSPIR_ERR_CUDA;
+    cl.fresh = false;
+    return KSPIR_OK;
 }
 
 void srv_finish_lane(Srv& s, Srv::Lane& L) {
@@ -139,16 +173,8 @@ void srv_launch(Srv& s, Srv::Lane& L) {
     while (!s.pending.empty() && (int)L.reqs.size() < s.p.lane_size) {
         Srv::Req* r = s.pending.front();
         s.pending.pop_front();
-        int rc = KSPIR_OK;
-        if (!srv_make_resident(s, r->client, &rc)) {
-            if (rc) {   // the keys could not be uploaded: fail this request
-                r->rc = rc;
-                r->state = 2;
-                s.clients[r->client].active--;
-                s.cv_done.notify_all();
-            } else {
-                keep.push_back(r);   // no free key slot now: stays queued, in order
-            }
+        if (!srv_make_resident(s, r->client)) {
+            keep.push_back(r);   // no free key slot now: stays queued, in order
             continue;
         }
         Srv::Client& cl = s.clients[r->client];
@@ -165,8 +191,15 @@ void srv_launch(Srv& s, Srv::Lane& L) {
     int rc = KSPIR_OK;
     {
         std::lock_guard<std::mutex> lk(c->mu);
-        if (cudaMemcpyAsync(c->bq64 + (size_t)L.slot0 * 4 * kN, L.hq, (size_t)n * 4 * kN * 8, cudaMemcpyHostToDevice,
-                            L.st) != cudaSuccess)
+        // keys: copy the fresh ones on this lane, wait for the others' last upload
+        for (Srv::Req* r : L.reqs) {
+            Srv::Client& cl = s.clients[r->client];
+            if (cl.fresh && !rc) rc = srv_upload(s, L, cl);
+        }
+        for (int k : slots)
+            if (!rc && cudaStreamWaitEvent(L.st, s.slot_ready[k], 0) != cudaSuccess) rc = KSPIR_ERR_CUDA;
+        if (!rc && cudaMemcpyAsync(c->bq64 + (size_t)L.slot0 * 4 * kN, L.hq, (size_t)n * 4 * kN * 8,
+                                   cudaMemcpyHostToDevice, L.st) != cudaSuccess)
             rc = KSPIR_ERR_CUDA;
         if (!rc) rc = enqueue_answer(c, L.slot0, n, slots.data(), L.st);
         if (!rc && cudaMemcpyAsync(L.hr, c->bresp + (size_t)L.slot0 * 2 * kN, (size_t)n * 2 * kN * 8,
@@ -178,7 +211,12 @@ void srv_launch(Srv& s, Srv::Lane& L) {
         for (Srv::Req* r : L.reqs) {
             r->rc = rc;
             r->state = 2;
-            s.clients[r->client].active--;
+            Srv::Client& cl = s.clients[r->client];
+            cl.active--;
+            if (cl.slot >= 0) {   // the slot's contents are unknown after a failure
+                s.slot_owner[cl.slot] = -1;
+                cl.slot = -1;
+            }
         }
         L.reqs.clear();
         s.cv_done.notify_all();
@@ -248,7 +286,14 @@ int kspir_server_create(kspir_ctx* c, const kspir_server_params* params, kspir_s
     s->key_slots = (int)std::min<long>(budget_slots, c->p.max_clients);
     if (s->key_slots < 1) return set_err(c, KSPIR_ERR_INVALID_ARG, "key budget below one client's keys");
     s->slot_owner.assign(s->key_slots, -1);
+    s->kw_baby = (size_t)c->N1h * 6 * 2 * kN;
+    s->kw_giant = (size_t)(c->N2 - 1) * 2 * 2 * kN;
+    s->kw_pack = (size_t)c->levels * 4 * 2 * kN;
+    s->kw_rgsw = (size_t)4 * 2 * kN;
+    const size_t kwords = s->kw_baby + s->kw_giant + s->kw_pack + s->kw_rgsw;
     KS_CUDA(c, cudaSetDevice(c->device));
+    s->slot_ready.assign(s->key_slots, nullptr);
+    for (auto& e : s->slot_ready) KS_CUDA(c, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     s->lanes.resize(p.lanes);
     for (int l = 0; l < p.lanes; l++) {
         auto& L = s->lanes[l];
@@ -257,6 +302,7 @@ int kspir_server_create(kspir_ctx* c, const kspir_server_params* params, kspir_s
         KS_CUDA(c, cudaEventCreateWithFlags(&L.done, cudaEventDisableTiming));
         KS_CUDA(c, cudaMallocHost(&L.hq, (size_t)p.lane_size * 4 * kN * 8));
         KS_CUDA(c, cudaMallocHost(&L.hr, (size_t)p.lane_size * 2 * kN * 8));
+        KS_CUDA(c, cudaMalloc(&L.kstage, kwords * 8));
     }
     s->t_stats = std::chrono::steady_clock::now();
     s->worker = std::thread(srv_loop, s.get());
@@ -279,7 +325,11 @@ int kspir_server_destroy(kspir_server* s) {
         cudaEventDestroy(L.done);
         cudaFreeHost(L.hq);
         cudaFreeHost(L.hr);
+        cudaFree(L.kstage);
     }
+    for (auto& e : s->slot_ready) cudaEventDestroy(e);
+    for (auto& kv : s->clients)
+        for (const void* ptr : kv.second.pinned) cudaHostUnregister(const_cast<void*>(ptr));
     for (auto& kv : s->reqs) delete kv.second;
     delete s;
     return KSPIR_OK;
@@ -288,13 +338,34 @@ int kspir_server_destroy(kspir_server* s) {
 int kspir_server_register_client(kspir_server* s, int64_t client, const uint64_t* baby, const uint64_t* giant,
                                  const uint64_t* packing, const uint64_t* rgsw) {
     if (!s || !baby || !rgsw) return KSPIR_ERR_INVALID_ARG;
+    kspir_ctx* c = s->c;
+    if ((s->kw_giant && !giant) || (s->kw_pack && !packing)) return KSPIR_ERR_INVALID_ARG;
+    // canonical words, checked once: rows 0-2 of each baby key mod crtMod, 3-5 mod bsMod
+    for (size_t p = 0; p < s->kw_baby / kN; p++)
+        if (!canonical(baby + p * kN, kN, ((p / 2) % 6) < 3 ? kCrtMod : (uint64_t)kBsMod))
+            return set_err(c, KSPIR_ERR_INVALID_ARG, "key word not canonical");
+    if ((giant && !canonical(giant, s->kw_giant, kCrtMod)) || (packing && !canonical(packing, s->kw_pack, kCrtMod)) ||
+        !canonical(rgsw, s->kw_rgsw, kCrtMod))
+        return set_err(c, KSPIR_ERR_INVALID_ARG, "key word not canonical");
     std::lock_guard<std::mutex> lk(s->mu);
     Srv::Client& cl = s->clients[client];
-    if (cl.active) return set_err(s->c, KSPIR_ERR_BUSY, "client has requests in flight");
+    if (cl.active) return set_err(c, KSPIR_ERR_BUSY, "client has requests in flight");
+    KS_CUDA(c, cudaSetDevice(c->device));
+    for (const void* ptr : cl.pinned) cudaHostUnregister(const_cast<void*>(ptr));
+    cl.pinned.clear();
     cl.baby = baby;
     cl.giant = giant;
     cl.packing = packing;
     cl.rgsw = rgsw;
+    // page-lock the caller's words so admission copies are asynchronous; if
+    // that is refused the copies still work, through pageable staging
+    const std::pair<const uint64_t*, size_t> ranges[4] = {
+        {baby, s->kw_baby}, {giant, s->kw_giant}, {packing, s->kw_pack}, {rgsw, s->kw_rgsw}};
+    for (const auto& rg : ranges)
+        if (rg.first && rg.second &&
+            cudaHostRegister(const_cast<uint64_t*>(rg.first), rg.second * 8, cudaHostRegisterDefault) == cudaSuccess)
+            cl.pinned.push_back(rg.first);
+    cudaGetLastError();   // a refused registration leaves no error behind
     if (cl.slot >= 0) {   // new keys: drop the resident copy
         s->slot_owner[cl.slot] = -1;
         cl.slot = -1;

@@ -161,7 +161,8 @@ def main():
     ap.add_argument("--lanes", type=int, default=2)
     ap.add_argument("--lane-size", type=int, default=64)
     ap.add_argument("--clients", type=int, default=48, help="registered clients per database")
-    ap.add_argument("--key-slots", type=int, default=32, help="device key slots per database (HBM budget)")
+    ap.add_argument("--key-slots", type=int, default=48,
+                    help="device key slots per database (HBM budget); below --clients, keys are evicted and re-admitted")
     ap.add_argument("--max-group", type=int, default=128)
     a = ap.parse_args()
     res = run([float(x) for x in a.rates.split(",")], a.duration, a.seed, [int(x) for x in a.dbs.split(",")],
