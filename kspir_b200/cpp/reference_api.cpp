@@ -1,0 +1,191 @@
+// The reference's three server-answer functions, implemented over the C ABI
+// of libkspir_b200 so that a program written against the reference (for
+// example its tests/test-pir.cpp) runs its online answer on the GPU unchanged:
+//
+//   matrix_vector_mul_bsgs_rns_crt_large   reference src/twosteps.h:55-57
+//   externalProduct                        reference src/lwe.h:292
+//   packingRLWEs                           reference src/answer.h:79-80
+//
+// Same signatures, argument meaning and in-place effects as the reference:
+// input[0] is modswitched in place to NTT form and result[j] comes back in NTT
+// form; externalProduct accumulates into `result` and returns both `result`
+// and `firstDim` in coefficient form; packingRLWEs writes the packed response
+// in coefficient form.  One difference: packingRLWEs leaves `rlwes` as it was
+// (the reference overwrites it with the packing tree's intermediates).
+//
+// The database, permutations and key objects are uploaded to the device the
+// first time they are seen and stay resident; an object at an address already
+// uploaded is assumed unchanged (the reference's callers build them once).
+// The reference's functions return void and check only with assert; an error
+// of the library here prints its message and aborts likewise.
+//
+// Built against the reference's headers, so it needs the reference tree:
+// oracle/Makefile target `testpir-gpu` links it with the reference's objects.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "answer.h"
+#include "lwe.h"
+#include "twosteps.h"
+
+#include "kspir_b200.h"
+
+namespace {
+
+constexpr int kPoly = KSPIR_N;
+
+struct Session {
+    kspir_ctx* ctx = nullptr;
+    int r = 0, N1 = 0;
+    const uint64_t* db = nullptr;
+    const void* perms = nullptr;
+    const void* bsgs = nullptr;   // key objects whose words are resident
+    const void* gsw = nullptr;
+    const void* pack = nullptr;
+    std::vector<uint64_t> baby, giant, packing, rgsw;   // words of client slot 0
+};
+Session g;
+
+void check(const char* what, int rc) {
+    if (rc == KSPIR_OK) return;
+    fprintf(stderr, "kspir_b200: %s: %s (%s)\n", what, kspir_strerror(rc),
+            kspir_last_error(g.ctx ? g.ctx : nullptr));
+    abort();
+}
+
+int log2i(int v) {
+    int l = 0;
+    while ((1 << l) < v) l++;
+    return l;
+}
+
+uint32_t pow5_mod2n(long e) {
+    uint64_t r = 1, b = 5, m = 2 * (uint64_t)kPoly;
+    while (e > 0) {
+        if (e & 1) r = r * b % m;
+        b = b * b % m;
+        e >>= 1;
+    }
+    return (uint32_t)r;
+}
+
+void put_rlwe(uint64_t* dst, const RlweCiphertext& c) {
+    memcpy(dst, c.a.data(), kPoly * 8);
+    memcpy(dst + kPoly, c.b.data(), kPoly * 8);
+}
+
+void get_rlwe(RlweCiphertext& c, const uint64_t* src) {
+    c.a.assign(src, src + kPoly);
+    c.b.assign(src + kPoly, src + 2 * kPoly);
+}
+
+// a context for (r, N1); the key words start as zeros until their objects arrive
+void ensure(int r, int N1) {
+    if (g.ctx && g.r == r && g.N1 == N1) return;
+    if (g.ctx) kspir_ctx_destroy(g.ctx);
+    g = Session();
+    kspir_params p;
+    p.r = r;
+    p.N1 = N1;
+    p.max_clients = 1;
+    p.max_inflight = 1;
+    check("kspir_ctx_create", kspir_ctx_create(0, &p, &g.ctx));
+    g.r = r;
+    g.N1 = N1;
+    const int N2 = kPoly / 2 / N1;
+    g.baby.assign((size_t)(N1 / 2) * 6 * 2 * kPoly, 0);
+    g.giant.assign((size_t)(N2 - 1) * 2 * 2 * kPoly, 0);
+    g.packing.assign((size_t)log2i(r) * 4 * 2 * kPoly, 0);
+    g.rgsw.assign((size_t)4 * 2 * kPoly, 0);
+}
+
+void upload_keys() {
+    check("kspir_client_keys_upload",
+          kspir_client_keys_upload(g.ctx, 0, g.baby.data(), g.giant.empty() ? nullptr : g.giant.data(),
+                                   g.packing.empty() ? nullptr : g.packing.data(), g.rgsw.data()));
+}
+
+}  // namespace
+
+void matrix_vector_mul_bsgs_rns_crt_large(std::vector<RlweCiphertext>& result, std::vector<RlweCiphertext>& input,
+                                          uint64_t* data, const AutoKeyBSGSRNS& autoKey, const int32_t N1,
+                                          std::vector<std::vector<int32_t> >& permutations, int32_t r) {
+    ensure(r, N1);
+    const int N2 = kPoly / 2 / N1;
+    if (g.db != data) {
+        check("kspir_db_upload", kspir_db_upload(g.ctx, data, (size_t)r * kPoly * (kPoly / 2)));
+        g.db = data;
+    }
+    if (g.perms != (const void*)&permutations) {
+        std::vector<int32_t> flat((size_t)N1 * kPoly);
+        for (int i = 0; i < N1; i++) memcpy(flat.data() + (size_t)i * kPoly, permutations[i].data(), kPoly * 4);
+        check("kspir_perms_upload", kspir_perms_upload(g.ctx, flat.data(), flat.size()));
+        g.perms = &permutations;
+    }
+    if (g.bsgs != (const void*)&autoKey) {
+        // baby keys keyMap[5^i], i = 1..N1/2 (six RLWEs each: crtMod rows, then bsMod
+        // rows); giant keys keyMap[5^(N1 c)], c = 1..N2-1 (two RLWEs each)
+        for (int i = 1; i <= N1 / 2; i++) {
+            const std::vector<RlweCiphertext>& v = autoKey.keyMap.at((int32_t)pow5_mod2n(i));
+            for (int j = 0; j < 6; j++) put_rlwe(g.baby.data() + ((size_t)(i - 1) * 6 + j) * 2 * kPoly, v[j]);
+        }
+        for (int c = 1; c < N2; c++) {
+            const std::vector<RlweCiphertext>& v = autoKey.keyMap.at((int32_t)pow5_mod2n((long)N1 * c));
+            for (int j = 0; j < 2; j++) put_rlwe(g.giant.data() + ((size_t)(c - 1) * 2 + j) * 2 * kPoly, v[j]);
+        }
+        upload_keys();
+        g.bsgs = &autoKey;
+    }
+    std::vector<uint64_t> q(4 * kPoly), res((size_t)r * 2 * kPoly);
+    put_rlwe(q.data(), input[0]);
+    put_rlwe(q.data() + 2 * kPoly, input[1]);
+    check("kspir_matrix_vector_mul_bsgs_rns_crt_large",
+          kspir_matrix_vector_mul_bsgs_rns_crt_large(g.ctx, 0, q.data(), res.data()));
+    for (int j = 0; j < r; j++) {
+        get_rlwe(result[j], res.data() + (size_t)j * 2 * kPoly);
+        result[j].setIsNtt(true);
+    }
+    get_rlwe(input[0], q.data());
+    input[0].setIsNtt(true);
+}
+
+void externalProduct(RlweCiphertext& result, RlweCiphertext& firstDim, const RGSWCiphertext& query) {
+    if (!g.ctx) ensure(1, 128);
+    if (g.gsw != (const void*)&query) {
+        for (int j = 0; j < 4; j++) {
+            memcpy(g.rgsw.data() + (size_t)j * 2 * kPoly, query.a[j].data(), kPoly * 8);
+            memcpy(g.rgsw.data() + (size_t)j * 2 * kPoly + kPoly, query.b[j].data(), kPoly * 8);
+        }
+        upload_keys();
+        g.gsw = &query;
+    }
+    std::vector<uint64_t> acc(2 * kPoly), fd(2 * kPoly);
+    put_rlwe(acc.data(), result);
+    put_rlwe(fd.data(), firstDim);
+    check("kspir_external_product", kspir_external_product(g.ctx, 0, acc.data(), fd.data(), 1));
+    get_rlwe(result, acc.data());
+    get_rlwe(firstDim, fd.data());
+    result.setIsNtt(false);
+    firstDim.setIsNtt(false);
+}
+
+void packingRLWEs(RlweCiphertext& result, std::vector<RlweCiphertext>& rlwes, const AutoKey& autokey) {
+    const int r = (int)rlwes.size();
+    if (!g.ctx || g.r != r) ensure(r, g.N1 ? g.N1 : 128);
+    if (g.pack != (const void*)&autokey) {
+        // keyMap[N/2^l + 1], l = 0..log2 r - 1, four RLWEs each
+        for (int l = 0; l < log2i(r); l++) {
+            const std::vector<RlweCiphertext>& v = autokey.keyMap.at(kPoly / (1 << l) + 1);
+            for (int j = 0; j < 4; j++) put_rlwe(g.packing.data() + ((size_t)l * 4 + j) * 2 * kPoly, v[j]);
+        }
+        upload_keys();
+        g.pack = &autokey;
+    }
+    std::vector<uint64_t> in((size_t)r * 2 * kPoly), out(2 * kPoly);
+    for (int j = 0; j < r; j++) put_rlwe(in.data() + (size_t)j * 2 * kPoly, rlwes[j]);
+    check("kspir_packing_rlwes", kspir_packing_rlwes(g.ctx, 0, in.data(), out.data()));
+    get_rlwe(result, out.data());
+    result.setIsNtt(false);
+}

@@ -1,0 +1,22 @@
+"""The drop-in: the reference's unmodified tests/test-pir.cpp, linked with
+kspir_b200/cpp/reference_api.cpp in place of the reference's three answer
+functions (built by `make -C oracle testpir-gpu`), runs its online answer on
+the GPU and recovers the planted record like the reference build does."""
+import os
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+BIN = os.path.join(ROOT, "oracle", "_ref", "test-pir-gpu")
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.skipif(not os.path.exists(BIN), reason="oracle/_ref/test-pir-gpu not built (needs the reference tree)")
+def test_unmodified_testpir_recovers_the_record_through_the_gpu():
+    out = subprocess.run([BIN], capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    want = "the recovered result = [" + ", ".join(str(i) for i in range(1, 17)) + ", ..., 4096]"
+    assert want in out.stdout, out.stdout[-2000:]
+    assert "online server response costs" in out.stdout
