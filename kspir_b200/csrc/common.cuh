@@ -98,6 +98,25 @@ __device__ __forceinline__ uint64_t crt_compose_res(uint32_t r1, uint32_t r2) {
     return (uint64_t)r1 + (uint64_t)kQ1 * t;
 }
 
+// x mod q, exact for every 64-bit x, q a prime in (2^27, 2^28); mu1 = 2^59 / q,
+// c32 = 2^32 mod q, mu2 = 2^57 / q.  Two Barrett steps with 32x32 products.
+__host__ __device__ __forceinline__ uint32_t mod28(uint64_t x, uint32_t q, uint32_t mu1, uint32_t c32, uint32_t mu2) {
+    const uint32_t xh = (uint32_t)(x >> 32), xl = (uint32_t)x;
+    uint32_t r = xh - (uint32_t)(((uint64_t)xh * mu1) >> 59) * q;   // in [0, 2q)
+    r = r >= q ? r - q : r;
+    const uint64_t y = (uint64_t)r * c32 + xl;                       // < 2^57, same residue
+    const uint32_t qh = (uint32_t)(((y >> 26) * mu2) >> 31);
+    uint32_t t = (uint32_t)y - qh * q;                                // in [0, 3q)
+    t = t >= q ? t - q : t;
+    return t >= q ? t - q : t;
+}
+
+// x mod q_ch for the crt primes (ch 0: q1, 1: q2), any 64-bit x.  (mod28 measured
+// no faster than this Barrett reduction inside the key-switch kernels.)
+__device__ __forceinline__ uint32_t mod_crt(uint64_t x, int ch) {
+    return reduce64(x, ch ? kQ2 : kQ1, c_dev.ch[ch].barrett);
+}
+
 __device__ __forceinline__ uint32_t mod_q1(uint64_t v) { return reduce64(v, kQ1, c_dev.ch[CH_Q1].barrett); }
 __device__ __forceinline__ uint32_t mod_q2(uint64_t v) { return reduce64(v, kQ2, c_dev.ch[CH_Q2].barrett); }
 __device__ __forceinline__ uint32_t mod_bs(uint64_t v) { return reduce64(v, kBsMod, c_dev.ch[CH_BS].barrett); }

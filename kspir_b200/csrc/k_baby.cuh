@@ -61,7 +61,9 @@ constexpr int kPerThread = kN / kNttThreads; // 8 coefficients per thread
 // of the eight transforms per rotation but measured slower on B200 even for
 // batches of 64: these CTAs are latency-bound, not issue-bound.)
 template <int ELL>
-__global__ void __launch_bounds__(kNttThreads) k_baby_rot(BabyArgs a, ClientKeysDev keys, NttTables tabs, Batch bt) {
+// Three CTAs per SM (at most 42 registers): with one (106 registers unbounded)
+// a batch of 64 ran 28 % slower.
+__global__ void __launch_bounds__(kNttThreads, 3) k_baby_rot(BabyArgs a, ClientKeysDev keys, NttTables tabs, Batch bt) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
     {
         const size_t wo = ws_off(bt);
@@ -157,7 +159,7 @@ __global__ void __launch_bounds__(kNttThreads) k_baby_rot(BabyArgs a, ClientKeys
 #pragma unroll
     for (int it = 0; it < kPerThread; it++) {
         const int k = tid + it * kNttThreads;
-        uint32_t A = negmod(reduce64(acc[it], cc.q, cc.barrett), cc.q);
+        uint32_t A = negmod(mod_crt(acc[it], ch), cc.q);
         if (comp == 1) A = addmod(A, __ldg(a.srcB + ch * kN + sig[k]), cc.q);
         if (inter) inter_out[ch * kN + k] = A;
         const uint32_t r = shoup_mul(submod(A, S[pidx(tid) + it * kPadStep], cc.q), cc.bsinv, cc.bsinv_p, cc.q);

@@ -83,19 +83,6 @@ __host__ __device__ __forceinline__ int mma_brow(int g, int lb) {
     return 16 * (g >> 2) + 8 * (lb >> 1) + 2 * (g & 3) + (lb & 1);
 }
 
-// x mod q, exact for every 64-bit x, q a prime in (2^27, 2^28); mu1 = 2^59 / q,
-// c32 = 2^32 mod q, mu2 = 2^57 / q.  Two Barrett steps with 32x32 products.
-__host__ __device__ __forceinline__ uint32_t mod28(uint64_t x, uint32_t q, uint32_t mu1, uint32_t c32, uint32_t mu2) {
-    const uint32_t xh = (uint32_t)(x >> 32), xl = (uint32_t)x;
-    uint32_t r = xh - (uint32_t)(((uint64_t)xh * mu1) >> 59) * q;   // in [0, 2q)
-    r = r >= q ? r - q : r;
-    const uint64_t y = (uint64_t)r * c32 + xl;                       // < 2^57, same residue
-    const uint32_t qh = (uint32_t)(((y >> 26) * mu2) >> 31);
-    uint32_t t = (uint32_t)y - qh * q;                                // in [0, 3q)
-    t = t >= q ? t - q : t;
-    return t >= q ? t - q : t;
-}
-
 // instruction descriptor: u8 x u8 -> s32, A and B K-major, M = 128
 __host__ __device__ constexpr uint32_t mma_idesc_u8(int n) {
     return (2u << 4) | ((uint32_t)(n >> 3) << 17) | ((128u >> 4) << 24);

@@ -169,8 +169,8 @@ __global__ void __launch_bounds__(kNttThreads) k_giant_fused(uint32_t* sout, con
                 mad_wide(sb, d, __ldg(key + ((j * 2 + 1) * 2 + ch) * kN + k));
             }
             const uint32_t bv = sout[sout_idx(row, 1 * 2 + ch, sig[k], rows)];
-            cbv[it] = addmod(bv, negmod(reduce64(sb, cc.q, cc.barrett), cc.q), cc.q);
-            sout[sout_idx(row, 0 * 2 + ch, k, rows)] = negmod(reduce64(sa, cc.q, cc.barrett), cc.q);
+            cbv[it] = addmod(bv, negmod(mod_crt(sb, ch), cc.q), cc.q);
+            sout[sout_idx(row, 0 * 2 + ch, k, rows)] = negmod(mod_crt(sa, ch), cc.q);
         }
         __syncthreads();   // every gather of this prime's b part is done
 #pragma unroll
@@ -271,9 +271,9 @@ __global__ void __launch_bounds__(kNttThreads) k_pack_fused(const uint32_t* __re
             mad_wide(sa, dv, __ldg(key + ((d * 2 + 0) * 2 + ch) * kN + k));
             mad_wide(sb, dv, __ldg(key + ((d * 2 + 1) * 2 + ch) * kN + k));
         }
-        const uint32_t a2 = negmod(reduce64(sa, cq.q, cq.barrett), q);
+        const uint32_t a2 = negmod(mod_crt(sa, ch), q);
         const int pk = pidx(tid) + it * kPadStep;
-        const uint32_t b2 = submod(P[ELL * kPadN + pk], reduce64(sb, cq.q, cq.barrett), q);
+        const uint32_t b2 = submod(P[ELL * kPadN + pk], mod_crt(sb, ch), q);
         P[pk] = a2;            // only this thread reads index k of these rows
         P[kPadN + pk] = b2;
     }
@@ -362,7 +362,7 @@ __global__ void __launch_bounds__(kNttThreads) k_ext_fused(const uint32_t* __res
 #pragma unroll
             for (int row = 0; row < 2 * ELL; row++)
                 mad_wide(s, P[row * kPadN + pidx(tid) + it * kPadStep], __ldg(rgsw + ((row * 2 + comp) * 2 + ch) * kN + k));
-            const uint32_t m = reduce64(s, cq.q, cq.barrett);
+            const uint32_t m = mod_crt(s, ch);
             outv[it][comp] = init ? addmod(__ldg(init + ((size_t)r * 4 + comp * 2 + ch) * kN + k), m, cq.q) : m;
         }
     }
