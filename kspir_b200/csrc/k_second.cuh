@@ -260,7 +260,6 @@ __global__ void __launch_bounds__(kNttThreads) k_pack_fused(const uint32_t* __re
         P[ELL * kPadN + pk] = neg ? negmod(vb, q) : vb;
     }
     cta_ntt_forward_m<ELL + 1>(P, kPadN, tws, ch);
-    const ChanConst cq = c_dev.ch[ch];
 #pragma unroll
     for (int it = 0; it < kPerThreadG; it++) {
         const int k = tid + it * kNttThreads;
