@@ -60,10 +60,12 @@ constexpr int kPerThread = kN / kNttThreads; // 8 coefficients per thread
 // parallel.  (One CTA per (rotation, component) doing both primes saves two
 // of the eight transforms per rotation but measured slower on B200 even for
 // batches of 64: these CTAs are latency-bound, not issue-bound.)
-template <int ELL>
-// Three CTAs per SM (at most 42 registers): with one (106 registers unbounded)
-// a batch of 64 ran 28 % slower.
-__global__ void __launch_bounds__(kNttThreads, 3) k_baby_rot(BabyArgs a, ClientKeysDev keys, NttTables tabs, Batch bt) {
+// MINB CTAs per SM: 2 (at most 64 registers) for one query -- its 252 CTAs fit
+// one wave with the most registers per thread -- and 3 (at most 42) for
+// batches, where occupancy wins (unbounded, 106 registers and one CTA per SM,
+// a batch of 64 ran 28 % slower).
+template <int ELL, int MINB>
+__global__ void __launch_bounds__(kNttThreads, MINB) k_baby_rot(BabyArgs a, ClientKeysDev keys, NttTables tabs, Batch bt) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
     {
         const size_t wo = ws_off(bt);

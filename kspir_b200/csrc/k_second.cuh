@@ -288,6 +288,119 @@ __global__ void __launch_bounds__(kNttThreads) k_pack_fused(const uint32_t* __re
 }
 
 // ---------------------------------------------------------------------------
+// packing level split over more CTAs, for single queries and small batches:
+// the fused kernel's CTA runs ELL + 1 forward and 2 inverse transforms in a
+// row, and the last levels have only 2 * I CTAs, so a level's latency is
+// those seven transforms.  Split, each CTA runs one:
+//   k_pack_split_fwd  (pair j, prime ch, d <= ELL): digit d (or temp.b for
+//                     d = ELL) -> transform -> its terms dig_d * key[d].a/.b
+//                     into part[j][ch][d][comp]
+//   k_pack_split_inv  (pair j, prime ch, comp): the sum of the terms ->
+//                     inverse transform -> + c2 into out[j]
+// Same residues as k_pack_fused (sums mod q in another order).
+constexpr int kPackPartPolys = 2 * 5 * 2;   // per pair: [prime][ELL + 1][comp]
+constexpr int kPackSplitSmem = kN * 8 + kPadN * 4;
+
+template <int ELL>
+__global__ void __launch_bounds__(kNttThreads) k_pack_split_fwd(const uint32_t* __restrict__ in,
+                                                                uint32_t* __restrict__ part,
+                                                                const uint32_t* __restrict__ key, int I,
+                                                                uint32_t ginv, NttTables tabs, GadgetB g, Batch bt) {
+    static_assert(2 * (ELL + 1) * 2 <= kPackPartPolys, "term buffer");
+    extern __shared__ __align__(16) uint8_t smem_raw[];
+    in = shifted(in, ws_off(bt));
+    part = shifted(part, ws_off(bt));
+    key = shifted(key, key_off(bt));
+    uint2* tws = reinterpret_cast<uint2*>(smem_raw);
+    uint32_t* S = reinterpret_cast<uint32_t*>(smem_raw + kN * 8);
+    const int d = blockIdx.x % (ELL + 1), ch = (blockIdx.x / (ELL + 1)) & 1, j = blockIdx.x / (ELL + 1) / 2;
+    const int tid = threadIdx.x;
+    const uint32_t* r0 = in + (size_t)j * 4 * kN;
+    const uint32_t* cc = in + (size_t)(I + j) * 4 * kN;
+    const uint32_t q = c_dev.ch[ch].q;
+    stage_twiddles(tws, tabs, ch, NTT_FWD);
+    auto cshift = [&](int comp, int pch, int p) -> uint32_t {   // (X^I c)[p]
+        const int s = p - I;
+        const uint32_t qq = pch ? kQ2 : kQ1;
+        return s >= 0 ? __ldg(cc + (comp * 2 + pch) * kN + s) : negmod(__ldg(cc + (comp * 2 + pch) * kN + s + kN), qq);
+    };
+#pragma unroll
+    for (int it = 0; it < kPerThreadG; it++) {
+        const int k = tid + it * kNttThreads;
+        bool neg;
+        const int src = auto_src(k, ginv, &neg);
+        uint32_t v;
+        if (d < ELL) {
+            uint32_t ra[2];
+#pragma unroll
+            for (int pch = 0; pch < 2; pch++) {
+                const uint32_t qq = pch ? kQ2 : kQ1;
+                const uint32_t x = submod(__ldg(r0 + (0 * 2 + pch) * kN + src), cshift(0, pch, src), qq);
+                ra[pch] = neg ? negmod(x, qq) : x;
+            }
+            int32_t dig[kMaxEll];
+            decompose_b(crt_compose_res(ra[0], ra[1]), kCrtMod, g, dig);
+            v = signed_to_res(dig[d], q);
+        } else {
+            const uint32_t vb = submod(__ldg(r0 + (1 * 2 + ch) * kN + src), cshift(1, ch, src), q);
+            v = neg ? negmod(vb, q) : vb;
+        }
+        S[pidx(tid) + it * kPadStep] = v;
+    }
+    cta_ntt_forward(S, tws, ch);
+    uint32_t* pa = part + (((size_t)j * 2 + ch) * (ELL + 1) + d) * 2 * kN;
+#pragma unroll
+    for (int it = 0; it < kPerThreadG; it++) {
+        const int k = tid + it * kNttThreads;
+        const uint32_t dv = S[pidx(tid) + it * kPadStep];
+        if (d < ELL) {
+            pa[k] = mod_crt((uint64_t)dv * __ldg(key + ((d * 2 + 0) * 2 + ch) * kN + k), ch);
+            pa[kN + k] = mod_crt((uint64_t)dv * __ldg(key + ((d * 2 + 1) * 2 + ch) * kN + k), ch);
+        } else {
+            pa[k] = dv;   // NTT(temp.b)
+        }
+    }
+}
+
+template <int ELL>
+__global__ void __launch_bounds__(kNttThreads) k_pack_split_inv(const uint32_t* __restrict__ in,
+                                                                const uint32_t* __restrict__ part,
+                                                                uint32_t* __restrict__ out, int I, NttTables tabs,
+                                                                Batch bt) {
+    extern __shared__ __align__(16) uint8_t smem_raw[];
+    in = shifted(in, ws_off(bt));
+    part = shifted(part, ws_off(bt));
+    out = shifted(out, ws_off(bt));
+    uint2* tws = reinterpret_cast<uint2*>(smem_raw);
+    uint32_t* S = reinterpret_cast<uint32_t*>(smem_raw + kN * 8);
+    const int comp = blockIdx.x & 1, ch = (blockIdx.x >> 1) & 1, j = blockIdx.x >> 2;
+    const int tid = threadIdx.x;
+    const uint32_t q = c_dev.ch[ch].q;
+    stage_twiddles(tws, tabs, ch, NTT_INV);
+    const uint32_t* pj = part + ((size_t)j * 2 + ch) * (ELL + 1) * 2 * kN;
+#pragma unroll
+    for (int it = 0; it < kPerThreadG; it++) {
+        const int k = tid + it * kNttThreads;
+        uint32_t sum = 0;
+#pragma unroll
+        for (int d = 0; d < ELL; d++) sum = addmod(sum, __ldg(pj + ((size_t)d * 2 + comp) * kN + k), q);
+        // a' = -sum_d dig_d key[d].a ;  b' = NTT(temp.b) - sum_d dig_d key[d].b
+        S[pidx(tid) + it * kPadStep] = comp == 0 ? negmod(sum, q) : submod(__ldg(pj + (size_t)ELL * 2 * kN + k), sum, q);
+    }
+    cta_ntt_inverse(S, tws, ch);
+    const uint32_t* r0 = in + (size_t)j * 4 * kN;
+    const uint32_t* cc = in + (size_t)(I + j) * 4 * kN + (comp * 2 + ch) * kN;
+#pragma unroll
+    for (int it = 0; it < kPerThreadG; it++) {
+        const int k = tid + it * kNttThreads;
+        const int s = k - I;
+        const uint32_t sh = s >= 0 ? __ldg(cc + s) : negmod(__ldg(cc + s + kN), q);
+        const uint32_t c2 = addmod(sh, __ldg(r0 + (comp * 2 + ch) * kN + k), q);
+        out[((size_t)j * 4 + comp * 2 + ch) * kN + k] = addmod(S[pidx(tid) + it * kPadStep], c2, q);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // fused external product: one CTA per (r, prime ch) runs externalProduct
 // (lwe.cpp:761-808) in shared memory:
 //   INTT(first_dim) (both primes, to compose) -> decompose_rlwe (2 ell rows)

@@ -273,6 +273,7 @@ Workspace ws_host(const kspir_ctx* c, int s) {
     w.ecoef = host_shift(w.ecoef, off);
     w.ext = host_shift(w.ext, off);
     w.ext2 = host_shift(w.ext2, off);
+    w.pkpart = host_shift(w.pkpart, off);
     w.err += (size_t)s * kErrStride;
     return w;
 }
@@ -377,6 +378,7 @@ int init_workspaces(kspir_ctx* c) {
         {(void**)&w.ecoef, (size_t)r * 4 * P},
         {(void**)&w.ext, (size_t)r * 4 * P},
         {(void**)&w.ext2, (size_t)half * 4 * P},
+        {(void**)&w.pkpart, (size_t)half * kPackPartPolys * P},
     };
     size_t total = 0;
     for (auto& pt : parts) total = align_up(total, 256) + pt.bytes;
@@ -448,6 +450,8 @@ int init_key_slots(kspir_ctx* c) {
 
 inline int blocks_for(long n, int t) { return (int)((n + t - 1) / t); }
 
+constexpr int kPackSplitMaxBatch = 4;   // batches up to this size pack with the split (latency) kernels
+
 // ---------------------------------------------------------------------------
 // launch sequence of `nq` queries in workspace slots slot0 .. slot0 + nq - 1
 // (blockIdx.y of every kernel is the query)
@@ -463,7 +467,11 @@ void enqueue_baby(kspir_ctx* c, int slot0, int nq, cudaStream_t st) {
     a1.cipherbuf = w.cipherbuf; a1.interA = w.interA; a1.interB = w.interB; a1.inter_bs = w.inter_bs;
     a1.N1 = c->N1; a1.col_base = 1; a1.inter_idx = c->N1h - 2;
     auto rot = [&](const BabyArgs& args, int nrot) {
-        if (nrot > 0) k_baby_rot<3><<<dim3(nrot * 4, nq), kNttThreads, kBabySmem, st>>>(args, c->keys0, c->ntabs, bt);
+        if (nrot <= 0) return;
+        if (nq == 1)
+            k_baby_rot<3, 2><<<dim3(nrot * 4, nq), kNttThreads, kBabySmem, st>>>(args, c->keys0, c->ntabs, bt);
+        else
+            k_baby_rot<3, 3><<<dim3(nrot * 4, nq), kNttThreads, kBabySmem, st>>>(args, c->keys0, c->ntabs, bt);
     };
     rot(a1, c->N1h - 1);
     k_ntt_jobs<true><<<dim3(2, nq), kNttThreads, kNttJobSmem, st>>>(c->jobs + c->seg_inter, c->ntabs, bt);
@@ -566,8 +574,15 @@ void enqueue_packing(kspir_ctx* c, int slot0, int nq, cudaStream_t st) {
         const int I = 1 << lv;
         const uint32_t ginv = inv_mod_2n((uint32_t)(kN / I + 1));
         uint32_t* out = (cur == w.ext) ? w.ext2 : w.ext;
-        k_pack_fused<4><<<dim3(I * 2, nq), kNttThreads, kPackSmem, st>>>(
-            cur, out, c->keys0.packing + (size_t)lv * pe * 4 * kN, I, ginv, c->ntabs, c->gad.pack, bt);
+        const uint32_t* key = c->keys0.packing + (size_t)lv * pe * 4 * kN;
+        if (nq <= kPackSplitMaxBatch) {   // latency: one transform per CTA
+            k_pack_split_fwd<4><<<dim3(I * 2 * 5, nq), kNttThreads, kPackSplitSmem, st>>>(cur, w.pkpart, key, I, ginv,
+                                                                                       c->ntabs, c->gad.pack, bt);
+            k_pack_split_inv<4><<<dim3(I * 4, nq), kNttThreads, kPackSplitSmem, st>>>(cur, w.pkpart, out, I, c->ntabs, bt);
+        } else {                          // throughput: the whole level per CTA pair
+            k_pack_fused<4><<<dim3(I * 2, nq), kNttThreads, kPackSmem, st>>>(cur, out, key, I, ginv, c->ntabs,
+                                                                             c->gad.pack, bt);
+        }
         cur = out;
     }
     k_compose_resp<<<dim3(2 * kN / 256, nq), 256, 0, st>>>(cur, w, bt);
@@ -575,8 +590,9 @@ void enqueue_packing(kspir_ctx* c, int slot0, int nq, cudaStream_t st) {
 
 // kernels launched by one enqueue_answer
 long answer_launches(const kspir_ctx* c, int kind, int nq) {
-    // clients 1, baby 7, scan, giant 2, external product 1, packing one per level + compose
-    return 1 + 7 + scan_launches(c, kind, nq) + (c->N2 > 1 ? 2 : 1) + 1 + c->levels + 1;
+    // clients 1, baby 7, scan, giant 2, external product 1, packing one or two per level + compose
+    const int per_level = nq <= kPackSplitMaxBatch ? 2 : 1;
+    return 1 + 7 + scan_launches(c, kind, nq) + (c->N2 > 1 ? 2 : 1) + 1 + per_level * c->levels + 1;
 }
 
 // Captures the four non-scan phases of (slot0, nq) as CUDA graphs (the scan
@@ -753,12 +769,15 @@ int kspir_ctx_create(int device, const kspir_params* params, kspir_ctx** out) {
     KS_CUDA(c.get(), cudaStreamCreateWithFlags(&c->capture, cudaStreamNonBlocking));
     if (const char* e = getenv("KSPIR_NO_GRAPHS")) c->use_graphs = !(e[0] == '1');
     KS_CUDA(c.get(), cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device));
-    KS_CUDA(c.get(), cudaFuncSetAttribute(k_baby_rot<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBabySmem));
+    KS_CUDA(c.get(), cudaFuncSetAttribute(k_baby_rot<3, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBabySmem));
+    KS_CUDA(c.get(), cudaFuncSetAttribute(k_baby_rot<3, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBabySmem));
     KS_CUDA(c.get(), cudaFuncSetAttribute(k_ntt_jobs<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kNttJobSmem));
     KS_CUDA(c.get(), cudaFuncSetAttribute(k_ntt_jobs<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kNttJobSmem));
     KS_CUDA(c.get(), cudaFuncSetAttribute(k_giant_fused<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGiantSmem));
     KS_CUDA(c.get(), cudaFuncSetAttribute(k_ext_fused<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kExtSmem));
     KS_CUDA(c.get(), cudaFuncSetAttribute(k_pack_fused<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, kPackSmem));
+    KS_CUDA(c.get(), cudaFuncSetAttribute(k_pack_split_fwd<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, kPackSplitSmem));
+    KS_CUDA(c.get(), cudaFuncSetAttribute(k_pack_split_inv<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, kPackSplitSmem));
 #define KS_ATTR(n) \
     KS_CUDA(c.get(), cudaFuncSetAttribute(k_scan<n>, cudaFuncAttributeMaxDynamicSharedMemorySize, ScanCfg<n>::SMEM));
     KS_ATTR(64) KS_ATTR(128) KS_ATTR(256)

@@ -52,6 +52,7 @@ struct Workspace {
     uint32_t* ecoef;        // [r][2 comp][2 ch][N] result, coefficient form
     uint32_t* ext;          // [r][2 comp][2 ch][N] external products, coefficient form
     uint32_t* ext2;         // [r/2][2 comp][2 ch][N] packing levels ping-pong with ext
+    uint32_t* pkpart;       // [r/2][2 ch][5][2 comp][N] terms of a split packing level
     uint64_t* resp64;       // [2][N] response words
     int* err;               // device error word (bounded waits), slot-indexed array
 };
@@ -98,6 +99,7 @@ __device__ __forceinline__ Workspace ws_at(Workspace w, const Batch& b) {
     w.ecoef = shifted(w.ecoef, off);
     w.ext = shifted(w.ext, off);
     w.ext2 = shifted(w.ext2, off);
+    w.pkpart = shifted(w.pkpart, off);
     w.err += (size_t)s * kErrStride;
     return w;
 }
