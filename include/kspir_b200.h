@@ -68,6 +68,25 @@ const char* kspir_strerror(int code);
  * r * N * N / 2 words, kept resident on the device. */
 int kspir_db_upload(kspir_ctx* ctx, const uint64_t* datacrt, size_t words);
 
+/* Server preprocessing on the device: reference database_tobsgsntt followed
+ * by database_tocrt (twosteps.h, twosteps.cpp:42-179; crt.cpp:859-885), for
+ * every sub-database k < r, as tests/test-pir.cpp:59-60 calls them.
+ *   data [r][N][N/2] words, data[k][i][j] = the reference's data[i][j] of
+ *        sub-database k; every word < bsgsp = 65537 (HEXL's inverse NTT
+ *        input range), else KSPIR_ERR_INVALID_ARG and the resident database is
+ *        left as it was.
+ * The result becomes the resident database, equal word for word to the
+ * datacrt the reference writes (kspir_db_upload of that datacrt is the same
+ * state).  device_ms (or NULL) receives the device time of validation and
+ * preprocessing.  Host buffer; returns when done. */
+int kspir_db_preprocess(kspir_ctx* ctx, const uint64_t* data, size_t words, float* device_ms);
+
+/* Same with the raw database already in device memory. */
+int kspir_db_preprocess_device(kspir_ctx* ctx, const uint64_t* d_data, size_t words, float* device_ms);
+
+/* Copies the resident database (datacrt layout, r * N * N / 2 words) to host. */
+int kspir_db_download(kspir_ctx* ctx, uint64_t* datacrt, size_t words);
+
 /* Replaces the permutations argument of matrix_vector_mul_bsgs_rns_crt_large
  * (twosteps.h:55-57). */
 int kspir_perms_upload(kspir_ctx* ctx, const int32_t* perms, size_t count);

@@ -24,8 +24,10 @@ constexpr uint32_t kBsMod = 16760833u; // crt.h:32
 constexpr uint64_t kBsModInvCrt = 51309461009346113ull;  // bsMod^-1 mod crtMod, crt.h:33
 constexpr uint32_t kCrtModInvBs = 3920321u;              // crtMod^-1 mod bsMod, crt.h:34
 
-// channels of the RNS representation
-enum Chan : int { CH_Q1 = 0, CH_Q2 = 1, CH_BS = 2, CH_COUNT = 3 };
+constexpr uint32_t kP = 65537u;        // plaintext modulus bsgsp, params.h:94
+
+// channels of the RNS representation (p: only for the database preprocessing)
+enum Chan : int { CH_Q1 = 0, CH_Q2 = 1, CH_BS = 2, CH_P = 3, CH_COUNT = 4 };
 
 // Per-channel constants, filled on the host (context.cu) and kept in
 // __constant__ memory.

@@ -20,6 +20,7 @@
 #include "common.cuh"
 #include "gadget.cuh"
 #include "k_baby.cuh"
+#include "k_db.cuh"
 #include "k_query.cuh"
 #include "k_scan.cuh"
 #include "k_scan_mma.cuh"
@@ -94,6 +95,27 @@ void slot_permutation(uint32_t g, uint16_t* sigma) {
 }
 
 uint32_t pow5(uint32_t e) { return (uint32_t)h_powmod(5, e, 2 * kN); }
+
+// Gather table of the database preprocessing: row R = k N1 + i of the
+// rearranged database takes entry G_i[j] of its diagonal row, where
+// G_i = query_encode^-1 o perm[i] (reference twosteps.cpp:104-118).
+// query_encode[t] = brv((rot_t - 1) / 2) with rot_t = 5^t mod 2N for t < N/2
+// and rot_{N-1-t} = -5^t mod 2N (utils.cpp:1473-1512, :1657-1675); perm[i] is
+// the slot permutation of X -> X^(5^i) (compute_permutation_matrix,
+// utils.cpp:1585-1619).
+std::vector<uint16_t> db_gather_table(int N1) {
+    std::vector<uint16_t> inv_qe(kN), perm(kN), g((size_t)N1 * kN);
+    for (uint32_t t = 0; t < (uint32_t)kN / 2; t++) {
+        const uint32_t rot = pow5(t);
+        inv_qe[h_bitrev12((rot - 1) / 2)] = (uint16_t)t;
+        inv_qe[h_bitrev12((2 * kN - rot - 1) / 2)] = (uint16_t)(kN - 1 - t);
+    }
+    for (int i = 0; i < N1; i++) {
+        slot_permutation(pow5((uint32_t)i), perm.data());
+        for (int j = 0; j < kN; j++) g[(size_t)i * kN + j] = inv_qe[perm[j]];
+    }
+    return g;
+}
 uint32_t inv_mod_2n(uint32_t g) { return (uint32_t)h_powmod(g, 2047, 2 * kN); }   // group order | 2048
 
 int ilog2i(int v) { int l = 0; while ((1 << l) < v) l++; return l; }
@@ -168,6 +190,8 @@ struct kspir_ctx {
     uint64_t* db = nullptr;
     bool db_loaded = false;
     bool mma = false;                 // batched tensor-core scan enabled (N1 = 128, several slots)
+    uint16_t* dbg = nullptr;          // gather table of the database preprocessing [N1][N]
+    int* dbflag = nullptr;            // its validation word
     uint8_t* dbop = nullptr;          // its database operand [N][2][G] tiles
     int G = 0;
     uint8_t* qop = nullptr;           // its query operand: launch at slot0 uses qop_at(slot0)
@@ -298,32 +322,41 @@ Batch batch_of(const kspir_ctx* c, int slot0) {
     return b;
 }
 
-int init_constants(kspir_ctx* c) {
+// the channel moduli, in Chan order
+const uint32_t kChanQ[CH_COUNT] = {kQ1, kQ2, kBsMod, kP};
+
+// every per-channel constant of c_dev (also written by the allocation-free set-up)
+DevConst make_dev_const() {
     DevConst dc{};
-    const uint32_t qs[3] = {kQ1, kQ2, kBsMod};
-    for (int ch = 0; ch < 3; ch++) {
+    for (int ch = 0; ch < CH_COUNT; ch++) {
         ChanConst& cc = dc.ch[ch];
-        cc.q = qs[ch];
-        cc.two_q = 2 * qs[ch];
-        cc.barrett = ~0ull / qs[ch];
-        cc.ninv = (uint32_t)h_invmod(kN, qs[ch]);
-        cc.ninv_p = shoup32(cc.ninv, qs[ch]);
-        cc.bsinv = ch < 2 ? (uint32_t)(kBsModInvCrt % qs[ch]) : 0;
-        cc.bsinv_p = shoup32(cc.bsinv, qs[ch]);
+        const uint32_t q = kChanQ[ch];
+        cc.q = q;
+        cc.two_q = 2 * q;
+        cc.barrett = ~0ull / q;
+        cc.ninv = (uint32_t)h_invmod(kN, q);
+        cc.ninv_p = shoup32(cc.ninv, q);
+        cc.bsinv = ch < 2 ? (uint32_t)(kBsModInvCrt % q) : 0;
+        cc.bsinv_p = shoup32(cc.bsinv, q);
     }
     dc.q1inv_mod_q2 = (uint32_t)h_invmod(kQ1 % kQ2, kQ2);
     dc.q1inv_mod_q2_p = shoup32(dc.q1inv_mod_q2, kQ2);
+    return dc;
+}
+
+int init_constants(kspir_ctx* c) {
+    const DevConst dc = make_dev_const();
     KS_CUDA(c, cudaMemcpyToSymbolAsync(c_dev, &dc, sizeof(dc), 0, cudaMemcpyHostToDevice, c->stream));
     KS_CUDA(c, cudaStreamSynchronize(c->stream));
 
     // twiddles: crt channels use root_of_unity_crt (reference crt.h:81) reduced
-    // per prime; bsMod uses HEXL's minimal primitive root
+    // per prime; bsMod and p use HEXL's minimal primitive root
     const uint64_t root_crt = 3375402822066082ull;
-    const uint64_t roots[3] = {root_crt % kQ1, root_crt % kQ2, h_min_root(kBsMod)};
+    const uint64_t roots[CH_COUNT] = {root_crt % kQ1, root_crt % kQ2, h_min_root(kBsMod), h_min_root(kP)};
     // per channel uint2 [2][N]: {psi^brv(k), Shoup} then {psi^-brv(k), Shoup}, k-major order
-    std::vector<uint32_t> tw(3 * 4 * kN);
-    for (int ch = 0; ch < 3; ch++) {
-        const uint64_t q = qs[ch], psi = roots[ch], pinv = h_invmod(psi, q);
+    std::vector<uint32_t> tw((size_t)CH_COUNT * 4 * kN);
+    for (int ch = 0; ch < CH_COUNT; ch++) {
+        const uint64_t q = kChanQ[ch], psi = roots[ch], pinv = h_invmod(psi, q);
         uint32_t* t = tw.data() + (size_t)ch * 4 * kN;
         for (int k = 0; k < kN; k++) {
             uint32_t e = h_bitrev12(k);
@@ -337,7 +370,7 @@ int init_constants(kspir_ctx* c) {
     }
     KS_CUDA(c, cudaMalloc(&c->tw, tw.size() * 4));
     KS_COPY(c, c->tw, tw.data(), tw.size() * 4, cudaMemcpyHostToDevice);
-    for (int ch = 0; ch < 3; ch++) c->ntabs.tw[ch] = reinterpret_cast<const uint2*>(c->tw + (size_t)ch * 4 * kN);
+    for (int ch = 0; ch < CH_COUNT; ch++) c->ntabs.tw[ch] = reinterpret_cast<const uint2*>(c->tw + (size_t)ch * 4 * kN);
 
     std::vector<uint16_t> sb((size_t)c->N1h * kN), sg((size_t)std::max(1, c->N2 - 1) * kN);
     for (int i = 0; i < c->N1h; i++) slot_permutation(pow5(i + 1), sb.data() + (size_t)i * kN);
@@ -771,6 +804,7 @@ int kspir_ctx_create(int device, const kspir_params* params, kspir_ctx** out) {
     KS_CUDA(c.get(), cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device));
     KS_CUDA(c.get(), cudaFuncSetAttribute(k_baby_rot<3, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBabySmem));
     KS_CUDA(c.get(), cudaFuncSetAttribute(k_baby_rot<3, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBabySmem));
+    KS_CUDA(c.get(), cudaFuncSetAttribute(k_db_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, kDbRowsSmem));
     KS_CUDA(c.get(), cudaFuncSetAttribute(k_ntt_jobs<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kNttJobSmem));
     KS_CUDA(c.get(), cudaFuncSetAttribute(k_ntt_jobs<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kNttJobSmem));
     KS_CUDA(c.get(), cudaFuncSetAttribute(k_giant_fused<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGiantSmem));
@@ -826,6 +860,8 @@ int kspir_ctx_destroy(kspir_ctx* c) {
     cudaFree(c->stage32);
     cudaFree(c->key_mem);
     cudaFree(c->db);
+    cudaFree(c->dbg);
+    cudaFree(c->dbflag);
     cudaFree(c->dbop);
     cudaFree(c->qop);
     cudaFree(c->perms);
@@ -848,6 +884,90 @@ int kspir_db_upload(kspir_ctx* c, const uint64_t* datacrt, size_t words) {
     int rc = build_dbop(c);
     if (rc) return rc;
     c->db_loaded = true;
+    return KSPIR_OK;
+}
+
+namespace {
+// Validates the raw database on the device, then overwrites the resident one
+// with its preprocessed form (k_db_rows), caller holds the lock.
+int db_preprocess_dev(kspir_ctx* c, const uint64_t* d_raw, float* device_ms) {
+    const int r = c->p.r;
+    const size_t words = (size_t)r * kN * (kN / 2);
+    cudaStream_t st = c->stream;
+    if (!c->dbg) {
+        const std::vector<uint16_t> g = db_gather_table(c->N1);
+        KS_CUDA(c, cudaMalloc(&c->dbflag, sizeof(int)));
+        KS_CUDA(c, cudaMalloc(&c->dbg, g.size() * 2));
+        KS_COPY(c, c->dbg, g.data(), g.size() * 2, cudaMemcpyHostToDevice);
+    }
+    if (!c->db) KS_CUDA(c, cudaMalloc(&c->db, words * 8));
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    if (device_ms) {
+        KS_CUDA(c, cudaEventCreate(&ev[0]));
+        KS_CUDA(c, cudaEventCreate(&ev[1]));
+        KS_CUDA(c, cudaEventRecord(ev[0], st));
+    }
+    int* flag = c->dbflag;
+    KS_CUDA(c, cudaMemsetAsync(flag, 0, sizeof(int), st));
+    k_check_canonical<<<c->nsm * 8, 256, 0, st>>>(d_raw, words, kP, flag);
+    KS_CUDA(c, cudaGetLastError());
+    int bad = 0;
+    KS_CUDA(c, cudaMemcpyAsync(&bad, flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+    KS_CUDA(c, cudaStreamSynchronize(st));
+    if (bad) {
+        if (device_ms) { cudaEventDestroy(ev[0]); cudaEventDestroy(ev[1]); }
+        return set_err(c, KSPIR_ERR_INVALID_ARG, "database entries must be below bsgsp = 65537");
+    }
+    c->db_loaded = false;
+    k_db_rows<<<dim3(kN / 2 / kDbRowsPerCta, r), kNttThreads, kDbRowsSmem, st>>>(d_raw, c->dbg, c->db, c->N1,
+                                                                                   c->ntabs);
+    KS_CUDA(c, cudaGetLastError());
+    int rc = build_dbop(c);   // synchronises
+    if (rc) return rc;
+    if (device_ms) {
+        KS_CUDA(c, cudaEventRecord(ev[1], st));
+        KS_CUDA(c, cudaEventSynchronize(ev[1]));
+        KS_CUDA(c, cudaEventElapsedTime(device_ms, ev[0], ev[1]));
+        cudaEventDestroy(ev[0]);
+        cudaEventDestroy(ev[1]);
+    }
+    KS_CUDA(c, cudaStreamSynchronize(st));
+    c->db_loaded = true;
+    return KSPIR_OK;
+}
+}  // namespace
+
+int kspir_db_preprocess(kspir_ctx* c, const uint64_t* data, size_t words, float* device_ms) {
+    if (!c || !data) return KSPIR_ERR_INVALID_ARG;
+    const size_t need = (size_t)c->p.r * kN * (kN / 2);
+    if (words != need) return set_err(c, KSPIR_ERR_INVALID_ARG, "raw database must be r*N*N/2 words");
+    std::lock_guard<std::mutex> lk(c->mu);
+    KS_CUDA(c, cudaSetDevice(c->device));
+    uint64_t* d_raw = nullptr;
+    KS_CUDA(c, cudaMalloc(&d_raw, need * 8));
+    int rc = copy_sync(c, d_raw, data, need * 8, cudaMemcpyHostToDevice);
+    if (!rc) rc = db_preprocess_dev(c, d_raw, device_ms);
+    cudaFree(d_raw);
+    return rc;
+}
+
+int kspir_db_preprocess_device(kspir_ctx* c, const uint64_t* d_data, size_t words, float* device_ms) {
+    if (!c || !d_data) return KSPIR_ERR_INVALID_ARG;
+    if (words != (size_t)c->p.r * kN * (kN / 2))
+        return set_err(c, KSPIR_ERR_INVALID_ARG, "raw database must be r*N*N/2 words");
+    std::lock_guard<std::mutex> lk(c->mu);
+    KS_CUDA(c, cudaSetDevice(c->device));
+    return db_preprocess_dev(c, d_data, device_ms);
+}
+
+int kspir_db_download(kspir_ctx* c, uint64_t* datacrt, size_t words) {
+    if (!c || !datacrt) return KSPIR_ERR_INVALID_ARG;
+    const size_t need = (size_t)c->p.r * kN * (kN / 2);
+    if (words != need) return set_err(c, KSPIR_ERR_INVALID_ARG, "database size must be r*N*N/2 words");
+    if (!c->db_loaded) return set_err(c, KSPIR_ERR_NOT_READY, "database not uploaded");
+    std::lock_guard<std::mutex> lk(c->mu);
+    KS_CUDA(c, cudaSetDevice(c->device));
+    KS_COPY(c, datacrt, c->db, need * 8, cudaMemcpyDeviceToHost);
     return KSPIR_OK;
 }
 
@@ -1358,20 +1478,7 @@ int na_setup(int device, cudaStream_t st) {
         cudaFuncSetAttribute(k_ntt_jobs<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kNttJobSmem) != cudaSuccess ||
         cudaFuncSetAttribute(k_ext_mac_intt, cudaFuncAttributeMaxDynamicSharedMemorySize, kMacSmem) != cudaSuccess)
         return KSPIR_ERR_CUDA;
-    DevConst dc{};
-    const uint32_t qs[3] = {kQ1, kQ2, kBsMod};
-    for (int ch = 0; ch < 3; ch++) {
-        ChanConst& cc = dc.ch[ch];
-        cc.q = qs[ch];
-        cc.two_q = 2 * qs[ch];
-        cc.barrett = ~0ull / qs[ch];
-        cc.ninv = (uint32_t)h_invmod(kN, qs[ch]);
-        cc.ninv_p = shoup32(cc.ninv, qs[ch]);
-        cc.bsinv = ch < 2 ? (uint32_t)(kBsModInvCrt % qs[ch]) : 0;
-        cc.bsinv_p = shoup32(cc.bsinv, qs[ch]);
-    }
-    dc.q1inv_mod_q2 = (uint32_t)h_invmod(kQ1 % kQ2, kQ2);
-    dc.q1inv_mod_q2_p = shoup32(dc.q1inv_mod_q2, kQ2);
+    const DevConst dc = make_dev_const();   // the same constants a context writes
     if (cudaMemcpyToSymbolAsync(c_dev, &dc, sizeof(dc), 0, cudaMemcpyHostToDevice, st) != cudaSuccess)
         return KSPIR_ERR_CUDA;
     const uint64_t root_crt = 3375402822066082ull;

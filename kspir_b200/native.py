@@ -41,6 +41,9 @@ SIGNATURES = {
     "kspir_last_error": (ctypes.c_char_p, [_vp]),
     "kspir_strerror": (ctypes.c_char_p, [_i]),
     "kspir_db_upload": (_i, [_vp, _vp, _sz]),
+    "kspir_db_preprocess": (_i, [_vp, _vp, _sz, _vp]),
+    "kspir_db_preprocess_device": (_i, [_vp, _vp, _sz, _vp]),
+    "kspir_db_download": (_i, [_vp, _vp, _sz]),
     "kspir_perms_upload": (_i, [_vp, _vp, _sz]),
     "kspir_client_keys_upload": (_i, [_vp, _i, _vp, _vp, _vp, _vp]),
     "kspir_answer": (_i, [_vp, _i, _vp, _vp]),
@@ -191,6 +194,27 @@ class Context:
     def upload_db(self, datacrt):
         d = _u64(datacrt).reshape(-1)
         self._check(self.lib.kspir_db_upload(self._h, ptr(d), d.size))
+
+    def preprocess_db(self, raw) -> float:
+        """Reference database_tobsgsntt + database_tocrt of every sub-database
+        (twosteps.cpp:42-179, crt.cpp:859-885) on the device; the result
+        becomes the resident database.  Returns the device time in ms."""
+        d = _u64(raw).reshape(-1)
+        ms = ctypes.c_float(0.0)
+        self._check(self.lib.kspir_db_preprocess(self._h, ptr(d), d.size, ctypes.byref(ms)))
+        return ms.value
+
+    def preprocess_db_device(self, d_raw: int, words: int) -> float:
+        ms = ctypes.c_float(0.0)
+        self._check(self.lib.kspir_db_preprocess_device(self._h, ctypes.c_void_p(d_raw), words, ctypes.byref(ms)))
+        return ms.value
+
+    def download_db(self, out: np.ndarray | None = None) -> np.ndarray:
+        words = self.r * N * N // 2
+        if out is None:
+            out = np.empty(words, dtype=np.uint64)
+        self._check(self.lib.kspir_db_download(self._h, ptr(out), out.size))
+        return out
 
     def upload_perms(self, perms):
         p = np.ascontiguousarray(perms, dtype=np.int32).reshape(-1)

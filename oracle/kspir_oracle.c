@@ -474,6 +474,61 @@ void ko_permutation_matrix(int32_t* perms, int N1) {
 }
 
 /* ------------------------------------------------------------------ */
+/* database preprocessing, twosteps.cpp:42-179 and crt.cpp:859-885      */
+
+/* query_encode, utils.cpp:1657-1675: find_index[rotate_index[i] / 2] */
+static void query_encode(int32_t* qe) {
+    int32_t* hexl_idx = malloc(sizeof(int32_t) * N);
+    int32_t* rot = malloc(sizeof(int32_t) * N);
+    int32_t* find = malloc(sizeof(int32_t) * N);
+    hexl_rotate_indexes(hexl_idx, rot);
+    for (int i = 0; i < N; i++) find[hexl_idx[i] >> 1] = i;
+    for (int i = 0; i < N; i++) qe[i] = find[rot[i] / 2];
+    free(hexl_idx); free(rot); free(find);
+}
+
+int ko_db_preprocess(const uint64_t* raw, int N1, uint64_t* datacrt) {
+    const int H = N / 2, N2 = N / 2 / N1;
+    for (size_t i = 0; i < (size_t)N * H; i++)
+        if (raw[i] >= KO_P) return -1;
+    int32_t* qe = malloc(sizeof(int32_t) * N);
+    int32_t* perms = malloc(sizeof(int32_t) * (size_t)N1 * N);
+    uint64_t* rows = malloc(8 * (size_t)H * N);
+    uint64_t* row = malloc(8 * N);
+    uint64_t* tmp = malloc(8 * N);
+    query_encode(qe);
+    ko_permutation_matrix(perms, N1);
+    /* diagonal rearrangement, twosteps.cpp:64-74 */
+    for (int i = 0; i < H; i++)
+        for (int j = 0; j < H; j++) {
+            int rr = (j - i + H) & (H - 1);
+            rows[(size_t)i * N + j] = raw[(size_t)rr * H + j];
+            rows[(size_t)i * N + N - 1 - j] = raw[(size_t)(N - 1 - rr) * H + j];
+        }
+    for (int k = 0; k < N2; k++)
+        for (int i = 0; i < N1; i++) {
+            uint64_t* x = rows + ((size_t)k * N1 + i) * N;
+            /* permutation, twosteps.cpp:104-118 */
+            for (int j = 0; j < N; j++) tmp[qe[j]] = x[j];
+            for (int j = 0; j < N; j++) row[j] = tmp[perms[(size_t)i * N + j]];
+            /* encode, twosteps.cpp:156-176 */
+            ko_ntt_inverse(row, KO_P);
+            for (int j = 0; j < N; j++)
+                if (row[j] > KO_P / 2) row[j] += KO_CRTMOD - KO_P;
+            ko_ntt_forward(row, KO_CRTMOD);
+            memcpy(x, row, 8 * N);
+        }
+    /* crt form, crt.cpp:868-880 */
+    for (int z = 0; z < N; z++)
+        for (int R = 0; R < H; R++) {
+            uint64_t t = rows[(size_t)R * N + z];
+            datacrt[(size_t)z * H + R] = ko_barrett_coeff(t, 0) | ko_barrett_coeff(t, 1) << 32;
+        }
+    free(qe); free(perms); free(rows); free(row); free(tmp);
+    return 0;
+}
+
+/* ------------------------------------------------------------------ */
 /* first dimension, twosteps.cpp                                        */
 
 #define POLY(p, i) ((p) + (size_t)(i) * N)

@@ -57,6 +57,11 @@ int ko_packing(uint64_t* rlwes_inout, int r, const uint64_t* packing, uint64_t* 
 /* One sub-database DB scan (crt.cpp:643-856): out [N2][2N]. */
 void ko_scan(const uint64_t* db, const uint64_t* cipherbuf, int N1, uint64_t* out);
 
+/* Server preprocessing of one sub-database: database_tobsgsntt then
+ * database_tocrt (twosteps.cpp:42-179, crt.cpp:859-885).  raw [N][N/2] words
+ * < p (else -1), datacrt [N][N/2]. */
+int ko_db_preprocess(const uint64_t* raw, int N1, uint64_t* datacrt);
+
 /* HEXL-order negacyclic transforms for modulus in {crtMod, bsMod, p, q1, q2}. */
 int ko_ntt_forward(uint64_t* a, uint64_t modulus);
 int ko_ntt_inverse(uint64_t* a, uint64_t modulus);

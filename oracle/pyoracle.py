@@ -78,6 +78,7 @@ def lib():
             L.ko_permutation_matrix.argtypes = [vp, ctypes.c_int]
             L.ko_pow_mod_index.argtypes = [ctypes.c_int, ctypes.c_int]
             L.ko_giant_steps.argtypes = [vp, vp, ctypes.c_int, vp]
+            L.ko_db_preprocess.argtypes = [vp, ctypes.c_int, vp]
             _lib = L
     return _lib
 
@@ -111,6 +112,9 @@ def ref():
             L.ref_decompose_bsgs.argtypes = [vp, vp, vp, vp]
             L.ref_decompose.argtypes = [vp, ctypes.c_int, ctypes.c_uint64, ctypes.c_uint64, vp]
             L.ref_decompose_rlwe.argtypes = [vp, vp, ctypes.c_int, ctypes.c_uint64, ctypes.c_uint64, vp]
+            L.ref_pir_keep_raw.argtypes = [ctypes.c_int]
+            L.ref_pir_get_raw.argtypes = [vp]
+            L.ref_db_preprocess.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp]
             _ref = L
     return _ref
 
@@ -197,6 +201,25 @@ def giant_steps(output, N1, giant):
 def scan(db_sub, cipherbuf, N1):
     out = np.zeros((N // 2 // N1) * 2 * N, dtype=np.uint64)
     lib().ko_scan(_p(db_sub), _p(cipherbuf), N1, _p(out))
+    return out
+
+
+def db_preprocess(raw, r, N1):
+    """database_tobsgsntt + database_tocrt of every sub-database (restatement)."""
+    num = N * N // 2
+    raw = np.ascontiguousarray(raw, dtype=np.uint64)
+    out = np.empty(r * num, dtype=np.uint64)
+    for k in range(r):
+        if lib().ko_db_preprocess(_p(raw[k * num:(k + 1) * num]), N1, _p(out[k * num:(k + 1) * num])):
+            raise ValueError("database entries must be below p")
+    return out
+
+
+def ref_db_preprocess(raw, r, N1):
+    """The same through the reference's own database_tobsgsntt / database_tocrt."""
+    raw = np.ascontiguousarray(raw, dtype=np.uint64)
+    out = np.empty(r * N * N // 2, dtype=np.uint64)
+    ref().ref_db_preprocess(_p(raw), r, N1, _p(out))
     return out
 
 

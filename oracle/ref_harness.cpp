@@ -99,7 +99,9 @@ struct PirState {
     Secret* key = nullptr;
     std::vector<uint64_t> query, baby, giant, packing, rgsw;
     std::vector<int32_t> perms;
+    std::vector<uint64_t> raw;   // the sampled database before preprocessing (kept on request)
 };
+bool g_keep_raw = false;
 PirState g_state;
 
 }  // namespace
@@ -130,6 +132,11 @@ int ref_pir_setup(uint32_t seed, int r, int N1) {
         for (size_t i = 0; i < (size_t)N; i++) input_record[i] = data[i][s.target_col];
         inverse_encode(input_record);
         for (size_t i = 0; i < (size_t)N; i++) data[i][s.target_col] = input_record[i];
+        if (g_keep_raw) {
+            s.raw.resize(num_words * (k + 1));
+            for (size_t i = 0; i < (size_t)N; i++)
+                memcpy(s.raw.data() + num_words * k + i * (N / 2), data[i].data(), (N / 2) * 8);
+        }
         database_tobsgsntt(data_ntt, data, crtMod, N1);
         database_tocrt(s.datacrt.data() + num_words * k, data_ntt, N1);
     }
@@ -175,6 +182,28 @@ int ref_pir_setup(uint32_t seed, int r, int N1) {
     s.perms.assign((size_t)N1 * kPoly, 0);
     for (int i = 0; i < N1; i++) memcpy(s.perms.data() + (size_t)i * kPoly, permutations[i].data(), kPoly * 4);
     return 0;
+}
+
+// Keep (1) the sampled database of the next ref_pir_setup before preprocessing.
+void ref_pir_keep_raw(int keep) { g_keep_raw = keep != 0; }
+
+// The kept database: [r][N][N/2], data[i][j] of sub-database k at (k N + i) N/2 + j.
+void ref_pir_get_raw(uint64_t* raw) {
+    if (raw && !g_state.raw.empty()) memcpy(raw, g_state.raw.data(), g_state.raw.size() * 8);
+}
+
+// database_tobsgsntt + database_tocrt of every sub-database, as
+// tests/test-pir.cpp:59-60 calls them: raw [r][N][N/2] -> datacrt [r][N][N/2].
+void ref_db_preprocess(const uint64_t* raw, int r, int N1, uint64_t* datacrt) {
+    const size_t num_words = (size_t)N * N / 2;
+    std::vector<std::vector<uint64_t> > data(N, std::vector<uint64_t>(N / 2, 0));
+    std::vector<std::vector<uint64_t> > data_ntt(N / 2, std::vector<uint64_t>(N, 0));
+    for (int k = 0; k < r; k++) {
+        for (size_t i = 0; i < (size_t)N; i++)
+            memcpy(data[i].data(), raw + num_words * k + i * (N / 2), (N / 2) * 8);
+        database_tobsgsntt(data_ntt, data, crtMod, N1);
+        database_tocrt(datacrt + num_words * k, data_ntt, N1);
+    }
 }
 
 void ref_pir_target(uint32_t* col, uint32_t* packing_slot) {

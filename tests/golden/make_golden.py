@@ -8,6 +8,9 @@ Runs the reference's own sources (compiled by ``make -C oracle ref`` into
 * a replay of ``tests/test-pir.cpp`` (glibc ``rand()`` stream after
   ``srand(seed)``, reference keygen, preprocessing and query) -- the response
   digest and the decrypted record (the known answer [1, 2, ..., 4096]);
+* database preprocessing (database_tobsgsntt + database_tocrt) of seeded
+  raw databases (``kspir_b200.synth.gen_raw_db``), of an edge-value pattern
+  and of the database test-pir.cpp samples -- input and output digests;
 * small unit vectors of the reference helpers (crt_compose, barrett_coeff,
   the decompositions) on edge values.
 
@@ -33,6 +36,8 @@ from oracle import pyoracle as po  # noqa: E402
 N = po.N
 CASES = [(2, 128, 5), (1, 128, 3), (4, 64, 7), (2, 256, 11)]
 TESTPIR = (1, 16, 128)   # seed, r, N1
+PREPROCESS = [(31, 1, 128), (32, 1, 64), (33, 1, 256), (34, 2, 128)]
+PREPROCESS_TESTPIR = (3, 2, 128)
 
 
 def sha(a: np.ndarray) -> str:
@@ -89,6 +94,29 @@ def main():
                           db_sha=sha(db), query_sha=sha(c["query"]), response_sha=sha(resp),
                           response_head=head(resp), bsgs_sha=sha(bsgs), ext_sha=sha(ext),
                           decrypted_head=head(msg, 16), decrypted_is_1_to_N=bool((msg == np.arange(1, N + 1)).all()))
+
+    # database preprocessing
+    from kspir_b200 import synth
+    pre = []
+    for seed, r, N1 in PREPROCESS:
+        raw = synth.gen_raw_db(seed, r)
+        dc = po.ref_db_preprocess(raw, r, N1)
+        pre.append(dict(kind="synthetic", seed=seed, r=r, N1=N1, raw_sha=sha(raw), datacrt_sha=sha(dc),
+                        datacrt_head=head(dc)))
+    raw = synth.edge_raw_db()
+    dc = po.ref_db_preprocess(raw, 1, 128)
+    pre.append(dict(kind="edges", r=1, N1=128, raw_sha=sha(raw), datacrt_sha=sha(dc), datacrt_head=head(dc)))
+    seed, r, N1 = PREPROCESS_TESTPIR
+    L.ref_pir_keep_raw(1)
+    L.ref_pir_setup(seed, r, N1)
+    L.ref_pir_keep_raw(0)
+    raw = np.zeros(r * N * N // 2, np.uint64)
+    L.ref_pir_get_raw(po._p(raw))
+    dc = np.zeros(r * N * N // 2, np.uint64)
+    L.ref_pir_get_inputs(po._p(dc), None, None, None, None, None, None)
+    pre.append(dict(kind="testpir", seed=seed, r=r, N1=N1, raw_sha=sha(raw), datacrt_sha=sha(dc),
+                    datacrt_head=head(dc)))
+    out["preprocess"] = pre
 
     # unit vectors on edge values
     edge64 = [0, 1, 2 ** 28 - 1, po.Q1 - 1, po.Q1, po.Q2, 2 ** 32 - 1, 2 ** 56 - 1, 2 ** 62, 2 ** 63 - 1,

@@ -220,3 +220,46 @@ def test_testpir_replay_known_answer():
     msg = np.zeros(N, np.uint64)
     L.ref_pir_decrypt(po._p(resp), po._p(msg))
     assert (msg == np.arange(1, N + 1)).all()
+
+
+# ---------------------------------------------------------------------------
+# database preprocessing (database_tobsgsntt + database_tocrt)
+
+@pytest.mark.parametrize("case", GOLDEN["preprocess"], ids=lambda c: f"{c['kind']}_r{c['r']}_N1{c['N1']}")
+def test_db_preprocess_matches_reference_golden(case):
+    from kspir_b200 import synth
+    if case["kind"] == "testpir":
+        pytest.skip("the raw database of the test-pir.cpp replay comes from the reference build")
+    if case["kind"] == "edges":
+        raw = synth.edge_raw_db()
+    else:
+        raw = synth.gen_raw_db(case["seed"], case["r"])
+    assert sha(raw) == case["raw_sha"]
+    out = po.db_preprocess(raw, case["r"], case["N1"])
+    assert [int(x) for x in out[:8]] == case["datacrt_head"]
+    assert sha(out) == case["datacrt_sha"]
+
+
+def test_db_preprocess_rejects_words_at_or_above_p():
+    raw = np.zeros(N * N // 2, np.uint64)
+    raw[12345] = po.P
+    with pytest.raises(ValueError):
+        po.db_preprocess(raw, 1, 128)
+
+
+@needs_ref
+def test_db_preprocess_equals_reference_on_testpir_database():
+    g = [c for c in GOLDEN["preprocess"] if c["kind"] == "testpir"][0]
+    seed, r, N1 = g["seed"], g["r"], g["N1"]
+    L = po.ref()
+    L.ref_pir_keep_raw(1)
+    L.ref_pir_setup(seed, r, N1)
+    L.ref_pir_keep_raw(0)
+    raw = np.zeros(r * N * N // 2, np.uint64)
+    L.ref_pir_get_raw(po._p(raw))
+    assert sha(raw) == g["raw_sha"]
+    out = po.db_preprocess(raw, r, N1)
+    assert sha(out) == g["datacrt_sha"]
+    live = np.zeros_like(out)
+    L.ref_pir_get_inputs(po._p(live), None, None, None, None, None, None)
+    assert (live == out).all()
