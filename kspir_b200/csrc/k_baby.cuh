@@ -38,7 +38,17 @@ struct BabyArgs {
     int32_t N1;
     int32_t col_base;        // cipherbuf column of key index 0
     int32_t inter_idx;       // key index whose pre-modswitch state is exported, or -1
+    int32_t cb_rm;           // 1: write cipherbuf rotation-major (see cipherbuf_rm_idx)
 };
+
+// Rotation-major cipherbuf, the layout the tensor-core scan's operand split
+// reads: u32 [N1 columns][2 comp][2 primes][N slots], so that a rotation's
+// CTA writes whole contiguous polynomials.  The reference layout
+// ([N][N1][2] words, primes packed in one word) scatters every 4-byte store
+// across a 16 * N1-byte stride; the CUDA-core scan streams it per slot.
+__host__ __device__ __forceinline__ size_t cipherbuf_rm_idx(int col, int comp, int ch, int z) {
+    return ((size_t)(col * 2 + comp) * 2 + ch) * kN + z;
+}
 
 // 5^e mod 2N
 __device__ __forceinline__ uint32_t pow5_mod2n(uint32_t e) {
@@ -165,7 +175,10 @@ __global__ void __launch_bounds__(kNttThreads, MINB) k_baby_rot(BabyArgs a, Clie
         if (comp == 1) A = addmod(A, __ldg(a.srcB + ch * kN + sig[k]), cc.q);
         if (inter) inter_out[ch * kN + k] = A;
         const uint32_t r = shoup_mul(submod(A, S[pidx(tid) + it * kPadStep], cc.q), cc.bsinv, cc.bsinv_p, cc.q);
-        cb32[(((size_t)k * a.N1 + col) * 2 + comp) * 2 + ch] = r;
+        if (a.cb_rm)
+            cb32[cipherbuf_rm_idx(col, comp, ch, k)] = r;
+        else
+            cb32[(((size_t)k * a.N1 + col) * 2 + comp) * 2 + ch] = r;
     }
 }
 

@@ -340,56 +340,66 @@ __global__ void __launch_bounds__(MmaCfg<BT>::THREADS, 1) k_scan_mma(ScanMmaArgs
 
 // Query operand of a batch: qop[z][ch][qt] tiles of 8 BT rows
 // n = mma_brow(comp * BT + b, lb), byte k = limb lb of the prime-ch residue of
-// cipherbuf[z][k][comp] of query qt * BT + b (workspace slot slot0 + that);
-// queries past nq are zero.  One thread per (z, qt, b, 16-byte chunk): it reads
-// the 16 cipherbuf entries of its chunk (256 contiguous bytes: both components
-// and both primes) and writes 16 chunks of 16 bytes.
+// entry (k, comp) of slot z of the cipherbuf of query qt * BT + b (workspace
+// slot slot0 + that); queries past nq are zero.  Built from the
+// rotation-major cipherbuf (cipherbuf_rm_idx: u32 [k][comp][ch][z]), a
+// transpose: one CTA per (block of 32 slots, query slot qt * BT + b).  The
+// CTA loads the 512 rows (k, comp, ch) of its slots
+// (128 contiguous bytes each) into shared memory, column zz stored at
+// zz ^ 4 (k / 16) so that the reads below hit 32 distinct banks, then each
+// thread takes slot zz and 16-entry chunk c of every (comp, ch): 16 words,
+// byte-transposed into the 4 limb rows' 16-byte chunks (eight threads write
+// the 128 bytes of one tile row).
+constexpr int kSplitZ = 32;
+constexpr int kSplitSmem = kMmaK * 4 * kSplitZ * 4;   // 64 KiB
+
 template <int BT>
-__global__ void k_qop_split(const uint64_t* __restrict__ cb0, size_t ws_bytes, int slot0, int nq, int QT,
-                            uint8_t* __restrict__ qop) {
+__global__ void __launch_bounds__(256) k_qop_split_rm(const uint32_t* __restrict__ cb0, size_t ws_bytes, int slot0,
+                                                     int nq, int QT, uint8_t* __restrict__ qop) {
     using C = MmaCfg<BT>;
-    const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long total = (long)kN * QT * BT * 8;
-    if (idx >= total) return;
-    const int c = (int)(idx & 7);
-    const int b = (int)((idx >> 3) % BT);
-    const long zq = (idx >> 3) / BT;            // z * QT + qt
-    const int qt = (int)(zq % QT), z = (int)(zq / QT);
-    const int bq = qt * BT + b;
-    uint4 w[16];   // entry k = 16 c + j: (comp 0 ch 0, comp 0 ch 1, comp 1 ch 0, comp 1 ch 1)
-    if (bq < nq) {
-        const uint4* cb = reinterpret_cast<const uint4*>(reinterpret_cast<const char*>(cb0) +
-                                                         (size_t)(slot0 + bq) * ws_bytes) +
-                          (size_t)z * kMmaK + 16 * c;
-#pragma unroll
-        for (int j = 0; j < 16; j++) w[j] = __ldg(cb + j);
-    } else {
-#pragma unroll
-        for (int j = 0; j < 16; j++) w[j] = make_uint4(0, 0, 0, 0);
+    extern __shared__ __align__(16) uint8_t smem_raw[];
+    uint32_t* V = reinterpret_cast<uint32_t*>(smem_raw);   // [512 rows][32 columns]
+    const int z0 = blockIdx.x * kSplitZ;
+    const int bq = blockIdx.y;                              // qt * BT + b
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const bool live = bq < nq;
+    if (live) {
+        const uint32_t* cb = reinterpret_cast<const uint32_t*>(reinterpret_cast<const char*>(cb0) +
+                                                              (size_t)(slot0 + bq) * ws_bytes);
+#pragma unroll 8
+        for (int row = warp; row < kMmaK * 4; row += 8)
+            V[row * kSplitZ + (lane ^ (4 * ((row >> 6) & 7)))] = __ldg(cb + (size_t)row * kN + z0 + lane);
+        __syncthreads();
     }
+    const int c = tid & 7;                                  // 16-entry chunk of k
+    const int zz = 4 * warp + ((tid >> 3) & 3);
+    const int z = z0 + zz;
+    const int qt = bq / BT, b = bq % BT;
 #pragma unroll
-    for (int ch = 0; ch < 2; ch++) {
+    for (int cv = 0; cv < 4; cv++) {
+        const int comp = cv >> 1, ch = cv & 1;
+        uint32_t w[4][4];   // [limb][word]
+#pragma unroll
+        for (int g = 0; g < 4; g++) {
+            uint32_t v[4];
+#pragma unroll
+            for (int t = 0; t < 4; t++) {
+                const int row = (16 * c + 4 * g + t) * 4 + cv;
+                v[t] = live ? V[row * kSplitZ + (zz ^ (4 * c))] : 0u;
+            }
+            // 4 x 4 byte transpose: word g of limb lb = byte lb of v[0..3]
+            const uint32_t t0 = __byte_perm(v[0], v[1], 0x5140), t1 = __byte_perm(v[0], v[1], 0x7362);
+            const uint32_t t2 = __byte_perm(v[2], v[3], 0x5140), t3 = __byte_perm(v[2], v[3], 0x7362);
+            w[0][g] = __byte_perm(t0, t2, 0x5410);
+            w[1][g] = __byte_perm(t0, t2, 0x7632);
+            w[2][g] = __byte_perm(t1, t3, 0x5410);
+            w[3][g] = __byte_perm(t1, t3, 0x7632);
+        }
         uint8_t* tile = qop + (((size_t)z * 2 + ch) * QT + qt) * C::BTILE;
 #pragma unroll
-        for (int comp = 0; comp < 2; comp++) {
-#pragma unroll
-            for (int lb = 0; lb < 4; lb++) {
-                uint32_t pk[4];
-#pragma unroll
-                for (int q4 = 0; q4 < 4; q4++) {
-                    uint32_t x = 0;
-#pragma unroll
-                    for (int t = 0; t < 4; t++) {
-                        const uint4 e = w[4 * q4 + t];
-                        const uint32_t v = comp == 0 ? (ch == 0 ? e.x : e.y) : (ch == 0 ? e.z : e.w);
-                        x |= ((v >> (8 * lb)) & 255u) << (8 * t);
-                    }
-                    pk[q4] = x;
-                }
-                const int n = mma_brow(comp * BT + b, lb);
-                *reinterpret_cast<uint4*>(tile + sw128_off(n, 16 * c)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
-            }
-        }
+        for (int lb = 0; lb < 4; lb++)
+            *reinterpret_cast<uint4*>(tile + sw128_off(mma_brow(comp * BT + b, lb), 16 * c)) =
+                make_uint4(w[lb][0], w[lb][1], w[lb][2], w[lb][3]);
     }
 }
 

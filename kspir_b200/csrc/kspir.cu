@@ -213,7 +213,7 @@ struct kspir_ctx {
     int* client_of = nullptr;         // [slots]
     uint32_t* stage32 = nullptr;      // [r][4][N] residues for the staged entry points
     NttJob* jobs = nullptr;           // transform job lists of slot 0
-    int seg_q = 0, n_q = 0, seg_inter = 0, seg_dig1 = 0;
+    int seg_q = 0, seg_q_rm = 0, n_q = 0, seg_inter = 0, seg_dig1 = 0;
     // client keys: key slot k is slot 0's layout shifted by k * key_bytes
     uint32_t* key_mem = nullptr;
     size_t key_bytes = 0;
@@ -439,16 +439,21 @@ int init_workspaces(kspir_ctx* c) {
     auto add = [&](const uint32_t* src, uint32_t* dst, int ch, int stride) {
         NttJob j; j.src = src; j.dst = dst; j.ch = ch; j.dst_stride = stride; jobs.push_back(j);
     };
-    // query: dig0 (9), query b crt (2), modswitched query -> cipherbuf column 0 (4)
-    c->seg_q = (int)jobs.size();
-    for (int j = 0; j < 3; j++)
-        for (int ch = 0; ch < 3; ch++) add(w.dig0 + (j * 3 + ch) * kN, w.dig0 + (j * 3 + ch) * kN, ch, 1);
-    for (int ch = 0; ch < 2; ch++) add(w.qbn + ch * kN, w.qbn + ch * kN, ch, 1);
+    // query: dig0 (9), query b crt (2), modswitched query -> cipherbuf column 0 (4);
+    // a second copy writes column 0 of the rotation-major cipherbuf
     uint32_t* cb32 = reinterpret_cast<uint32_t*>(w.cipherbuf);
-    for (int comp = 0; comp < 2; comp++)
-        for (int ch = 0; ch < 2; ch++)
-            add(w.col0 + (comp * 2 + ch) * kN, cb32 + 2 * comp + ch, ch, 4 * N1);
-    c->n_q = (int)jobs.size() - c->seg_q;
+    for (int rm = 0; rm < 2; rm++) {
+        (rm ? c->seg_q_rm : c->seg_q) = (int)jobs.size();
+        for (int j = 0; j < 3; j++)
+            for (int ch = 0; ch < 3; ch++) add(w.dig0 + (j * 3 + ch) * kN, w.dig0 + (j * 3 + ch) * kN, ch, 1);
+        for (int ch = 0; ch < 2; ch++) add(w.qbn + ch * kN, w.qbn + ch * kN, ch, 1);
+        for (int comp = 0; comp < 2; comp++)
+            for (int ch = 0; ch < 2; ch++) {
+                if (rm) add(w.col0 + (comp * 2 + ch) * kN, cb32 + cipherbuf_rm_idx(0, comp, ch, 0), ch, 1);
+                else add(w.col0 + (comp * 2 + ch) * kN, cb32 + 2 * comp + ch, ch, 4 * N1);
+            }
+        c->n_q = (int)jobs.size() - (rm ? c->seg_q_rm : c->seg_q);
+    }
     c->seg_inter = (int)jobs.size();
     for (int ch = 0; ch < 2; ch++) add(w.interA + ch * kN, w.inter_acoef + ch * kN, ch, 1);
     c->seg_dig1 = (int)jobs.size();
@@ -490,12 +495,15 @@ constexpr int kPackSplitMaxBatch = 4;   // batches up to this size pack with the
 // (blockIdx.y of every kernel is the query)
 
 // baby steps -> cipherbuf (reference evalAutoSRNSSmallKeys + reorientCipher)
-void enqueue_baby(kspir_ctx* c, int slot0, int nq, cudaStream_t st) {
+// rm: write the cipherbuf rotation-major (the tensor-core scans read that one)
+void enqueue_baby(kspir_ctx* c, int slot0, int nq, bool rm, cudaStream_t st) {
     const Workspace& w = c->ws0;
     const Batch bt = batch_of(c, slot0);
     k_query_prep<<<dim3(kN / 256, nq), 256, 0, st>>>(w, c->gad.baby, bt);
-    k_ntt_jobs<false><<<dim3(c->n_q, nq), kNttThreads, kNttJobSmem, st>>>(c->jobs + c->seg_q, c->ntabs, bt);
+    k_ntt_jobs<false><<<dim3(c->n_q, nq), kNttThreads, kNttJobSmem, st>>>(c->jobs + (rm ? c->seg_q_rm : c->seg_q),
+                                                                        c->ntabs, bt);
     BabyArgs a1{};
+    a1.cb_rm = rm ? 1 : 0;
     a1.dig = w.dig0; a1.srcB = w.qbn; a1.srcBbs = w.qbbs; a1.perms = c->perms; a1.sigma = c->sigma_baby;
     a1.cipherbuf = w.cipherbuf; a1.interA = w.interA; a1.interB = w.interB; a1.inter_bs = w.inter_bs;
     a1.N1 = c->N1; a1.col_base = 1; a1.inter_idx = c->N1h - 2;
@@ -536,8 +544,9 @@ void launch_scan_mma(kspir_ctx* c, int slot0, int nq, cudaStream_t st) {
     using C = MmaCfg<BT>;
     const int QT = (nq + BT - 1) / BT;
     uint8_t* qop = qop_at(c, slot0);
-    k_qop_split<BT><<<blocks_for((long)kN * QT * BT * 8, 256), 256, 0, st>>>(c->ws0.cipherbuf, c->ws_bytes, slot0, nq,
-                                                                              QT, qop);
+    // the baby steps wrote this launch's cipherbufs rotation-major
+    k_qop_split_rm<BT><<<dim3(kN / kSplitZ, QT * BT), 256, kSplitSmem, st>>>(
+        reinterpret_cast<const uint32_t*>(c->ws0.cipherbuf), c->ws_bytes, slot0, nq, QT, qop);
     ScanMmaArgs a;
     a.dbop = c->dbop;
     a.qop = qop;
@@ -633,8 +642,8 @@ long answer_launches(const kspir_ctx* c, int kind, int nq) {
 // events).  Pointers are fixed for the context's lifetime and the key slot of
 // each query is read from client_of at run time, so the graphs stay valid for
 // any clients and across key or database uploads.
-int build_graphs(kspir_ctx* c, int slot0, int nq, kspir_ctx::PhaseGraphs** out) {
-    auto key = std::make_pair(slot0, nq);
+int build_graphs(kspir_ctx* c, int slot0, int nq, bool rm, kspir_ctx::PhaseGraphs** out) {
+    auto key = std::make_pair(slot0, nq * 2 + (rm ? 1 : 0));
     auto it = c->graphs.find(key);
     if (it != c->graphs.end()) { *out = &it->second; return KSPIR_OK; }
     kspir_ctx::PhaseGraphs pg;
@@ -642,7 +651,7 @@ int build_graphs(kspir_ctx* c, int slot0, int nq, kspir_ctx::PhaseGraphs** out) 
     for (int ph = 0; ph < 4; ph++) {
         cudaGraph_t g = nullptr;
         KS_CUDA(c, cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-        if (ph == 0) enqueue_baby(c, slot0, nq, cs);
+        if (ph == 0) enqueue_baby(c, slot0, nq, rm, cs);
         else if (ph == 1) enqueue_giant(c, slot0, nq, cs);
         else if (ph == 2) enqueue_ext(c, slot0, nq, c->p.r, nullptr, nullptr, cs);
         else enqueue_packing(c, slot0, nq, cs);
@@ -667,7 +676,7 @@ int enqueue_answer(kspir_ctx* c, int slot0, int nq, const int* clients, cudaStre
     auto& ev = c->ring[slot];
     if (c->use_graphs) {
         kspir_ctx::PhaseGraphs* pg = nullptr;
-        int rc = build_graphs(c, slot0, nq, &pg);
+        int rc = build_graphs(c, slot0, nq, kind != SCAN_CUDA, &pg);
         if (rc) return rc;
         cudaEventRecord(ev[0], st);
         KS_CUDA(c, cudaGraphLaunch(pg->g[0], st));
@@ -682,7 +691,7 @@ int enqueue_answer(kspir_ctx* c, int slot0, int nq, const int* clients, cudaStre
         cudaEventRecord(ev[5], st);
     } else {
         cudaEventRecord(ev[0], st);
-        enqueue_baby(c, slot0, nq, st);
+        enqueue_baby(c, slot0, nq, kind != SCAN_CUDA, st);
         cudaEventRecord(ev[1], st);
         enqueue_scan(c, slot0, nq, kind, st);
         cudaEventRecord(ev[2], st);
@@ -756,6 +765,7 @@ int build_dbop(kspir_ctx* c) {
 template <int BT>
 int mma_attr(kspir_ctx* c) {
     KS_CUDA(c, cudaFuncSetAttribute(k_scan_mma<BT>, cudaFuncAttributeMaxDynamicSharedMemorySize, MmaCfg<BT>::SMEM));
+    KS_CUDA(c, cudaFuncSetAttribute(k_qop_split_rm<BT>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSplitSmem));
     return KSPIR_OK;
 }
 
@@ -1219,7 +1229,7 @@ int kspir_matrix_vector_mul_bsgs_rns_crt_large(kspir_ctx* c, int client, uint64_
     KS_CUDA(c, cudaSetDevice(c->device));
     KS_CUDA(c, cudaMemcpyAsync(c->bq64, query_inout, 4 * kN * 8, cudaMemcpyHostToDevice, st));
     k_set_clients<<<1, 32, 0, st>>>(c->client_of, 0, ClientList{1, {client}});
-    enqueue_baby(c, 0, 1, st);
+    enqueue_baby(c, 0, 1, false, st);
     enqueue_scan(c, 0, 1, SCAN_CUDA, st);
     enqueue_giant(c, 0, 1, st);
     // result words, and the modswitched query (cipherbuf column 0) back into query1[0]
@@ -1317,6 +1327,16 @@ int kspir_fetch_stage_slot(kspir_ctx* c, int slot, int stage, uint64_t* out, siz
         const size_t n = (size_t)kN * c->N1 * 2;
         if (words != n) return set_err(c, KSPIR_ERR_INVALID_ARG, "size mismatch");
         KS_COPY(c, out, w.cipherbuf, n * 8, cudaMemcpyDeviceToHost);
+        if (c->last_kind != SCAN_CUDA) {
+            // the tensor-core scans' launches write it rotation-major: back to [N][N1][2]
+            std::vector<uint32_t> rm(2 * n);
+            memcpy(rm.data(), out, n * 8);
+            for (int k = 0; k < c->N1; k++)
+                for (int comp = 0; comp < 2; comp++)
+                    for (int z = 0; z < kN; z++)
+                        out[((size_t)z * c->N1 + k) * 2 + comp] =
+                            rm[cipherbuf_rm_idx(k, comp, 0, z)] | (uint64_t)rm[cipherbuf_rm_idx(k, comp, 1, z)] << 32;
+        }
         return KSPIR_OK;
     }
     const uint32_t* src = nullptr;
