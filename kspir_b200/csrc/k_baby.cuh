@@ -62,61 +62,63 @@ __device__ __forceinline__ uint32_t pow5_mod2n(uint32_t e) {
 }
 
 constexpr int kBabySmem = kN * 8 + kPadN * 4;       // twiddles + one padded polynomial
+constexpr int kBabyPairSmem = kN * 8 + 2 * kPadN * 4;   // twiddles + two padded polynomials
 constexpr int kPerThread = kN / kNttThreads; // 8 coefficients per thread
 
-// One CTA per (rotation, component, crt prime): blockIdx.x = 4*ki + 2*comp + ch;
-// blockIdx.y = query of the batch.  Each CTA recomputes the bsMod part of its
-// component (one inverse transform) so the four CTAs of a rotation run in
-// parallel.  (One CTA per (rotation, component) doing both primes saves two
-// of the eight transforms per rotation but measured slower on B200 even for
-// batches of 64: these CTAs are latency-bound, not issue-bound.)
-// MINB CTAs per SM: 2 (at most 64 registers) for one query -- its 252 CTAs fit
-// one wave with the most registers per thread -- and 3 (at most 42) for
-// batches, where occupancy wins (unbounded, 106 registers and one CTA per SM,
-// a batch of 64 ran 28 % slower).
-template <int ELL, int MINB>
-__global__ void __launch_bounds__(kNttThreads, MINB) k_baby_rot(BabyArgs a, ClientKeysDev keys, NttTables tabs, Batch bt) {
-    extern __shared__ __align__(16) uint8_t smem_raw[];
-    {
-        const size_t wo = ws_off(bt);
-        a.dig = shifted(a.dig, wo);
-        a.srcB = shifted(a.srcB, wo);
-        a.srcBbs = shifted(a.srcBbs, wo);
-        a.cipherbuf = shifted(a.cipherbuf, wo);
-        a.interA = shifted(a.interA, wo);
-        a.interB = shifted(a.interB, wo);
-        a.inter_bs = shifted(a.inter_bs, wo);
-        keys = keys_at(keys, bt);
-    }
-    uint2* tws = reinterpret_cast<uint2*>(smem_raw);
-    uint32_t* S = reinterpret_cast<uint32_t*>(smem_raw + kN * 8);
+// Per-rotation state shared by the two kernel shapes below.
+struct BabyRot {
+    int ki, comp, col, tid;
+    bool inter;
+    size_t wo;              // workspace offset of the query
+    const uint32_t* kbs;    // bsMod keys of rotation ki
+    const uint32_t* kcrt;   // crt keys of rotation ki
+    const int32_t* perm;    // caller permutation of rotation ki
+};
 
-    const int ki = blockIdx.x >> 2;            // key index: rotation by 5^(ki+1)
-    const int comp = (blockIdx.x >> 1) & 1;    // 0 = a, 1 = b
-    const int ch = blockIdx.x & 1;             // crt prime
-    const int col = a.col_base + ki;
-    const bool inter = (ki == a.inter_idx);
-    const int tid = threadIdx.x;
-    const int32_t* __restrict__ perm = a.perms + (size_t)(ki + 1) * kN;
-    const uint32_t* __restrict__ kbs = keys.baby_bs + (size_t)ki * ELL * 2 * kN;
-    const uint32_t* __restrict__ kcrt = keys.baby_crt + (size_t)ki * ELL * 2 * 2 * kN;
-    const uint32_t* __restrict__ dig = a.dig;
-
-    stage_twiddles(tws, tabs, CH_BS, NTT_INV);
-    int pk[kPerThread];
+// perm[k] of this thread's coefficients (reloaded by each multiply-accumulate
+// rather than held in registers across the transforms)
+__device__ __forceinline__ void baby_perm(const BabyRot& R, int* pk) {
 #pragma unroll
-    for (int it = 0; it < kPerThread; it++) pk[it] = __ldg(perm + tid + it * kNttThreads);
+    for (int it = 0; it < kPerThread; it++) pk[it] = __ldg(R.perm + R.tid + it * kNttThreads);
+}
 
-    // bsMod part of this component: -sum_j d_j[perm] * key_j
+// The workspace pointers of BabyArgs are slot-0 pointers: each use adds the
+// query's workspace offset R.wo (kept as one value rather than seven shifted
+// pointers, which would pin fourteen registers for the whole kernel).
+template <int ELL>
+__device__ __forceinline__ void baby_setup(BabyRot& R, const BabyArgs& a, const ClientKeysDev& keys,
+                                           const Batch& bt, int ki, int comp) {
+    R.ki = ki;
+    R.comp = comp;
+    R.col = a.col_base + ki;
+    R.tid = threadIdx.x;
+    R.inter = (ki == a.inter_idx);
+    R.wo = ws_off(bt);
+    const size_t ko = key_off(bt);
+    R.kbs = shifted(keys.baby_bs, ko) + (size_t)ki * ELL * 2 * kN;
+    R.kcrt = shifted(keys.baby_crt, ko) + (size_t)ki * ELL * 2 * 2 * kN;
+    R.perm = a.perms + (size_t)(ki + 1) * kN;
+}
+
+// x2 of this component into S (coefficient form, canonical mod bsMod):
+//   INTT_bs(-sum_j d_j[perm] * key_j) (+ auto_g(b mod bsMod) for comp 1).
+// The caller has staged the bsMod inverse twiddles into tws (unsynchronised).
+// export_inter: this CTA writes the intermediate rotation's x2.
+template <int ELL>
+__device__ __forceinline__ void baby_bs_part(const BabyRot& R, const BabyArgs& a, uint32_t* S, const uint2* tws,
+                                             bool export_inter) {
+    const int tid = R.tid;
     {
         const ChanConst cb = c_dev.ch[CH_BS];
+        int pk[kPerThread];
+        baby_perm(R, pk);
         uint64_t acc[kPerThread];
 #pragma unroll
         for (int it = 0; it < kPerThread; it++) acc[it] = 0;
 #pragma unroll
         for (int j = 0; j < ELL; j++) {
-            const uint32_t* d = dig + (size_t)(j * 3 + CH_BS) * kN;
-            const uint32_t* kk = kbs + (size_t)(j * 2 + comp) * kN;
+            const uint32_t* d = shifted(a.dig, R.wo) + (size_t)(j * 3 + CH_BS) * kN;
+            const uint32_t* kk = R.kbs + (size_t)(j * 2 + R.comp) * kN;
 #pragma unroll
             for (int it = 0; it < kPerThread; it++)
                 acc[it] += (uint64_t)__ldg(d + pk[it]) * __ldg(kk + tid + it * kNttThreads);
@@ -127,9 +129,9 @@ __global__ void __launch_bounds__(kNttThreads, MINB) k_baby_rot(BabyArgs a, Clie
     }
     cta_ntt_inverse(S, tws, CH_BS);
 
-    if (comp == 1) {
+    if (R.comp == 1) {
         // x2b += auto_g(b mod bsMod)   (automorphic_rns, twosteps.cpp:1045-1048)
-        const uint32_t ginv = pow5_mod2n(2048u - (uint32_t)(ki + 1));
+        const uint32_t ginv = pow5_mod2n(2048u - (uint32_t)(R.ki + 1));
         const uint32_t qb = c_dev.ch[CH_BS].q;
 #pragma unroll
         for (int it = 0; it < kPerThread; it++) {
@@ -137,33 +139,44 @@ __global__ void __launch_bounds__(kNttThreads, MINB) k_baby_rot(BabyArgs a, Clie
             const int pk2 = pidx(tid) + it * kPadStep;
             bool neg;
             const int src = auto_src(k, ginv, &neg);
-            uint32_t v = __ldg(a.srcBbs + src);
+            uint32_t v = __ldg(shifted(a.srcBbs, R.wo) + src);
             if (neg) v = negmod(v, qb);
             S[pk2] = addmod(S[pk2], v, qb);
         }
     }
-    if (inter && ch == 0) {
+    if (R.inter && export_inter) {
 #pragma unroll
         for (int it = 0; it < kPerThread; it++) {
             const int k = tid + it * kNttThreads;
-            a.inter_bs[comp * kN + k] = S[pidx(tid) + it * kPadStep];
+            shifted(a.inter_bs, R.wo)[R.comp * kN + k] = S[pidx(tid) + it * kPadStep];
         }
     }
-    const uint16_t* __restrict__ sig = a.sigma + (size_t)ki * kN;
-    uint32_t* cb32 = reinterpret_cast<uint32_t*>(a.cipherbuf);
-    uint32_t* inter_out = comp == 0 ? a.interA : a.interB;
-    __syncthreads();   // x2 complete and the inverse twiddles no longer read
+}
+
+// Prime ch of the rotation: NTT_ch(x2) from S (in place), the crt
+// multiply-accumulate, the modswitch, and the cipherbuf store.  Starts with
+// a barrier (x2 complete, tws free) and stages the forward twiddles itself.
+template <int ELL>
+__device__ __forceinline__ void baby_crt_part(const BabyRot& R, const BabyArgs& a, uint32_t* S, uint2* tws,
+                                              const NttTables& tabs, int ch) {
+    const int tid = R.tid, comp = R.comp;
+    const uint16_t* __restrict__ sig = a.sigma + (size_t)R.ki * kN;
+    uint32_t* cb32 = reinterpret_cast<uint32_t*>(shifted(a.cipherbuf, R.wo));
+    uint32_t* inter_out = shifted(comp == 0 ? a.interA : a.interB, R.wo);
+    __syncthreads();   // x2 complete and the previous twiddles no longer read
     stage_twiddles(tws, tabs, ch, NTT_FWD);
     cta_ntt_forward(S, tws, ch);   // NTT_ch(x2), x2 < bsMod < q
 
     const ChanConst cc = c_dev.ch[ch];
+    int pk[kPerThread];
+    baby_perm(R, pk);
     uint64_t acc[kPerThread];
 #pragma unroll
     for (int it = 0; it < kPerThread; it++) acc[it] = 0;
 #pragma unroll
     for (int j = 0; j < ELL; j++) {
-        const uint32_t* d = dig + (size_t)(j * 3 + ch) * kN;
-        const uint32_t* kk = kcrt + (size_t)((j * 2 + comp) * 2 + ch) * kN;
+        const uint32_t* d = shifted(a.dig, R.wo) + (size_t)(j * 3 + ch) * kN;
+        const uint32_t* kk = R.kcrt + (size_t)((j * 2 + comp) * 2 + ch) * kN;
 #pragma unroll
         for (int it = 0; it < kPerThread; it++)
             acc[it] += (uint64_t)__ldg(d + pk[it]) * __ldg(kk + tid + it * kNttThreads);
@@ -172,14 +185,56 @@ __global__ void __launch_bounds__(kNttThreads, MINB) k_baby_rot(BabyArgs a, Clie
     for (int it = 0; it < kPerThread; it++) {
         const int k = tid + it * kNttThreads;
         uint32_t A = negmod(mod_crt(acc[it], ch), cc.q);
-        if (comp == 1) A = addmod(A, __ldg(a.srcB + ch * kN + sig[k]), cc.q);
-        if (inter) inter_out[ch * kN + k] = A;
+        if (comp == 1) A = addmod(A, __ldg(shifted(a.srcB, R.wo) + ch * kN + sig[k]), cc.q);
+        if (R.inter) inter_out[ch * kN + k] = A;
         const uint32_t r = shoup_mul(submod(A, S[pidx(tid) + it * kPadStep], cc.q), cc.bsinv, cc.bsinv_p, cc.q);
         if (a.cb_rm)
-            cb32[cipherbuf_rm_idx(col, comp, ch, k)] = r;
+            cb32[cipherbuf_rm_idx(R.col, comp, ch, k)] = r;
         else
-            cb32[(((size_t)k * a.N1 + col) * 2 + comp) * 2 + ch] = r;
+            cb32[(((size_t)k * a.N1 + R.col) * 2 + comp) * 2 + ch] = r;
     }
+}
+
+// One CTA per (rotation, component, crt prime): blockIdx.x = 4*ki + 2*comp + ch;
+// blockIdx.y = query of the batch.  Each CTA recomputes the bsMod part of its
+// component (one inverse transform) so the four CTAs of a rotation run in
+// parallel: the shape for one query, whose 252 CTAs then fit one wave.
+// MINB CTAs per SM: 2 (at most 64 registers).
+template <int ELL, int MINB>
+__global__ void __launch_bounds__(kNttThreads, MINB) k_baby_rot(BabyArgs a, ClientKeysDev keys, NttTables tabs, Batch bt) {
+    extern __shared__ __align__(16) uint8_t smem_raw[];
+    uint2* tws = reinterpret_cast<uint2*>(smem_raw);
+    uint32_t* S = reinterpret_cast<uint32_t*>(smem_raw + kN * 8);
+    const int ch = blockIdx.x & 1;
+    BabyRot R;
+    stage_twiddles(tws, tabs, CH_BS, NTT_INV);
+    baby_setup<ELL>(R, a, keys, bt, blockIdx.x >> 2, (blockIdx.x >> 1) & 1);
+    baby_bs_part<ELL>(R, a, S, tws, ch == 0);
+    baby_crt_part<ELL>(R, a, S, tws, tabs, ch);
+}
+
+// One CTA per (rotation, component): blockIdx.x = 2*ki + comp.  The bsMod part
+// runs once for both primes (six transforms per rotation instead of eight):
+// the shape for batches, which have CTAs enough to fill the GPU without the
+// duplicated work.  MINB 2: at 3 CTAs per SM (42 registers) it spills, and
+// measured no faster (batch of 64: baby steps 1.68 ms at 3, 1.66 ms at 2,
+// 1.74 ms for the four-CTA shape).
+template <int ELL, int MINB>
+__global__ void __launch_bounds__(kNttThreads, MINB) k_baby_pair(BabyArgs a, ClientKeysDev keys, NttTables tabs, Batch bt) {
+    extern __shared__ __align__(16) uint8_t smem_raw[];
+    uint2* tws = reinterpret_cast<uint2*>(smem_raw);
+    uint32_t* S = reinterpret_cast<uint32_t*>(smem_raw + kN * 8);
+    uint32_t* S2 = S + kPadN;
+    BabyRot R;
+    stage_twiddles(tws, tabs, CH_BS, NTT_INV);
+    baby_setup<ELL>(R, a, keys, bt, blockIdx.x >> 1, blockIdx.x & 1);
+    baby_bs_part<ELL>(R, a, S, tws, true);
+    // the second prime transforms its own copy of x2 (each thread copies the
+    // coefficients it wrote: no barrier needed)
+#pragma unroll
+    for (int it = 0; it < kPerThread; it++) S2[pidx(R.tid) + it * kPadStep] = S[pidx(R.tid) + it * kPadStep];
+    baby_crt_part<ELL>(R, a, S, tws, tabs, 0);
+    baby_crt_part<ELL>(R, a, S2, tws, tabs, 1);
 }
 
 }  // namespace kspir

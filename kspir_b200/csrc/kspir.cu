@@ -512,7 +512,7 @@ void enqueue_baby(kspir_ctx* c, int slot0, int nq, bool rm, cudaStream_t st) {
         if (nq == 1)
             k_baby_rot<3, 2><<<dim3(nrot * 4, nq), kNttThreads, kBabySmem, st>>>(args, c->keys0, c->ntabs, bt);
         else
-            k_baby_rot<3, 3><<<dim3(nrot * 4, nq), kNttThreads, kBabySmem, st>>>(args, c->keys0, c->ntabs, bt);
+            k_baby_pair<3, 2><<<dim3(nrot * 2, nq), kNttThreads, kBabyPairSmem, st>>>(args, c->keys0, c->ntabs, bt);
     };
     rot(a1, c->N1h - 1);
     k_ntt_jobs<true><<<dim3(2, nq), kNttThreads, kNttJobSmem, st>>>(c->jobs + c->seg_inter, c->ntabs, bt);
@@ -813,7 +813,7 @@ int kspir_ctx_create(int device, const kspir_params* params, kspir_ctx** out) {
     if (const char* e = getenv("KSPIR_NO_GRAPHS")) c->use_graphs = !(e[0] == '1');
     KS_CUDA(c.get(), cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device));
     KS_CUDA(c.get(), cudaFuncSetAttribute(k_baby_rot<3, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBabySmem));
-    KS_CUDA(c.get(), cudaFuncSetAttribute(k_baby_rot<3, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBabySmem));
+    KS_CUDA(c.get(), cudaFuncSetAttribute(k_baby_pair<3, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBabyPairSmem));
     KS_CUDA(c.get(), cudaFuncSetAttribute(k_db_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, kDbRowsSmem));
     KS_CUDA(c.get(), cudaFuncSetAttribute(k_ntt_jobs<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kNttJobSmem));
     KS_CUDA(c.get(), cudaFuncSetAttribute(k_ntt_jobs<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kNttJobSmem));
