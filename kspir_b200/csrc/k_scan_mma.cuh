@@ -347,15 +347,16 @@ __global__ void __launch_bounds__(MmaCfg<BT>::THREADS, 1) k_scan_mma(ScanMmaArgs
 // CTA loads the 512 rows (k, comp, ch) of its slots
 // (128 contiguous bytes each) into shared memory, column zz stored at
 // zz ^ 4 (k / 16) so that the reads below hit 32 distinct banks, then each
-// thread takes slot zz and 16-entry chunk c of every (comp, ch): 16 words,
+// thread takes slot zz, 16-entry chunk c and component comp of both primes: 16 words,
 // byte-transposed into the 4 limb rows' 16-byte chunks (eight threads write
 // the 128 bytes of one tile row).
 constexpr int kSplitZ = 32;
+constexpr int kSplitThreads = 512;
 constexpr int kSplitSmem = kMmaK * 4 * kSplitZ * 4;   // 64 KiB
 
 template <int BT>
-__global__ void __launch_bounds__(256) k_qop_split_rm(const uint32_t* __restrict__ cb0, size_t ws_bytes, int slot0,
-                                                     int nq, int QT, uint8_t* __restrict__ qop) {
+__global__ void __launch_bounds__(kSplitThreads) k_qop_split_rm(const uint32_t* __restrict__ cb0, size_t ws_bytes,
+                                                               int slot0, int nq, int QT, uint8_t* __restrict__ qop) {
     using C = MmaCfg<BT>;
     extern __shared__ __align__(16) uint8_t smem_raw[];
     uint32_t* V = reinterpret_cast<uint32_t*>(smem_raw);   // [512 rows][32 columns]
@@ -366,18 +367,20 @@ __global__ void __launch_bounds__(256) k_qop_split_rm(const uint32_t* __restrict
     if (live) {
         const uint32_t* cb = reinterpret_cast<const uint32_t*>(reinterpret_cast<const char*>(cb0) +
                                                               (size_t)(slot0 + bq) * ws_bytes);
+        constexpr int W = kSplitThreads / 32;
 #pragma unroll 8
-        for (int row = warp; row < kMmaK * 4; row += 8)
+        for (int row = warp; row < kMmaK * 4; row += W)
             V[row * kSplitZ + (lane ^ (4 * ((row >> 6) & 7)))] = __ldg(cb + (size_t)row * kN + z0 + lane);
         __syncthreads();
     }
     const int c = tid & 7;                                  // 16-entry chunk of k
-    const int zz = 4 * warp + ((tid >> 3) & 3);
+    const int zz = 4 * (warp & 7) + ((tid >> 3) & 3);
+    const int comp = warp >> 3;                             // warps 0-7: a, 8-15: b
     const int z = z0 + zz;
     const int qt = bq / BT, b = bq % BT;
 #pragma unroll
-    for (int cv = 0; cv < 4; cv++) {
-        const int comp = cv >> 1, ch = cv & 1;
+    for (int ch = 0; ch < 2; ch++) {
+        const int cv = comp * 2 + ch;
         uint32_t w[4][4];   // [limb][word]
 #pragma unroll
         for (int g = 0; g < 4; g++) {

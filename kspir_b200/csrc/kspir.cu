@@ -545,7 +545,7 @@ void launch_scan_mma(kspir_ctx* c, int slot0, int nq, cudaStream_t st) {
     const int QT = (nq + BT - 1) / BT;
     uint8_t* qop = qop_at(c, slot0);
     // the baby steps wrote this launch's cipherbufs rotation-major
-    k_qop_split_rm<BT><<<dim3(kN / kSplitZ, QT * BT), 256, kSplitSmem, st>>>(
+    k_qop_split_rm<BT><<<dim3(kN / kSplitZ, QT * BT), kSplitThreads, kSplitSmem, st>>>(
         reinterpret_cast<const uint32_t*>(c->ws0.cipherbuf), c->ws_bytes, slot0, nq, QT, qop);
     ScanMmaArgs a;
     a.dbop = c->dbop;
