@@ -84,6 +84,18 @@ int kspir_db_preprocess(kspir_ctx* ctx, const uint64_t* data, size_t words, floa
 /* Same with the raw database already in device memory. */
 int kspir_db_preprocess_device(kspir_ctx* ctx, const uint64_t* d_data, size_t words, float* device_ms);
 
+/* The reference's two preprocessing functions one for one, for one
+ * sub-database, on the device (host buffers; the context supplies N1):
+ *   kspir_database_tobsgsntt  database_tobsgsntt(result, data, crtMod, N1)
+ *       (twosteps.h:19-20, twosteps.cpp:42-179): data [N][N/2] words < 65537
+ *       (else KSPIR_ERR_INVALID_ARG), result [N/2][N] rows mod crtMod.
+ *   kspir_database_tocrt      database_tocrt(datacrt, data_ntt, N1)
+ *       (crt.h:133, crt.cpp:859-885): data_ntt [N/2][N] (any 64-bit words),
+ *       datacrt [N][N/2].
+ * Neither touches the resident database. */
+int kspir_database_tobsgsntt(kspir_ctx* ctx, const uint64_t* data, uint64_t* result);
+int kspir_database_tocrt(kspir_ctx* ctx, const uint64_t* data_ntt, uint64_t* datacrt);
+
 /* Copies the resident database (datacrt layout, r * N * N / 2 words) to host. */
 int kspir_db_download(kspir_ctx* ctx, uint64_t* datacrt, size_t words);
 

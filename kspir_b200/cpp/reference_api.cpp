@@ -6,6 +6,11 @@
 //   externalProduct                        reference src/lwe.h:292
 //   packingRLWEs                           reference src/answer.h:79-80
 //
+// and the server preprocessing that builds the database those answers read:
+//
+//   database_tobsgsntt                     reference src/twosteps.h:19-20
+//   database_tocrt                         reference src/crt.h:133
+//
 // Same signatures, argument meaning and in-place effects as the reference:
 // input[0] is modswitched in place to NTT form and result[j] comes back in NTT
 // form; externalProduct accumulates into `result` and returns both `result`
@@ -27,6 +32,7 @@
 #include <vector>
 
 #include "answer.h"
+#include "crt.h"
 #include "lwe.h"
 #include "twosteps.h"
 
@@ -107,7 +113,63 @@ void upload_keys() {
                                    g.packing.empty() ? nullptr : g.packing.data(), g.rgsw.data()));
 }
 
+// The preprocessing runs in a context of its own (one sub-database at a time,
+// N1 of the call), so it never disturbs the answer session's resident data.
+struct PrepSession {
+    kspir_ctx* ctx = nullptr;
+    int N1 = 0;
+    std::vector<uint64_t> in, out;   // flat copies of one sub-database
+};
+PrepSession gp;
+
+void ensure_prep(int N1) {
+    if (gp.ctx && gp.N1 == N1) return;
+    if (gp.ctx) kspir_ctx_destroy(gp.ctx);
+    gp.ctx = nullptr;
+    kspir_params p;
+    p.r = 1;
+    p.N1 = N1;
+    p.max_clients = 1;
+    p.max_inflight = 1;
+    int rc = kspir_ctx_create(0, &p, &gp.ctx);
+    if (rc != KSPIR_OK) {
+        fprintf(stderr, "kspir_b200: kspir_ctx_create: %s (%s)\n", kspir_strerror(rc), kspir_last_error(nullptr));
+        abort();
+    }
+    gp.N1 = N1;
+    gp.in.resize((size_t)kPoly * (kPoly / 2));
+    gp.out.resize((size_t)kPoly * (kPoly / 2));
+}
+
+void check_prep(const char* what, int rc) {
+    if (rc == KSPIR_OK) return;
+    fprintf(stderr, "kspir_b200: %s: %s (%s)\n", what, kspir_strerror(rc), kspir_last_error(gp.ctx));
+    abort();
+}
+
 }  // namespace
+
+void database_tobsgsntt(std::vector<std::vector<uint64_t> >& result, std::vector<std::vector<uint64_t> >& data,
+                        uint64_t modulus, int32_t N1) {
+    // the reference lifts to modulus and transforms mod crtMod (USE_CRTMOD):
+    // the device path implements the combination the reference's callers use
+    if (modulus != crtMod) {
+        fprintf(stderr, "kspir_b200: database_tobsgsntt: only modulus = crtMod is supported\n");
+        abort();
+    }
+    ensure_prep(N1);
+    const size_t H = kPoly / 2;
+    for (size_t i = 0; i < (size_t)kPoly; i++) memcpy(gp.in.data() + i * H, data[i].data(), H * 8);
+    check_prep("kspir_database_tobsgsntt", kspir_database_tobsgsntt(gp.ctx, gp.in.data(), gp.out.data()));
+    for (size_t i = 0; i < H; i++) memcpy(result[i].data(), gp.out.data() + i * kPoly, kPoly * 8);
+}
+
+void database_tocrt(uint64_t* datacrt, std::vector<std::vector<uint64_t> >& data_ntt, int32_t N1) {
+    ensure_prep(N1);
+    const size_t H = kPoly / 2;
+    for (size_t i = 0; i < H; i++) memcpy(gp.in.data() + i * kPoly, data_ntt[i].data(), kPoly * 8);
+    check_prep("kspir_database_tocrt", kspir_database_tocrt(gp.ctx, gp.in.data(), datacrt));
+}
 
 void matrix_vector_mul_bsgs_rns_crt_large(std::vector<RlweCiphertext>& result, std::vector<RlweCiphertext>& input,
                                           uint64_t* data, const AutoKeyBSGSRNS& autoKey, const int32_t N1,

@@ -43,10 +43,13 @@ __device__ __forceinline__ size_t db_diag_index(int R, int c) {
 // grid (N/2 / 4, sub-databases), 512 threads.
 //   raw   [sub][N][N/2] words < bsgsp (validated by the caller)
 //   gtab  [N1][N] gather table G
-//   out   [sub][N][N/2] datacrt words
+//   out   [sub][N][N/2] datacrt words (database_tocrt applied)
+//   rows  ROWS: also [sub][N/2][N] rows mod crtMod, database_tobsgsntt's own
+//         output (its `result`)
+template <bool ROWS>
 __global__ void __launch_bounds__(kNttThreads, 1)
 k_db_rows(const uint64_t* __restrict__ raw, const uint16_t* __restrict__ gtab, uint64_t* __restrict__ out,
-          int N1, NttTables tabs) {
+          uint64_t* __restrict__ rows, int N1, NttTables tabs) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
     uint8_t* smem = smem_raw;
     uint2* tws = reinterpret_cast<uint2*>(smem);
@@ -80,6 +83,15 @@ k_db_rows(const uint64_t* __restrict__ raw, const uint16_t* __restrict__ gtab, u
     stage_twiddles(tws, tabs, CH_Q2, NTT_FWD);
     cta_ntt_forward_m<kDbRowsPerCta>(s2, kPadN, tws, CH_Q2);
 
+    if (ROWS) {
+        // the canonical value mod crtMod of each slot, row by row (coalesced)
+#pragma unroll
+        for (int t = 0; t < kDbRowsPerCta; t++) {
+            uint64_t* o = rows + sub + (size_t)(R0 + t) * kN;
+            for (int z = threadIdx.x; z < kN; z += kNttThreads)
+                o[z] = crt_compose_res(s1[t * kPadN + pidx(z)], s2[t * kPadN + pidx(z)]);
+        }
+    }
     // slot z of rows R0..R0+3: one 32-byte sector at datacrt[z * N/2 + R0]
     uint64_t* o = out + sub + R0;
     for (int z = threadIdx.x; z < kN; z += kNttThreads) {
@@ -93,6 +105,26 @@ k_db_rows(const uint64_t* __restrict__ raw, const uint16_t* __restrict__ gtab, u
         d[0] = a;
         d[1] = b;
     }
+}
+
+// database_tocrt alone (crt.cpp:859-885) on rows mod crtMod of one or more
+// sub-databases: datacrt[z][R] = (x mod q1) | (x mod q2) << 32 for
+// x = rows[R][z], any 64-bit x (the reference's Barrett reduction is exact
+// for every 64-bit input).  32 x 32 tiles through shared memory; grid
+// (N / 32, N/2 / 32, sub-databases), 32 x 8 threads.
+__global__ void k_db_tocrt(const uint64_t* __restrict__ rows, uint64_t* __restrict__ datacrt) {
+    __shared__ uint64_t tile[32][33];
+    const size_t sub = (size_t)blockIdx.z * kN * (kN / 2);
+    const int z0 = blockIdx.x * 32, R0 = blockIdx.y * 32;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+#pragma unroll
+    for (int i = ty; i < 32; i += 8) {
+        const uint64_t x = rows[sub + (size_t)(R0 + i) * kN + z0 + tx];
+        tile[i][tx] = mod_q1(x) | (uint64_t)mod_q2(x) << 32;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = ty; i < 32; i += 8) datacrt[sub + (size_t)(z0 + i) * (kN / 2) + R0 + tx] = tile[tx][i];
 }
 
 }  // namespace kspir

@@ -192,6 +192,11 @@ struct kspir_ctx {
     bool mma = false;                 // batched tensor-core scan enabled (N1 = 128, several slots)
     uint16_t* dbg = nullptr;          // gather table of the database preprocessing [N1][N]
     int* dbflag = nullptr;            // its validation word
+    // one-sub-database preprocessing calls (kspir_database_*): device raw,
+    // rows and datacrt; pinned host staging and the last rows returned
+    uint64_t* prep_dev = nullptr;
+    uint64_t* prep_host = nullptr;
+    bool prep_rows_valid = false;
     uint8_t* dbop = nullptr;          // its database operand [N][2][G] tiles
     int G = 0;
     uint8_t* qop = nullptr;           // its query operand: launch at slot0 uses qop_at(slot0)
@@ -814,7 +819,8 @@ int kspir_ctx_create(int device, const kspir_params* params, kspir_ctx** out) {
     KS_CUDA(c.get(), cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device));
     KS_CUDA(c.get(), cudaFuncSetAttribute(k_baby_rot<3, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBabySmem));
     KS_CUDA(c.get(), cudaFuncSetAttribute(k_baby_pair<3, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBabyPairSmem));
-    KS_CUDA(c.get(), cudaFuncSetAttribute(k_db_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, kDbRowsSmem));
+    KS_CUDA(c.get(), cudaFuncSetAttribute(k_db_rows<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kDbRowsSmem));
+    KS_CUDA(c.get(), cudaFuncSetAttribute(k_db_rows<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kDbRowsSmem));
     KS_CUDA(c.get(), cudaFuncSetAttribute(k_ntt_jobs<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kNttJobSmem));
     KS_CUDA(c.get(), cudaFuncSetAttribute(k_ntt_jobs<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kNttJobSmem));
     KS_CUDA(c.get(), cudaFuncSetAttribute(k_giant_fused<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGiantSmem));
@@ -872,6 +878,8 @@ int kspir_ctx_destroy(kspir_ctx* c) {
     cudaFree(c->db);
     cudaFree(c->dbg);
     cudaFree(c->dbflag);
+    cudaFree(c->prep_dev);
+    if (c->prep_host) cudaFreeHost(c->prep_host);
     cudaFree(c->dbop);
     cudaFree(c->qop);
     cudaFree(c->perms);
@@ -900,16 +908,33 @@ int kspir_db_upload(kspir_ctx* c, const uint64_t* datacrt, size_t words) {
 namespace {
 // Validates the raw database on the device, then overwrites the resident one
 // with its preprocessed form (k_db_rows), caller holds the lock.
+// the gather table of the context's N1 and the validation word, built once
+int ensure_db_tables(kspir_ctx* c) {
+    if (c->dbg) return KSPIR_OK;
+    const std::vector<uint16_t> g = db_gather_table(c->N1);
+    KS_CUDA(c, cudaMalloc(&c->dbflag, sizeof(int)));
+    KS_CUDA(c, cudaMalloc(&c->dbg, g.size() * 2));
+    KS_COPY(c, c->dbg, g.data(), g.size() * 2, cudaMemcpyHostToDevice);
+    return KSPIR_OK;
+}
+
+// 1 when some of the n raw words is >= bsgsp (synchronises)
+int db_words_invalid(kspir_ctx* c, const uint64_t* d_raw, size_t n, int* bad) {
+    cudaStream_t st = c->stream;
+    KS_CUDA(c, cudaMemsetAsync(c->dbflag, 0, sizeof(int), st));
+    k_check_canonical<<<c->nsm * 8, 256, 0, st>>>(d_raw, n, kP, c->dbflag);
+    KS_CUDA(c, cudaGetLastError());
+    KS_CUDA(c, cudaMemcpyAsync(bad, c->dbflag, sizeof(int), cudaMemcpyDeviceToHost, st));
+    KS_CUDA(c, cudaStreamSynchronize(st));
+    return KSPIR_OK;
+}
+
 int db_preprocess_dev(kspir_ctx* c, const uint64_t* d_raw, float* device_ms) {
     const int r = c->p.r;
     const size_t words = (size_t)r * kN * (kN / 2);
     cudaStream_t st = c->stream;
-    if (!c->dbg) {
-        const std::vector<uint16_t> g = db_gather_table(c->N1);
-        KS_CUDA(c, cudaMalloc(&c->dbflag, sizeof(int)));
-        KS_CUDA(c, cudaMalloc(&c->dbg, g.size() * 2));
-        KS_COPY(c, c->dbg, g.data(), g.size() * 2, cudaMemcpyHostToDevice);
-    }
+    int rc0 = ensure_db_tables(c);
+    if (rc0) return rc0;
     if (!c->db) KS_CUDA(c, cudaMalloc(&c->db, words * 8));
     cudaEvent_t ev[2] = {nullptr, nullptr};
     if (device_ms) {
@@ -917,20 +942,16 @@ int db_preprocess_dev(kspir_ctx* c, const uint64_t* d_raw, float* device_ms) {
         KS_CUDA(c, cudaEventCreate(&ev[1]));
         KS_CUDA(c, cudaEventRecord(ev[0], st));
     }
-    int* flag = c->dbflag;
-    KS_CUDA(c, cudaMemsetAsync(flag, 0, sizeof(int), st));
-    k_check_canonical<<<c->nsm * 8, 256, 0, st>>>(d_raw, words, kP, flag);
-    KS_CUDA(c, cudaGetLastError());
     int bad = 0;
-    KS_CUDA(c, cudaMemcpyAsync(&bad, flag, sizeof(int), cudaMemcpyDeviceToHost, st));
-    KS_CUDA(c, cudaStreamSynchronize(st));
+    rc0 = db_words_invalid(c, d_raw, words, &bad);
+    if (rc0) return rc0;
     if (bad) {
         if (device_ms) { cudaEventDestroy(ev[0]); cudaEventDestroy(ev[1]); }
         return set_err(c, KSPIR_ERR_INVALID_ARG, "database entries must be below bsgsp = 65537");
     }
     c->db_loaded = false;
-    k_db_rows<<<dim3(kN / 2 / kDbRowsPerCta, r), kNttThreads, kDbRowsSmem, st>>>(d_raw, c->dbg, c->db, c->N1,
-                                                                                   c->ntabs);
+    k_db_rows<false><<<dim3(kN / 2 / kDbRowsPerCta, r), kNttThreads, kDbRowsSmem, st>>>(d_raw, c->dbg, c->db,
+                                                                                          nullptr, c->N1, c->ntabs);
     KS_CUDA(c, cudaGetLastError());
     int rc = build_dbop(c);   // synchronises
     if (rc) return rc;
@@ -968,6 +989,69 @@ int kspir_db_preprocess_device(kspir_ctx* c, const uint64_t* d_data, size_t word
     std::lock_guard<std::mutex> lk(c->mu);
     KS_CUDA(c, cudaSetDevice(c->device));
     return db_preprocess_dev(c, d_data, device_ms);
+}
+
+namespace {
+constexpr size_t kSubWords = (size_t)kN * (kN / 2);
+
+int ensure_prep_buffers(kspir_ctx* c) {
+    if (!c->prep_dev) KS_CUDA(c, cudaMalloc(&c->prep_dev, 3 * kSubWords * 8));
+    if (!c->prep_host) KS_CUDA(c, cudaHostAlloc(&c->prep_host, 2 * kSubWords * 8, cudaHostAllocDefault));
+    return KSPIR_OK;
+}
+}  // namespace
+
+int kspir_database_tobsgsntt(kspir_ctx* c, const uint64_t* data, uint64_t* result) {
+    if (!c || !data || !result) return KSPIR_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(c->mu);
+    KS_CUDA(c, cudaSetDevice(c->device));
+    int rc = ensure_db_tables(c);
+    if (!rc) rc = ensure_prep_buffers(c);
+    if (rc) return rc;
+    c->prep_rows_valid = false;
+    uint64_t* d_raw = c->prep_dev;
+    uint64_t* d_rows = c->prep_dev + kSubWords;
+    uint64_t* d_crt = c->prep_dev + 2 * kSubWords;
+    uint64_t* h_in = c->prep_host;
+    uint64_t* h_rows = c->prep_host + kSubWords;
+    memcpy(h_in, data, kSubWords * 8);
+    KS_COPY(c, d_raw, h_in, kSubWords * 8, cudaMemcpyHostToDevice);
+    int bad = 0;
+    rc = db_words_invalid(c, d_raw, kSubWords, &bad);
+    if (rc) return rc;
+    if (bad) return set_err(c, KSPIR_ERR_INVALID_ARG, "database entries must be below bsgsp = 65537");
+    // the datacrt comes out of the same pass and stays on the device for a
+    // database_tocrt of exactly these rows
+    k_db_rows<true><<<dim3(kN / 2 / kDbRowsPerCta, 1), kNttThreads, kDbRowsSmem, c->stream>>>(
+        d_raw, c->dbg, d_crt, d_rows, c->N1, c->ntabs);
+    KS_CUDA(c, cudaGetLastError());
+    KS_COPY(c, h_rows, d_rows, kSubWords * 8, cudaMemcpyDeviceToHost);
+    memcpy(result, h_rows, kSubWords * 8);
+    c->prep_rows_valid = true;
+    return KSPIR_OK;
+}
+
+int kspir_database_tocrt(kspir_ctx* c, const uint64_t* data_ntt, uint64_t* datacrt) {
+    if (!c || !data_ntt || !datacrt) return KSPIR_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(c->mu);
+    KS_CUDA(c, cudaSetDevice(c->device));
+    int rc = ensure_prep_buffers(c);
+    if (rc) return rc;
+    uint64_t* d_rows = c->prep_dev + kSubWords;
+    uint64_t* d_crt = c->prep_dev + 2 * kSubWords;
+    uint64_t* h_in = c->prep_host;
+    // rows equal to the last database_tobsgsntt output (compared, not
+    // assumed): its datacrt is already on the device
+    if (!(c->prep_rows_valid && memcmp(data_ntt, c->prep_host + kSubWords, kSubWords * 8) == 0)) {
+        c->prep_rows_valid = false;
+        memcpy(h_in, data_ntt, kSubWords * 8);
+        KS_COPY(c, d_rows, h_in, kSubWords * 8, cudaMemcpyHostToDevice);
+        k_db_tocrt<<<dim3(kN / 32, kN / 2 / 32, 1), dim3(32, 8), 0, c->stream>>>(d_rows, d_crt);
+        KS_CUDA(c, cudaGetLastError());
+    }
+    KS_COPY(c, h_in, d_crt, kSubWords * 8, cudaMemcpyDeviceToHost);
+    memcpy(datacrt, h_in, kSubWords * 8);
+    return KSPIR_OK;
 }
 
 int kspir_db_download(kspir_ctx* c, uint64_t* datacrt, size_t words) {

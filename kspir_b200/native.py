@@ -44,6 +44,8 @@ SIGNATURES = {
     "kspir_db_preprocess": (_i, [_vp, _vp, _sz, _vp]),
     "kspir_db_preprocess_device": (_i, [_vp, _vp, _sz, _vp]),
     "kspir_db_download": (_i, [_vp, _vp, _sz]),
+    "kspir_database_tobsgsntt": (_i, [_vp, _vp, _vp]),
+    "kspir_database_tocrt": (_i, [_vp, _vp, _vp]),
     "kspir_perms_upload": (_i, [_vp, _vp, _sz]),
     "kspir_client_keys_upload": (_i, [_vp, _i, _vp, _vp, _vp, _vp]),
     "kspir_answer": (_i, [_vp, _i, _vp, _vp]),
@@ -208,6 +210,26 @@ class Context:
         ms = ctypes.c_float(0.0)
         self._check(self.lib.kspir_db_preprocess_device(self._h, ctypes.c_void_p(d_raw), words, ctypes.byref(ms)))
         return ms.value
+
+    def database_tobsgsntt(self, data) -> np.ndarray:
+        """Reference database_tobsgsntt of one sub-database on the device:
+        data [N][N/2] words < 65537 -> rows [N/2][N] mod crtMod."""
+        d = _u64(data).reshape(-1)
+        if d.size != N * N // 2:
+            raise ValueError("one sub-database: N * N / 2 words")
+        out = np.empty(N * N // 2, dtype=np.uint64)
+        self._check(self.lib.kspir_database_tobsgsntt(self._h, ptr(d), ptr(out)))
+        return out
+
+    def database_tocrt(self, data_ntt) -> np.ndarray:
+        """Reference database_tocrt of one sub-database on the device:
+        rows [N/2][N] -> datacrt [N][N/2]."""
+        d = _u64(data_ntt).reshape(-1)
+        if d.size != N * N // 2:
+            raise ValueError("one sub-database: N * N / 2 words")
+        out = np.empty(N * N // 2, dtype=np.uint64)
+        self._check(self.lib.kspir_database_tocrt(self._h, ptr(d), ptr(out)))
+        return out
 
     def download_db(self, out: np.ndarray | None = None) -> np.ndarray:
         words = self.r * N * N // 2

@@ -487,13 +487,12 @@ static void query_encode(int32_t* qe) {
     free(hexl_idx); free(rot); free(find);
 }
 
-int ko_db_preprocess(const uint64_t* raw, int N1, uint64_t* datacrt) {
+int ko_database_tobsgsntt(const uint64_t* raw, int N1, uint64_t* rows) {
     const int H = N / 2, N2 = N / 2 / N1;
     for (size_t i = 0; i < (size_t)N * H; i++)
         if (raw[i] >= KO_P) return -1;
     int32_t* qe = malloc(sizeof(int32_t) * N);
     int32_t* perms = malloc(sizeof(int32_t) * (size_t)N1 * N);
-    uint64_t* rows = malloc(8 * (size_t)H * N);
     uint64_t* row = malloc(8 * N);
     uint64_t* tmp = malloc(8 * N);
     query_encode(qe);
@@ -518,14 +517,26 @@ int ko_db_preprocess(const uint64_t* raw, int N1, uint64_t* datacrt) {
             ko_ntt_forward(row, KO_CRTMOD);
             memcpy(x, row, 8 * N);
         }
-    /* crt form, crt.cpp:868-880 */
+    free(qe); free(perms); free(row); free(tmp);
+    return 0;
+}
+
+void ko_database_tocrt(const uint64_t* rows, uint64_t* datacrt) {
+    /* crt.cpp:868-880 */
+    const int H = N / 2;
     for (int z = 0; z < N; z++)
         for (int R = 0; R < H; R++) {
             uint64_t t = rows[(size_t)R * N + z];
             datacrt[(size_t)z * H + R] = ko_barrett_coeff(t, 0) | ko_barrett_coeff(t, 1) << 32;
         }
-    free(qe); free(perms); free(rows); free(row); free(tmp);
-    return 0;
+}
+
+int ko_db_preprocess(const uint64_t* raw, int N1, uint64_t* datacrt) {
+    uint64_t* rows = malloc(8 * (size_t)(N / 2) * N);
+    int rc = ko_database_tobsgsntt(raw, N1, rows);
+    if (rc == 0) ko_database_tocrt(rows, datacrt);
+    free(rows);
+    return rc;
 }
 
 /* ------------------------------------------------------------------ */

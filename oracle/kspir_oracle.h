@@ -61,6 +61,10 @@ void ko_scan(const uint64_t* db, const uint64_t* cipherbuf, int N1, uint64_t* ou
  * database_tocrt (twosteps.cpp:42-179, crt.cpp:859-885).  raw [N][N/2] words
  * < p (else -1), datacrt [N][N/2]. */
 int ko_db_preprocess(const uint64_t* raw, int N1, uint64_t* datacrt);
+/* The two steps apart: database_tobsgsntt (raw -> rows [N/2][N] mod crtMod,
+ * -1 for a word >= p) and database_tocrt (rows -> datacrt [N][N/2]). */
+int ko_database_tobsgsntt(const uint64_t* raw, int N1, uint64_t* rows);
+void ko_database_tocrt(const uint64_t* rows, uint64_t* datacrt);
 
 /* HEXL-order negacyclic transforms for modulus in {crtMod, bsMod, p, q1, q2}. */
 int ko_ntt_forward(uint64_t* a, uint64_t modulus);

@@ -79,6 +79,8 @@ def lib():
             L.ko_pow_mod_index.argtypes = [ctypes.c_int, ctypes.c_int]
             L.ko_giant_steps.argtypes = [vp, vp, ctypes.c_int, vp]
             L.ko_db_preprocess.argtypes = [vp, ctypes.c_int, vp]
+            L.ko_database_tobsgsntt.argtypes = [vp, ctypes.c_int, vp]
+            L.ko_database_tocrt.argtypes = [vp, vp]
             _lib = L
     return _lib
 
@@ -115,6 +117,8 @@ def ref():
             L.ref_pir_keep_raw.argtypes = [ctypes.c_int]
             L.ref_pir_get_raw.argtypes = [vp]
             L.ref_db_preprocess.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp]
+            L.ref_database_tobsgsntt.argtypes = [vp, ctypes.c_int, vp]
+            L.ref_database_tocrt.argtypes = [vp, ctypes.c_int, vp]
             _ref = L
     return _ref
 
@@ -212,6 +216,37 @@ def db_preprocess(raw, r, N1):
     for k in range(r):
         if lib().ko_db_preprocess(_p(raw[k * num:(k + 1) * num]), N1, _p(out[k * num:(k + 1) * num])):
             raise ValueError("database entries must be below p")
+    return out
+
+
+def database_tobsgsntt(raw_sub, N1):
+    """database_tobsgsntt of one sub-database (restatement): rows [N/2][N]."""
+    raw_sub = np.ascontiguousarray(raw_sub, dtype=np.uint64)
+    out = np.empty(N * N // 2, dtype=np.uint64)
+    if lib().ko_database_tobsgsntt(_p(raw_sub), N1, _p(out)):
+        raise ValueError("database entries must be below p")
+    return out
+
+
+def database_tocrt(rows):
+    """database_tocrt of one sub-database (restatement): datacrt [N][N/2]."""
+    rows = np.ascontiguousarray(rows, dtype=np.uint64)
+    out = np.empty(N * N // 2, dtype=np.uint64)
+    lib().ko_database_tocrt(_p(rows), _p(out))
+    return out
+
+
+def ref_database_tobsgsntt(raw_sub, N1):
+    raw_sub = np.ascontiguousarray(raw_sub, dtype=np.uint64)
+    out = np.empty(N * N // 2, dtype=np.uint64)
+    ref().ref_database_tobsgsntt(_p(raw_sub), N1, _p(out))
+    return out
+
+
+def ref_database_tocrt(rows, N1=128):
+    rows = np.ascontiguousarray(rows, dtype=np.uint64)
+    out = np.empty(N * N // 2, dtype=np.uint64)
+    ref().ref_database_tocrt(_p(rows), N1, _p(out))
     return out
 
 

@@ -206,6 +206,22 @@ void ref_db_preprocess(const uint64_t* raw, int r, int N1, uint64_t* datacrt) {
     }
 }
 
+// database_tobsgsntt alone: raw [N][N/2] -> rows [N/2][N] (its `result`).
+void ref_database_tobsgsntt(const uint64_t* raw, int N1, uint64_t* rows) {
+    std::vector<std::vector<uint64_t> > data(N, std::vector<uint64_t>(N / 2, 0));
+    std::vector<std::vector<uint64_t> > data_ntt(N / 2, std::vector<uint64_t>(N, 0));
+    for (size_t i = 0; i < (size_t)N; i++) memcpy(data[i].data(), raw + i * (N / 2), (N / 2) * 8);
+    database_tobsgsntt(data_ntt, data, crtMod, N1);
+    for (size_t i = 0; i < (size_t)N / 2; i++) memcpy(rows + i * N, data_ntt[i].data(), N * 8);
+}
+
+// database_tocrt alone: rows [N/2][N] -> datacrt [N][N/2].
+void ref_database_tocrt(const uint64_t* rows, int N1, uint64_t* datacrt) {
+    std::vector<std::vector<uint64_t> > data_ntt(N / 2, std::vector<uint64_t>(N, 0));
+    for (size_t i = 0; i < (size_t)N / 2; i++) memcpy(data_ntt[i].data(), rows + i * N, N * 8);
+    database_tocrt(datacrt, data_ntt, N1);
+}
+
 void ref_pir_target(uint32_t* col, uint32_t* packing_slot) {
     *col = g_state.target_col;
     *packing_slot = g_state.target_packing;

@@ -1,4 +1,5 @@
-"""Database preprocessing on the device (kspir_db_preprocess): the reference's
+"""Database preprocessing on the device (kspir_db_preprocess, and the one-for-one
+kspir_database_tobsgsntt / kspir_database_tocrt): the reference's
 database_tobsgsntt + database_tocrt (twosteps.cpp:42-179, crt.cpp:859-885).
 
 Integer work, so the bar is word-for-word equality with the oracle's
@@ -121,3 +122,26 @@ def test_preprocess_testpir_database_recovers_the_record():
     msg = np.zeros(N, np.uint64)
     L.ref_pir_decrypt(po._p(resp), po._p(msg))
     assert (msg == np.arange(1, N + 1)).all(), msg[:8]
+
+
+@pytest.mark.parametrize("N1", [64, 128, 256])
+def test_database_tobsgsntt_and_tocrt_one_for_one(N1):
+    # the reference's two functions separately, one sub-database: the rows mod
+    # crtMod of database_tobsgsntt, and database_tocrt on arbitrary 64-bit words
+    raw = synth.gen_raw_db(70 + N1, 1)
+    raw[:9] = synth.edge_raw_db()[:9]
+    rng = np.random.default_rng(N1)
+    words = rng.integers(0, 2 ** 64 - 1, size=N * N // 2, dtype=np.uint64, endpoint=True)
+    words[:6] = [0, 2 ** 64 - 1, po.Q1, po.Q2, po.CRTMOD, po.CRTMOD - 1]
+    with kb.Context(1, N1) as ctx:
+        rows = ctx.database_tobsgsntt(raw)
+        assert (rows == po.database_tobsgsntt(raw, N1)).all()
+        assert (ctx.database_tocrt(rows) == po.db_preprocess(raw, 1, N1)).all()
+        assert (ctx.database_tocrt(words) == po.database_tocrt(words)).all()
+        bad = raw.copy()
+        bad[5] = 1 << 40
+        with pytest.raises(kb.KspirError) as ei:
+            ctx.database_tobsgsntt(bad)
+        assert ei.value.code == kb.native.ERR_INVALID_ARG
+    if po.ref_available():
+        assert (rows == po.ref_database_tobsgsntt(raw, N1)).all()

@@ -1,7 +1,9 @@
 """The drop-in: the reference's unmodified tests/test-pir.cpp, linked with
 kspir_b200/cpp/reference_api.cpp in place of the reference's three answer
-functions (built by `make -C oracle testpir-gpu`), runs its online answer on
-the GPU and recovers the planted record like the reference build does."""
+functions and its two preprocessing functions (database_tobsgsntt,
+database_tocrt; built by `make -C oracle testpir-gpu`), preprocesses its
+database and runs its online answer on the GPU, and recovers the planted
+record like the reference build does."""
 import os
 import subprocess
 
@@ -20,3 +22,4 @@ def test_unmodified_testpir_recovers_the_record_through_the_gpu():
     want = "the recovered result = [" + ", ".join(str(i) for i in range(1, 17)) + ", ..., 4096]"
     assert want in out.stdout, out.stdout[-2000:]
     assert "online server response costs" in out.stdout
+    assert "server preprocessing costs" in out.stdout

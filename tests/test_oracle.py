@@ -263,3 +263,16 @@ def test_db_preprocess_equals_reference_on_testpir_database():
     live = np.zeros_like(out)
     L.ref_pir_get_inputs(po._p(live), None, None, None, None, None, None)
     assert (live == out).all()
+
+
+@needs_ref
+def test_db_preprocess_steps_equal_reference():
+    from kspir_b200 import synth
+    raw = synth.gen_raw_db(35, 1)
+    rows = po.database_tobsgsntt(raw, 64)
+    assert (rows == po.ref_database_tobsgsntt(raw, 64)).all()
+    rng = np.random.default_rng(36)
+    words = rng.integers(0, 2 ** 64 - 1, size=N * N // 2, dtype=np.uint64, endpoint=True)
+    words[:4] = [0, 2 ** 64 - 1, po.Q1, po.CRTMOD]
+    assert (po.database_tocrt(words) == po.ref_database_tocrt(words)).all()
+    assert (po.database_tocrt(rows) == po.db_preprocess(raw, 1, 64)).all()
