@@ -45,6 +45,7 @@ extern "C" {
 #define KSPIR_ERR_OOM -4           /* device allocation failed */
 #define KSPIR_ERR_TIMEOUT -5       /* a bounded device-side wait gave up */
 #define KSPIR_ERR_BUSY -6          /* no free slot (serving admission) */
+#define KSPIR_ERR_IO -7            /* file error, or a malformed / corrupted container */
 
 #define KSPIR_N 4096
 
@@ -95,6 +96,46 @@ int kspir_db_preprocess_device(kspir_ctx* ctx, const uint64_t* d_data, size_t wo
  * Neither touches the resident database. */
 int kspir_database_tobsgsntt(kspir_ctx* ctx, const uint64_t* data, uint64_t* result);
 int kspir_database_tocrt(kspir_ctx* ctx, const uint64_t* data_ntt, uint64_t* datacrt);
+
+/* ------------------------------------------------------------------------
+ * Wire and file formats.  The reference has no serialization; these carry the
+ * words of its objects (RlweCiphertext lwe.h:48-110: a then b; the key maps
+ * flattened as for kspir_client_keys_upload) packed to their moduli: words
+ * mod crtMod as 7 little-endian bytes, words mod bsMod as 3.  Each container
+ * has a header with a format version and a 64-bit checksum of its payload;
+ * a wrong magic, version, size or checksum gives KSPIR_ERR_IO, a word not
+ * below its modulus KSPIR_ERR_INVALID_ARG.  Host-only except the database
+ * file functions.
+ *
+ * Client key bundle: 64-byte header + baby (rows 0-2 at 7 bytes, rows 3-5 at
+ * 3 bytes per word), giant, packing, rgsw (7 bytes per word); 17.7 MiB at
+ * r = 16, N1 = 128 (27.1 MiB as u64 words).  kspir_key_bundle_bytes gives the
+ * size (0 for an invalid shape).  kspir_client_keys_upload_bundle =
+ * kspir_key_bundle_read + kspir_client_keys_upload. */
+size_t kspir_key_bundle_bytes(int r, int N1);
+int kspir_key_bundle_write(int r, int N1, const uint64_t* baby, const uint64_t* giant, const uint64_t* packing,
+                           const uint64_t* rgsw, uint8_t* out, size_t out_bytes);
+int kspir_key_bundle_read(const uint8_t* bundle, size_t bytes, int r, int N1, uint64_t* baby, uint64_t* giant,
+                          uint64_t* packing, uint64_t* rgsw);
+int kspir_client_keys_upload_bundle(kspir_ctx* ctx, int client, const uint8_t* bundle, size_t bytes);
+
+/* Query and response messages: 16-byte header + packed words.  A query
+ * ([2][2][N], crtMod part then bsMod part) is 81,936 bytes (131,072 as u64
+ * words), a response ([2][N] mod crtMod) 57,360 bytes (65,536). */
+#define KSPIR_QUERY_WIRE_BYTES (16 + 2 * KSPIR_N * 7 + 2 * KSPIR_N * 3)
+#define KSPIR_RESPONSE_WIRE_BYTES (16 + 2 * KSPIR_N * 7)
+int kspir_query_pack(const uint64_t* query, uint8_t* out);
+int kspir_query_unpack(const uint8_t* in, size_t bytes, uint64_t* query);
+int kspir_response_pack(const uint64_t* response, uint8_t* out);
+int kspir_response_unpack(const uint8_t* in, size_t bytes, uint64_t* response);
+
+/* The resident (preprocessed) database as a file: 64-byte header (r, N1,
+ * checksum computed on the device) + the datacrt words, 8 bytes each.
+ * kspir_db_load checks the file against the context's (r, N1) and the
+ * checksum before it replaces the resident database (a failed load leaves it
+ * as it was); it skips the preprocessing on a restart. */
+int kspir_db_save(kspir_ctx* ctx, const char* path);
+int kspir_db_load(kspir_ctx* ctx, const char* path);
 
 /* Copies the resident database (datacrt layout, r * N * N / 2 words) to host. */
 int kspir_db_download(kspir_ctx* ctx, uint64_t* datacrt, size_t words);

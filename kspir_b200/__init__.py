@@ -23,9 +23,11 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from .native import (BSMOD, CRTMOD, N, Q1, Q2, SCAN_CUDA, SCAN_MMA4, SCAN_MMA8, SCAN_MMA16, SCAN_MMA32, SCAN_NAMES,
-                     Context, KspirError, LIB_PATH, STAGE_CIPHERBUF, STAGE_EXT, STAGE_RESULT, STAGE_SCAN, Server, load,
-                     permutation_matrix)
+from .native import (BSMOD, CRTMOD, N, Q1, Q2, QUERY_WIRE_BYTES, RESPONSE_WIRE_BYTES, SCAN_CUDA, SCAN_MMA4,
+                     SCAN_MMA8, SCAN_MMA16, SCAN_MMA32, SCAN_NAMES, Context, KspirError, LIB_PATH, STAGE_CIPHERBUF,
+                     STAGE_EXT, STAGE_RESULT, STAGE_SCAN, Server, key_bundle_bytes, key_bundle_read,
+                     key_bundle_write, load, permutation_matrix, query_pack, query_unpack, response_pack,
+                     response_unpack)
 
 __all__ = [
     "N", "Q1", "Q2", "CRTMOD", "BSMOD", "Context", "Server", "KspirError", "load", "LIB_PATH", "permutation_matrix",
@@ -33,6 +35,8 @@ __all__ = [
     "SCAN_CUDA", "SCAN_MMA4", "SCAN_MMA8", "SCAN_MMA16", "SCAN_MMA32", "SCAN_NAMES",
     "AutoKeyBSGSRNS", "AutoKey", "RGSWCiphertext",
     "matrix_vector_mul_bsgs_rns_crt_large", "externalProduct", "packingRLWEs",
+    "key_bundle_bytes", "key_bundle_write", "key_bundle_read", "query_pack", "query_unpack", "response_pack",
+    "response_unpack", "QUERY_WIRE_BYTES", "RESPONSE_WIRE_BYTES",
 ]
 
 

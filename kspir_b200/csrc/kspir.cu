@@ -21,6 +21,7 @@
 #include "gadget.cuh"
 #include "k_baby.cuh"
 #include "k_db.cuh"
+#include "formats.cuh"
 #include "k_query.cuh"
 #include "k_scan.cuh"
 #include "k_scan_mma.cuh"
@@ -790,6 +791,7 @@ const char* kspir_strerror(int code) {
         case KSPIR_ERR_OOM: return "out of device memory";
         case KSPIR_ERR_TIMEOUT: return "device-side wait timed out";
         case KSPIR_ERR_BUSY: return "no free slot";
+        case KSPIR_ERR_IO: return "file or format error";
         default: return "unknown error";
     }
 }
@@ -1062,6 +1064,261 @@ int kspir_db_download(kspir_ctx* c, uint64_t* datacrt, size_t words) {
     std::lock_guard<std::mutex> lk(c->mu);
     KS_CUDA(c, cudaSetDevice(c->device));
     KS_COPY(c, datacrt, c->db, need * 8, cudaMemcpyDeviceToHost);
+    return KSPIR_OK;
+}
+
+// ---------------------------------------------------------------------------
+// wire and file formats (formats.cuh)
+
+}  // extern "C"
+
+namespace {
+bool shape_ok(int r, int N1) {
+    auto pow2 = [](int v) { return v > 0 && (v & (v - 1)) == 0; };
+    return pow2(r) && r <= 512 && pow2(N1) && N1 >= 64 && N1 <= 256;
+}
+
+// per-word byte width of each row of the key payload, in payload order, with
+// the array it comes from and the modulus its words are below
+template <class F>
+void key_rows(int r, int N1, F&& f) {
+    const int N2 = kN / 2 / N1, levels = log2_ceil(r);
+    for (int i = 0; i < N1 / 2; i++)
+        for (int j = 0; j < 6; j++)
+            for (int comp = 0; comp < 2; comp++)
+                f(0, (((size_t)i * 6 + j) * 2 + comp) * kN, j < 3 ? 7 : 3, j < 3 ? kCrtMod : (uint64_t)kBsMod);
+    for (size_t k = 0; k < (size_t)(N2 - 1) * 2 * 2; k++) f(1, k * kN, 7, kCrtMod);
+    for (size_t k = 0; k < (size_t)levels * 4 * 2; k++) f(2, k * kN, 7, kCrtMod);
+    for (size_t k = 0; k < 4 * 2; k++) f(3, k * kN, 7, kCrtMod);
+}
+}  // namespace
+
+extern "C" {
+
+size_t kspir_key_bundle_bytes(int r, int N1) {
+    return shape_ok(r, N1) ? kFileHeader + key_payload_bytes(r, N1) : 0;
+}
+
+int kspir_key_bundle_write(int r, int N1, const uint64_t* baby, const uint64_t* giant, const uint64_t* packing,
+                           const uint64_t* rgsw, uint8_t* out, size_t out_bytes) {
+    if (!shape_ok(r, N1) || !baby || !rgsw || !out) return set_err(nullptr, KSPIR_ERR_INVALID_ARG, "invalid arguments");
+    if ((kN / 2 / N1 > 1 && !giant) || (r > 1 && !packing)) return set_err(nullptr, KSPIR_ERR_INVALID_ARG, "missing key array");
+    if (out_bytes != kspir_key_bundle_bytes(r, N1)) return set_err(nullptr, KSPIR_ERR_INVALID_ARG, "bundle size");
+    const uint64_t* src[4] = {baby, giant, packing, rgsw};
+    bool ok = true;
+    key_rows(r, N1, [&](int a, size_t off, int, uint64_t q) { ok = ok && canonical(src[a] + off, kN, q); });
+    if (!ok) return set_err(nullptr, KSPIR_ERR_INVALID_ARG, "key word not canonical");
+    uint8_t* p = out + kFileHeader;
+    key_rows(r, N1, [&](int a, size_t off, int width, uint64_t) {
+        pack_words(src[a] + off, kN, width, p);
+        p += (size_t)kN * width;
+    });
+    FileHeader h{};
+    memcpy(h.magic, kKeyMagic, 8);
+    h.version = kFormatVersion;
+    h.n = kN;
+    h.r = (uint32_t)r;
+    h.n1 = (uint32_t)N1;
+    h.payload_bytes = key_payload_bytes(r, N1);
+    h.checksum = payload_checksum(out + kFileHeader, h.payload_bytes);
+    memcpy(out, &h, sizeof(h));
+    return KSPIR_OK;
+}
+
+int kspir_key_bundle_read(const uint8_t* bundle, size_t bytes, int r, int N1, uint64_t* baby, uint64_t* giant,
+                          uint64_t* packing, uint64_t* rgsw) {
+    if (!shape_ok(r, N1) || !bundle || !baby || !rgsw) return set_err(nullptr, KSPIR_ERR_INVALID_ARG, "invalid arguments");
+    if ((kN / 2 / N1 > 1 && !giant) || (r > 1 && !packing)) return set_err(nullptr, KSPIR_ERR_INVALID_ARG, "missing key array");
+    FileHeader h;
+    if (bytes < sizeof(h)) return set_err(nullptr, KSPIR_ERR_IO, "key bundle truncated");
+    memcpy(&h, bundle, sizeof(h));
+    if (memcmp(h.magic, kKeyMagic, 8) != 0 || h.version != kFormatVersion || h.n != (uint32_t)kN)
+        return set_err(nullptr, KSPIR_ERR_IO, "not a key bundle of this format version");
+    if (h.r != (uint32_t)r || h.n1 != (uint32_t)N1) return set_err(nullptr, KSPIR_ERR_INVALID_ARG, "key bundle for another (r, N1)");
+    if (h.payload_bytes != key_payload_bytes(r, N1) || bytes != kFileHeader + h.payload_bytes)
+        return set_err(nullptr, KSPIR_ERR_IO, "key bundle size");
+    if (payload_checksum(bundle + kFileHeader, h.payload_bytes) != h.checksum)
+        return set_err(nullptr, KSPIR_ERR_IO, "key bundle checksum mismatch");
+    uint64_t* dst[4] = {baby, giant, packing, rgsw};
+    const uint8_t* p = bundle + kFileHeader;
+    bool ok = true;
+    key_rows(r, N1, [&](int a, size_t off, int width, uint64_t q) {
+        unpack_words(p, kN, width, dst[a] + off);
+        ok = ok && canonical(dst[a] + off, kN, q);
+        p += (size_t)kN * width;
+    });
+    return ok ? KSPIR_OK : set_err(nullptr, KSPIR_ERR_INVALID_ARG, "key word not canonical");
+}
+
+int kspir_client_keys_upload_bundle(kspir_ctx* c, int client, const uint8_t* bundle, size_t bytes) {
+    if (!c) return KSPIR_ERR_INVALID_ARG;
+    const int r = c->p.r, N1 = c->N1;
+    std::vector<uint64_t> baby((size_t)(N1 / 2) * 6 * 2 * kN), giant((size_t)(c->N2 - 1) * 2 * 2 * kN),
+        packing((size_t)c->levels * 4 * 2 * kN), rgsw((size_t)4 * 2 * kN);
+    int rc = kspir_key_bundle_read(bundle, bytes, r, N1, baby.data(), giant.empty() ? nullptr : giant.data(),
+                                   packing.empty() ? nullptr : packing.data(), rgsw.data());
+    if (rc) return set_err(c, rc, g_thread_err);
+    return kspir_client_keys_upload(c, client, baby.data(), giant.empty() ? nullptr : giant.data(),
+                                    packing.empty() ? nullptr : packing.data(), rgsw.data());
+}
+
+int kspir_query_pack(const uint64_t* query, uint8_t* out) {
+    if (!query || !out) return set_err(nullptr, KSPIR_ERR_INVALID_ARG, "null pointer");
+    if (!canonical(query, 2 * kN, kCrtMod) || !canonical(query + 2 * kN, 2 * kN, kBsMod))
+        return set_err(nullptr, KSPIR_ERR_INVALID_ARG, "query word not canonical");
+    pack_words(query, 2 * kN, 7, out + kWireHeader);
+    pack_words(query + 2 * kN, 2 * kN, 3, out + kWireHeader + (size_t)2 * kN * 7);
+    WireHeader h{};
+    memcpy(h.magic, kWireMagic, 4);
+    h.version = (uint16_t)kFormatVersion;
+    h.kind = 1;
+    h.checksum = payload_checksum(out + kWireHeader, kQueryWireBytes - kWireHeader);
+    memcpy(out, &h, sizeof(h));
+    return KSPIR_OK;
+}
+
+int kspir_response_pack(const uint64_t* response, uint8_t* out) {
+    if (!response || !out) return set_err(nullptr, KSPIR_ERR_INVALID_ARG, "null pointer");
+    if (!canonical(response, 2 * kN, kCrtMod)) return set_err(nullptr, KSPIR_ERR_INVALID_ARG, "response word not canonical");
+    pack_words(response, 2 * kN, 7, out + kWireHeader);
+    WireHeader h{};
+    memcpy(h.magic, kWireMagic, 4);
+    h.version = (uint16_t)kFormatVersion;
+    h.kind = 2;
+    h.checksum = payload_checksum(out + kWireHeader, kResponseWireBytes - kWireHeader);
+    memcpy(out, &h, sizeof(h));
+    return KSPIR_OK;
+}
+
+namespace {
+int wire_check(const uint8_t* in, size_t bytes, uint16_t kind, size_t want) {
+    if (!in) return set_err(nullptr, KSPIR_ERR_INVALID_ARG, "null pointer");
+    WireHeader h;
+    if (bytes != want) return set_err(nullptr, KSPIR_ERR_IO, "wire message size");
+    memcpy(&h, in, sizeof(h));
+    if (memcmp(h.magic, kWireMagic, 4) != 0 || h.version != kFormatVersion || h.kind != kind)
+        return set_err(nullptr, KSPIR_ERR_IO, "not a wire message of this kind and format version");
+    if (payload_checksum(in + kWireHeader, want - kWireHeader) != h.checksum)
+        return set_err(nullptr, KSPIR_ERR_IO, "wire message checksum mismatch");
+    return KSPIR_OK;
+}
+}  // namespace
+
+int kspir_query_unpack(const uint8_t* in, size_t bytes, uint64_t* query) {
+    if (!query) return set_err(nullptr, KSPIR_ERR_INVALID_ARG, "null pointer");
+    int rc = wire_check(in, bytes, 1, kQueryWireBytes);
+    if (rc) return rc;
+    unpack_words(in + kWireHeader, 2 * kN, 7, query);
+    unpack_words(in + kWireHeader + (size_t)2 * kN * 7, 2 * kN, 3, query + 2 * kN);
+    if (!canonical(query, 2 * kN, kCrtMod) || !canonical(query + 2 * kN, 2 * kN, kBsMod))
+        return set_err(nullptr, KSPIR_ERR_INVALID_ARG, "query word not canonical");
+    return KSPIR_OK;
+}
+
+int kspir_response_unpack(const uint8_t* in, size_t bytes, uint64_t* response) {
+    if (!response) return set_err(nullptr, KSPIR_ERR_INVALID_ARG, "null pointer");
+    int rc = wire_check(in, bytes, 2, kResponseWireBytes);
+    if (rc) return rc;
+    unpack_words(in + kWireHeader, 2 * kN, 7, response);
+    if (!canonical(response, 2 * kN, kCrtMod)) return set_err(nullptr, KSPIR_ERR_INVALID_ARG, "response word not canonical");
+    return KSPIR_OK;
+}
+
+namespace {
+// checksum of the n words at d on the device (synchronises)
+int device_checksum(kspir_ctx* c, const uint64_t* d, size_t n, uint64_t* out) {
+    unsigned long long* acc = nullptr;
+    KS_CUDA(c, cudaMalloc(&acc, sizeof(*acc)));
+    int rc = KSPIR_OK;
+    cudaError_t e = cudaMemsetAsync(acc, 0, sizeof(*acc), c->stream);
+    if (e == cudaSuccess) {
+        k_words_checksum<<<c->nsm * 8, 256, 0, c->stream>>>(d, n, acc);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, acc, sizeof(*acc), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) rc = set_err(c, KSPIR_ERR_CUDA, std::string("database checksum: ") + cudaGetErrorString(e));
+    cudaFree(acc);
+    return rc;
+}
+}  // namespace
+
+int kspir_db_save(kspir_ctx* c, const char* path) {
+    if (!c || !path) return KSPIR_ERR_INVALID_ARG;
+    if (!c->db_loaded) return set_err(c, KSPIR_ERR_NOT_READY, "database not uploaded");
+    std::lock_guard<std::mutex> lk(c->mu);
+    KS_CUDA(c, cudaSetDevice(c->device));
+    const size_t words = (size_t)c->p.r * kN * (kN / 2);
+    FileHeader h{};
+    memcpy(h.magic, kDbMagic, 8);
+    h.version = kFormatVersion;
+    h.n = kN;
+    h.r = (uint32_t)c->p.r;
+    h.n1 = (uint32_t)c->N1;
+    h.payload_bytes = words * 8;
+    int rc = device_checksum(c, c->db, words, &h.checksum);
+    if (rc) return rc;
+    FILE* f = fopen(path, "wb");
+    if (!f) return set_err(c, KSPIR_ERR_IO, std::string("cannot create ") + path);
+    bool ok = fwrite(&h, sizeof(h), 1, f) == 1;
+    // through a pinned staging buffer, 64 MiB at a time
+    const size_t chunk = (size_t)8 << 20;
+    uint64_t* stage = nullptr;
+    if (ok && cudaHostAlloc(&stage, chunk * 8, cudaHostAllocDefault) != cudaSuccess) ok = false;
+    for (size_t off = 0; ok && off < words; off += chunk) {
+        const size_t n = std::min(chunk, words - off);
+        ok = cudaMemcpyAsync(stage, c->db + off, n * 8, cudaMemcpyDeviceToHost, c->stream) == cudaSuccess &&
+             cudaStreamSynchronize(c->stream) == cudaSuccess && fwrite(stage, 8, n, f) == n;
+    }
+    if (stage) cudaFreeHost(stage);
+    ok = (fclose(f) == 0) && ok;
+    return ok ? KSPIR_OK : set_err(c, KSPIR_ERR_IO, std::string("writing ") + path);
+}
+
+int kspir_db_load(kspir_ctx* c, const char* path) {
+    if (!c || !path) return KSPIR_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(c->mu);
+    KS_CUDA(c, cudaSetDevice(c->device));
+    const size_t words = (size_t)c->p.r * kN * (kN / 2);
+    FILE* f = fopen(path, "rb");
+    if (!f) return set_err(c, KSPIR_ERR_IO, std::string("cannot open ") + path);
+    FileHeader h;
+    int rc = KSPIR_OK;
+    if (fread(&h, sizeof(h), 1, f) != 1 || memcmp(h.magic, kDbMagic, 8) != 0 || h.version != kFormatVersion ||
+        h.n != (uint32_t)kN)
+        rc = set_err(c, KSPIR_ERR_IO, std::string(path) + ": not a database file of this format version");
+    else if (h.r != (uint32_t)c->p.r || h.n1 != (uint32_t)c->N1 || h.payload_bytes != words * 8)
+        rc = set_err(c, KSPIR_ERR_INVALID_ARG, std::string(path) + ": database of another (r, N1)");
+    // into a fresh device buffer: the resident database changes only once the
+    // whole file has arrived and its checksum matches
+    uint64_t* d = nullptr;
+    uint64_t* stage = nullptr;
+    const size_t chunk = (size_t)8 << 20;
+    if (!rc && cudaMalloc(&d, words * 8) != cudaSuccess) rc = set_err(c, KSPIR_ERR_OOM, "database buffer");
+    if (!rc && cudaHostAlloc(&stage, chunk * 8, cudaHostAllocDefault) != cudaSuccess)
+        rc = set_err(c, KSPIR_ERR_OOM, "staging buffer");
+    for (size_t off = 0; !rc && off < words; off += chunk) {
+        const size_t n = std::min(chunk, words - off);
+        if (fread(stage, 8, n, f) != n) rc = set_err(c, KSPIR_ERR_IO, std::string(path) + ": truncated");
+        else if (cudaMemcpyAsync(d + off, stage, n * 8, cudaMemcpyHostToDevice, c->stream) != cudaSuccess ||
+                 cudaStreamSynchronize(c->stream) != cudaSuccess)
+            rc = set_err(c, KSPIR_ERR_CUDA, "database upload");
+    }
+    fclose(f);
+    if (stage) cudaFreeHost(stage);
+    uint64_t sum = 0;
+    if (!rc) rc = device_checksum(c, d, words, &sum);
+    if (!rc && sum != h.checksum) rc = set_err(c, KSPIR_ERR_IO, std::string(path) + ": checksum mismatch");
+    if (rc) {
+        cudaFree(d);
+        return rc;
+    }
+    cudaFree(c->db);
+    c->db = d;
+    c->db_loaded = false;
+    rc = build_dbop(c);
+    if (rc) return rc;
+    c->db_loaded = true;
     return KSPIR_OK;
 }
 

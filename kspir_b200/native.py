@@ -44,6 +44,16 @@ SIGNATURES = {
     "kspir_db_preprocess": (_i, [_vp, _vp, _sz, _vp]),
     "kspir_db_preprocess_device": (_i, [_vp, _vp, _sz, _vp]),
     "kspir_db_download": (_i, [_vp, _vp, _sz]),
+    "kspir_key_bundle_bytes": (_sz, [_i, _i]),
+    "kspir_key_bundle_write": (_i, [_i, _i, _vp, _vp, _vp, _vp, _vp, _sz]),
+    "kspir_key_bundle_read": (_i, [_vp, _sz, _i, _i, _vp, _vp, _vp, _vp]),
+    "kspir_client_keys_upload_bundle": (_i, [_vp, _i, _vp, _sz]),
+    "kspir_query_pack": (_i, [_vp, _vp]),
+    "kspir_query_unpack": (_i, [_vp, _sz, _vp]),
+    "kspir_response_pack": (_i, [_vp, _vp]),
+    "kspir_response_unpack": (_i, [_vp, _sz, _vp]),
+    "kspir_db_save": (_i, [_vp, ctypes.c_char_p]),
+    "kspir_db_load": (_i, [_vp, ctypes.c_char_p]),
     "kspir_database_tobsgsntt": (_i, [_vp, _vp, _vp]),
     "kspir_database_tocrt": (_i, [_vp, _vp, _vp]),
     "kspir_perms_upload": (_i, [_vp, _vp, _sz]),
@@ -145,6 +155,71 @@ class KspirError(RuntimeError):
         self.code = code
 
 
+ERR_IO = -7
+QUERY_WIRE_BYTES = 16 + 2 * N * 7 + 2 * N * 3
+RESPONSE_WIRE_BYTES = 16 + 2 * N * 7
+
+
+def _host_check(rc: int):
+    if rc:
+        lib = load()
+        raise KspirError(rc, lib.kspir_last_error(None).decode() or lib.kspir_strerror(rc).decode())
+
+
+def _key_shapes(r: int, N1: int) -> dict:
+    N2, levels = N // 2 // N1, max(0, int(r).bit_length() - 1)
+    return dict(baby=(N1 // 2) * 6 * 2 * N, giant=(N2 - 1) * 2 * 2 * N, packing=levels * 4 * 2 * N, rgsw=4 * 2 * N)
+
+
+def key_bundle_bytes(r: int, N1: int) -> int:
+    return int(load().kspir_key_bundle_bytes(r, N1))
+
+
+def key_bundle_write(r: int, N1: int, baby, giant, packing, rgsw) -> np.ndarray:
+    """One client's key material as a checksummed bundle (packed words)."""
+    arrs = [None if a is None or np.size(a) == 0 else _u64(a).reshape(-1) for a in (baby, giant, packing, rgsw)]
+    out = np.empty(key_bundle_bytes(r, N1), dtype=np.uint8)
+    _host_check(load().kspir_key_bundle_write(r, N1, *[ptr(a) for a in arrs], ptr(out), out.size))
+    return out
+
+
+def key_bundle_read(bundle, r: int, N1: int) -> dict:
+    b = np.ascontiguousarray(bundle, dtype=np.uint8).reshape(-1)
+    shapes = _key_shapes(r, N1)
+    keys = {k: np.empty(n, dtype=np.uint64) for k, n in shapes.items()}
+    args = [ptr(keys[k]) if shapes[k] else None for k in ("baby", "giant", "packing", "rgsw")]
+    _host_check(load().kspir_key_bundle_read(ptr(b), b.size, r, N1, *args))
+    return keys
+
+
+def query_pack(query) -> np.ndarray:
+    q = _u64(query).reshape(-1)
+    out = np.empty(QUERY_WIRE_BYTES, dtype=np.uint8)
+    _host_check(load().kspir_query_pack(ptr(q), ptr(out)))
+    return out
+
+
+def query_unpack(msg) -> np.ndarray:
+    m = np.ascontiguousarray(msg, dtype=np.uint8).reshape(-1)
+    out = np.empty(4 * N, dtype=np.uint64)
+    _host_check(load().kspir_query_unpack(ptr(m), m.size, ptr(out)))
+    return out
+
+
+def response_pack(response) -> np.ndarray:
+    r = _u64(response).reshape(-1)
+    out = np.empty(RESPONSE_WIRE_BYTES, dtype=np.uint8)
+    _host_check(load().kspir_response_pack(ptr(r), ptr(out)))
+    return out
+
+
+def response_unpack(msg) -> np.ndarray:
+    m = np.ascontiguousarray(msg, dtype=np.uint8).reshape(-1)
+    out = np.empty(2 * N, dtype=np.uint64)
+    _host_check(load().kspir_response_unpack(ptr(m), m.size, ptr(out)))
+    return out
+
+
 def _u64(a) -> np.ndarray:
     a = np.ascontiguousarray(a, dtype=np.uint64)
     return a
@@ -196,6 +271,18 @@ class Context:
     def upload_db(self, datacrt):
         d = _u64(datacrt).reshape(-1)
         self._check(self.lib.kspir_db_upload(self._h, ptr(d), d.size))
+
+    def upload_client_bundle(self, client: int, bundle):
+        b = np.ascontiguousarray(bundle, dtype=np.uint8).reshape(-1)
+        self._check(self.lib.kspir_client_keys_upload_bundle(self._h, client, ptr(b), b.size))
+
+    def save_db(self, path: str):
+        """The resident database as a checksummed file (kspir_db_save)."""
+        self._check(self.lib.kspir_db_save(self._h, os.fsencode(path)))
+
+    def load_db(self, path: str):
+        """Replaces the resident database with a file of kspir_db_save."""
+        self._check(self.lib.kspir_db_load(self._h, os.fsencode(path)))
 
     def preprocess_db(self, raw) -> float:
         """Reference database_tobsgsntt + database_tocrt of every sub-database
