@@ -46,6 +46,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "answer ms/query & batched queries/s at 256 MB DB (bit-exact); GB/s vs HBM peak"
 N = 4096
+CRTMOD = 268369921 * 249561089
 
 
 def parse():
@@ -244,6 +245,29 @@ def bench_preprocess(args, ctx, raw, rank):
     return out
 
 
+def bench_client(ctx, n=128, reps=5):
+    """Device test clients: query_bsgs_rns for n clients in one call, and
+    decrypt_bsgs_total of n responses (host buffers in and out, timed end to
+    end on the host; synthetic ternary secrets)."""
+    rng = np.random.default_rng(99)
+    sec = rng.integers(-1, 2, size=(n, N)).astype(np.int64)
+    sec = np.where(sec < 0, sec + CRTMOD, sec).astype(np.uint64)
+    rows = rng.integers(0, N // 2, size=n).astype(np.uint32)
+    q = ctx.client_queries(sec, rows, seed=1)          # warm-up (tables, allocation)
+    t0 = time.perf_counter()
+    for i in range(reps):
+        q = ctx.client_queries(sec, rows, seed=2 + i)
+    tq = (time.perf_counter() - t0) / reps
+    resp = np.ascontiguousarray(q[:, :2 * N])          # any canonical crtMod words
+    ctx.client_decrypt(sec, resp, 16)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        ctx.client_decrypt(sec, resp, 16)
+    td = (time.perf_counter() - t0) / reps
+    return {"batch": n, "queries_per_s": n / tq, "decrypts_per_s": n / td,
+            "note": "end to end through kspir_client_queries / kspir_client_decrypt with host buffers"}
+
+
 def run_gpu(args, rank, world, local_rank):
     import torch
 
@@ -361,6 +385,7 @@ def run_gpu(args, rank, world, local_rank):
         if batched:
             out["batched"] = batched
         out["db_preprocess"] = prep
+        out["client"] = bench_client(ctx)
         if world == 1 and not args.no_cpu_baseline:
             threads = host_threads()
             rate, kind, n, th = cpu_answer_rate(db, cl, perms, r, N1, args.cpu_seconds, threads)

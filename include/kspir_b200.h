@@ -137,6 +137,28 @@ int kspir_response_unpack(const uint8_t* in, size_t bytes, uint64_t* response);
 int kspir_db_save(kspir_ctx* ctx, const char* path);
 int kspir_db_load(kspir_ctx* ctx, const char* path);
 
+/* ------------------------------------------------------------------------
+ * The client side on the device (test clients, load generation).  Host
+ * buffers, n queries / responses per call, run on the context's device.
+ *
+ * kspir_client_queries: query_bsgs_rns (twosteps.cpp:279-318) for each
+ *   (secrets[i], rows[i]): secrets [n][N] in coefficient form mod crtMod (the
+ *   reference Secret's words; each must be small: below bsMod/2 or above
+ *   crtMod - bsMod/2), rows[i] < N/2, queries [n][2][2][N] (the layout of
+ *   kspir_answer's query).  Same algebra and message scaling as the
+ *   reference; its rand() draws are replaced by Philox4x32-10 keyed by `seed`
+ *   (query i uses counter block i), so a query is a deterministic function of
+ *   (secret, row, seed, i).
+ * kspir_client_decrypt: decrypt_bsgs_total (twosteps.cpp:388-418) of responses
+ *   [n][2][N] (coefficient form) under secrets [n][N] for a packing number r
+ *   (a power of two up to 4096): messages [n][N].  The reference's
+ *   QInv(r, crtMod) has no entry for r = 128 (it returns 0 there); this uses
+ *   r^-1 mod crtMod, the value of every entry it has. */
+int kspir_client_queries(kspir_ctx* ctx, int n, const uint64_t* secrets, const uint32_t* rows, uint64_t seed,
+                         uint64_t* queries);
+int kspir_client_decrypt(kspir_ctx* ctx, int n, const uint64_t* secrets, const uint64_t* responses, int r,
+                         uint64_t* messages);
+
 /* Copies the resident database (datacrt layout, r * N * N / 2 words) to host. */
 int kspir_db_download(kspir_ctx* ctx, uint64_t* datacrt, size_t words);
 

@@ -20,6 +20,7 @@
 #include "common.cuh"
 #include "gadget.cuh"
 #include "k_baby.cuh"
+#include "k_client.cuh"
 #include "k_db.cuh"
 #include "formats.cuh"
 #include "k_query.cuh"
@@ -104,6 +105,18 @@ uint32_t pow5(uint32_t e) { return (uint32_t)h_powmod(5, e, 2 * kN); }
 // and rot_{N-1-t} = -5^t mod 2N (utils.cpp:1473-1512, :1657-1675); perm[i] is
 // the slot permutation of X -> X^(5^i) (compute_permutation_matrix,
 // utils.cpp:1585-1619).
+// query_encode[t] (utils.cpp:1657-1675): brv((rot_t - 1) / 2), rot_t = 5^t mod 2N
+// for t < N/2 and rot_{N-1-t} = -5^t mod 2N
+std::vector<int32_t> query_encode_table() {
+    std::vector<int32_t> qe(kN);
+    for (uint32_t t = 0; t < (uint32_t)kN / 2; t++) {
+        const uint32_t rot = pow5(t);
+        qe[t] = (int32_t)h_bitrev12((rot - 1) / 2);
+        qe[kN - 1 - t] = (int32_t)h_bitrev12((2 * kN - rot - 1) / 2);
+    }
+    return qe;
+}
+
 std::vector<uint16_t> db_gather_table(int N1) {
     std::vector<uint16_t> inv_qe(kN), perm(kN), g((size_t)N1 * kN);
     for (uint32_t t = 0; t < (uint32_t)kN / 2; t++) {
@@ -198,6 +211,9 @@ struct kspir_ctx {
     uint64_t* prep_dev = nullptr;
     uint64_t* prep_host = nullptr;
     bool prep_rows_valid = false;
+    // client-side helpers: query_encode [N] int32, the message scaling table [p]
+    int32_t* cl_qenc = nullptr;
+    uint64_t* cl_dm = nullptr;
     uint8_t* dbop = nullptr;          // its database operand [N][2][G] tiles
     int G = 0;
     uint8_t* qop = nullptr;           // its query operand: launch at slot0 uses qop_at(slot0)
@@ -821,6 +837,8 @@ int kspir_ctx_create(int device, const kspir_params* params, kspir_ctx** out) {
     KS_CUDA(c.get(), cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device));
     KS_CUDA(c.get(), cudaFuncSetAttribute(k_baby_rot<3, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBabySmem));
     KS_CUDA(c.get(), cudaFuncSetAttribute(k_baby_pair<3, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBabyPairSmem));
+    KS_CUDA(c.get(), cudaFuncSetAttribute(k_client_query, cudaFuncAttributeMaxDynamicSharedMemorySize, kClientSmem));
+    KS_CUDA(c.get(), cudaFuncSetAttribute(k_client_decrypt, cudaFuncAttributeMaxDynamicSharedMemorySize, kClientSmem));
     KS_CUDA(c.get(), cudaFuncSetAttribute(k_db_rows<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kDbRowsSmem));
     KS_CUDA(c.get(), cudaFuncSetAttribute(k_db_rows<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kDbRowsSmem));
     KS_CUDA(c.get(), cudaFuncSetAttribute(k_ntt_jobs<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kNttJobSmem));
@@ -881,6 +899,8 @@ int kspir_ctx_destroy(kspir_ctx* c) {
     cudaFree(c->dbg);
     cudaFree(c->dbflag);
     cudaFree(c->prep_dev);
+    cudaFree(c->cl_qenc);
+    cudaFree(c->cl_dm);
     if (c->prep_host) cudaFreeHost(c->prep_host);
     cudaFree(c->dbop);
     cudaFree(c->qop);
@@ -1054,6 +1074,112 @@ int kspir_database_tocrt(kspir_ctx* c, const uint64_t* data_ntt, uint64_t* datac
     KS_COPY(c, h_in, d_crt, kSubWords * 8, cudaMemcpyDeviceToHost);
     memcpy(datacrt, h_in, kSubWords * 8);
     return KSPIR_OK;
+}
+
+// ---------------------------------------------------------------------------
+// client side (k_client.cuh)
+
+}  // extern "C"
+
+namespace {
+// a small secret word: s < B or s > crtMod - B, B = bsMod / 2 (the centred
+// lift into bsMod, guass_to_modulus, is then meaningful)
+bool small_secret(const uint64_t* s, size_t n) {
+    for (size_t i = 0; i < n; i++)
+        if (!(s[i] < kBsMod / 2 || (s[i] < kCrtMod && s[i] > kCrtMod - kBsMod / 2))) return false;
+    return true;
+}
+
+int ensure_client_tables(kspir_ctx* c) {
+    if (c->cl_dm) return KSPIR_OK;
+    const std::vector<int32_t> qe = query_encode_table();
+    // the reference's own expression, twosteps.cpp:303, as it compiles: a
+    // long double quotient (x87 on the host here too) through the C library's
+    // round(double)
+    std::vector<uint64_t> dm(kP);
+    for (uint64_t me = 0; me < kP; me++) dm[me] = (uint64_t)::round((double)((long double)me * kCrtMod / kP));
+    KS_CUDA(c, cudaMalloc(&c->cl_qenc, kN * 4));
+    KS_CUDA(c, cudaMalloc(&c->cl_dm, kP * 8));
+    KS_COPY(c, c->cl_qenc, qe.data(), kN * 4, cudaMemcpyHostToDevice);
+    KS_COPY(c, c->cl_dm, dm.data(), kP * 8, cudaMemcpyHostToDevice);
+    return KSPIR_OK;
+}
+
+// one device allocation carved into pieces (16-byte aligned)
+struct Carve {
+    uint8_t* base = nullptr;
+    size_t off = 0;
+    template <class T>
+    T* take(size_t count) {
+        T* p = reinterpret_cast<T*>(base + off);
+        off += (count * sizeof(T) + 255) & ~(size_t)255;
+        return p;
+    }
+};
+}  // namespace
+
+extern "C" {
+
+int kspir_client_queries(kspir_ctx* c, int n, const uint64_t* secrets, const uint32_t* rows, uint64_t seed,
+                         uint64_t* queries) {
+    if (!c || n < 1 || n > 65535 || !secrets || !rows || !queries) return KSPIR_ERR_INVALID_ARG;
+    for (int i = 0; i < n; i++)
+        if (rows[i] >= (uint32_t)kN / 2) return set_err(c, KSPIR_ERR_INVALID_ARG, "row must be below N/2");
+    if (!small_secret(secrets, (size_t)n * kN)) return set_err(c, KSPIR_ERR_INVALID_ARG, "secret words must be small");
+    std::lock_guard<std::mutex> lk(c->mu);
+    KS_CUDA(c, cudaSetDevice(c->device));
+    int rc = ensure_client_tables(c);
+    if (rc) return rc;
+    const size_t sw = (size_t)n * kN, qw = (size_t)n * 4 * kN, rw = (size_t)n * 6 * kN;
+    Carve cv;
+    KS_CUDA(c, cudaMalloc(&cv.base, sw * 8 + qw * 8 + rw * 4 + (size_t)n * 4 + 1024));
+    uint64_t* d_s = cv.take<uint64_t>(sw);
+    uint64_t* d_q = cv.take<uint64_t>(qw);
+    uint32_t* d_res = cv.take<uint32_t>(rw);
+    uint32_t* d_rows = cv.take<uint32_t>(n);
+    rc = copy_sync(c, d_s, secrets, sw * 8, cudaMemcpyHostToDevice);
+    if (!rc) rc = copy_sync(c, d_rows, rows, (size_t)n * 4, cudaMemcpyHostToDevice);
+    if (!rc) {
+        ClientQueryArgs qa{d_s, d_rows, c->cl_qenc, c->cl_dm, seed, d_res};
+        k_client_query<<<dim3(3, n), kNttThreads, kClientSmem, c->stream>>>(qa, c->ntabs);
+        k_client_query_words<<<blocks_for((long)n * 2 * kN, 256), 256, 0, c->stream>>>(d_res, d_q, n);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) rc = set_err(c, KSPIR_ERR_CUDA, std::string("client query: ") + cudaGetErrorString(e));
+    }
+    if (!rc) rc = copy_sync(c, queries, d_q, qw * 8, cudaMemcpyDeviceToHost);
+    cudaFree(cv.base);
+    return rc;
+}
+
+int kspir_client_decrypt(kspir_ctx* c, int n, const uint64_t* secrets, const uint64_t* responses, int r,
+                         uint64_t* messages) {
+    if (!c || n < 1 || n > 65535 || !secrets || !responses || !messages || r < 1 || r > 4096 || (r & (r - 1)))
+        return KSPIR_ERR_INVALID_ARG;
+    if (!canonical(secrets, (size_t)n * kN, kCrtMod) || !canonical(responses, (size_t)n * 2 * kN, kCrtMod))
+        return set_err(c, KSPIR_ERR_INVALID_ARG, "word not canonical");
+    std::lock_guard<std::mutex> lk(c->mu);
+    KS_CUDA(c, cudaSetDevice(c->device));
+    // QInv(r, crtMod) (utils.cpp:118-190) is r^-1 mod crtMod for every r of its
+    // table; it has no entry for 128 (and returns 0 there)
+    const uint64_t qinv = (uint64_t)h_invmod((uint64_t)r % kCrtMod, kCrtMod);
+    const size_t sw = (size_t)n * kN, rw = (size_t)n * 2 * kN;
+    Carve cv;
+    KS_CUDA(c, cudaMalloc(&cv.base, sw * 8 + rw * 8 + rw * 4 + sw * 8 + 1024));
+    uint64_t* d_s = cv.take<uint64_t>(sw);
+    uint64_t* d_r = cv.take<uint64_t>(rw);
+    uint32_t* d_res = cv.take<uint32_t>(rw);
+    uint64_t* d_m = cv.take<uint64_t>(sw);
+    int rc = copy_sync(c, d_s, secrets, sw * 8, cudaMemcpyHostToDevice);
+    if (!rc) rc = copy_sync(c, d_r, responses, rw * 8, cudaMemcpyHostToDevice);
+    if (!rc) {
+        k_client_decrypt<<<dim3(2, n), kNttThreads, kClientSmem, c->stream>>>(d_s, d_r, qinv, d_res, c->ntabs);
+        k_client_round<<<blocks_for((long)n * kN, 256), 256, 0, c->stream>>>(d_res, d_m, n);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) rc = set_err(c, KSPIR_ERR_CUDA, std::string("client decrypt: ") + cudaGetErrorString(e));
+    }
+    if (!rc) rc = copy_sync(c, messages, d_m, sw * 8, cudaMemcpyDeviceToHost);
+    cudaFree(cv.base);
+    return rc;
 }
 
 int kspir_db_download(kspir_ctx* c, uint64_t* datacrt, size_t words) {

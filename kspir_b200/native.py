@@ -54,6 +54,8 @@ SIGNATURES = {
     "kspir_response_unpack": (_i, [_vp, _sz, _vp]),
     "kspir_db_save": (_i, [_vp, ctypes.c_char_p]),
     "kspir_db_load": (_i, [_vp, ctypes.c_char_p]),
+    "kspir_client_queries": (_i, [_vp, _i, _vp, _vp, ctypes.c_uint64, _vp]),
+    "kspir_client_decrypt": (_i, [_vp, _i, _vp, _vp, _i, _vp]),
     "kspir_database_tobsgsntt": (_i, [_vp, _vp, _vp]),
     "kspir_database_tocrt": (_i, [_vp, _vp, _vp]),
     "kspir_perms_upload": (_i, [_vp, _vp, _sz]),
@@ -297,6 +299,26 @@ class Context:
         ms = ctypes.c_float(0.0)
         self._check(self.lib.kspir_db_preprocess_device(self._h, ctypes.c_void_p(d_raw), words, ctypes.byref(ms)))
         return ms.value
+
+    def client_queries(self, secrets, rows, seed: int) -> np.ndarray:
+        """query_bsgs_rns on the device for each (secret, row): [n][4N] words."""
+        sec = _u64(secrets).reshape(-1, N)
+        rw = np.ascontiguousarray(rows, dtype=np.uint32).reshape(-1)
+        if sec.shape[0] != rw.size:
+            raise ValueError("one secret per row")
+        out = np.empty((rw.size, 4 * N), dtype=np.uint64)
+        self._check(self.lib.kspir_client_queries(self._h, rw.size, ptr(sec), ptr(rw), seed, ptr(out)))
+        return out
+
+    def client_decrypt(self, secrets, responses, r: int) -> np.ndarray:
+        """decrypt_bsgs_total on the device: [n][N] message words."""
+        sec = _u64(secrets).reshape(-1, N)
+        rsp = _u64(responses).reshape(-1, 2 * N)
+        if sec.shape[0] != rsp.shape[0]:
+            raise ValueError("one secret per response")
+        out = np.empty((rsp.shape[0], N), dtype=np.uint64)
+        self._check(self.lib.kspir_client_decrypt(self._h, rsp.shape[0], ptr(sec), ptr(rsp), r, ptr(out)))
+        return out
 
     def database_tobsgsntt(self, data) -> np.ndarray:
         """Reference database_tobsgsntt of one sub-database on the device:

@@ -11,6 +11,7 @@
 #define _GNU_SOURCE
 #include "kspir_oracle.h"
 
+#include <math.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -529,6 +530,23 @@ void ko_database_tocrt(const uint64_t* rows, uint64_t* datacrt) {
             uint64_t t = rows[(size_t)R * N + z];
             datacrt[(size_t)z * H + R] = ko_barrett_coeff(t, 0) | ko_barrett_coeff(t, 1) << 32;
         }
+}
+
+/* The scaled message of query_bsgs_rns (twosteps.cpp:288-307) for row t:
+ * m[query_encode[t]] = m[query_encode[N-1-t]] = 1, INTT mod p, then
+ * round((long double)me * crtMod / p) as the reference compiles it: the
+ * unqualified round there is the C library's round(double), so the long
+ * double quotient is first rounded to a double (53-bit mantissa: the scaled
+ * words, below 2^56, land on multiples of 4 or 8), then to an integer. */
+void ko_query_message(int t, uint64_t* dm) {
+    int32_t* qe = malloc(sizeof(int32_t) * N);
+    query_encode(qe);
+    memset(dm, 0, 8 * N);
+    dm[qe[t]] = 1;
+    dm[qe[N - 1 - t]] = 1;
+    ko_ntt_inverse(dm, KO_P);
+    for (int i = 0; i < N; i++) dm[i] = (uint64_t)round((double)((long double)dm[i] * KO_CRTMOD / KO_P));
+    free(qe);
 }
 
 int ko_db_preprocess(const uint64_t* raw, int N1, uint64_t* datacrt) {

@@ -61,6 +61,9 @@ void ko_scan(const uint64_t* db, const uint64_t* cipherbuf, int N1, uint64_t* ou
  * database_tocrt (twosteps.cpp:42-179, crt.cpp:859-885).  raw [N][N/2] words
  * < p (else -1), datacrt [N][N/2]. */
 int ko_db_preprocess(const uint64_t* raw, int N1, uint64_t* datacrt);
+/* The scaled message of query_bsgs_rns for row t (twosteps.cpp:288-307): dm [N]. */
+void ko_query_message(int t, uint64_t* dm);
+
 /* The two steps apart: database_tobsgsntt (raw -> rows [N/2][N] mod crtMod,
  * -1 for a word >= p) and database_tocrt (rows -> datacrt [N][N/2]). */
 int ko_database_tobsgsntt(const uint64_t* raw, int N1, uint64_t* rows);

@@ -81,6 +81,7 @@ def lib():
             L.ko_db_preprocess.argtypes = [vp, ctypes.c_int, vp]
             L.ko_database_tobsgsntt.argtypes = [vp, ctypes.c_int, vp]
             L.ko_database_tocrt.argtypes = [vp, vp]
+            L.ko_query_message.argtypes = [ctypes.c_int, vp]
             _lib = L
     return _lib
 
@@ -119,6 +120,8 @@ def ref():
             L.ref_db_preprocess.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp]
             L.ref_database_tobsgsntt.argtypes = [vp, ctypes.c_int, vp]
             L.ref_database_tocrt.argtypes = [vp, ctypes.c_int, vp]
+            L.ref_pir_get_secret.argtypes = [vp]
+            L.ref_pir_decrypt_r.argtypes = [vp, ctypes.c_int, vp]
             _ref = L
     return _ref
 
@@ -247,6 +250,13 @@ def ref_database_tocrt(rows, N1=128):
     rows = np.ascontiguousarray(rows, dtype=np.uint64)
     out = np.empty(N * N // 2, dtype=np.uint64)
     ref().ref_database_tocrt(_p(rows), N1, _p(out))
+    return out
+
+
+def query_message(t: int) -> np.ndarray:
+    """The scaled message dm of query_bsgs_rns for row t (restatement)."""
+    out = np.empty(N, dtype=np.uint64)
+    lib().ko_query_message(t, _p(out))
     return out
 
 

@@ -184,6 +184,23 @@ int ref_pir_setup(uint32_t seed, int r, int N1) {
     return 0;
 }
 
+// The test-pir secret in coefficient form mod crtMod (Secret::data).
+void ref_pir_get_secret(uint64_t* s) {
+    if (g_state.key->isNttForm()) g_state.key->toCoeffForm();
+    std::vector<uint64_t> d = g_state.key->getData();
+    memcpy(s, d.data(), kPoly * 8);
+}
+
+// decrypt_bsgs_total (twosteps.cpp:388-418) of a coefficient-form response
+// under the test-pir secret with packing number r.
+void ref_pir_decrypt_r(const uint64_t* response, int r, uint64_t* message) {
+    RlweCiphertext c(N, crtMod);
+    load_rlwe(c, response, false);
+    std::vector<uint64_t> m(N);
+    decrypt_bsgs_total(m, c, *g_state.key, r);
+    memcpy(message, m.data(), kPoly * 8);
+}
+
 // Keep (1) the sampled database of the next ref_pir_setup before preprocessing.
 void ref_pir_keep_raw(int keep) { g_keep_raw = keep != 0; }
 
