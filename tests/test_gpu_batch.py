@@ -126,3 +126,20 @@ def test_batch_rejects_bad_input():
         # the context still answers afterwards
         got = ctx.answer_batch(np.zeros(2, np.int32), q)
         assert (got[1] == po.answer(db, r, N1, dict(clients[0], query=q[1]))).all()
+
+
+@pytest.mark.parametrize("r,N1", [(1, 64), (4, 256), (2, 64)])
+def test_batch_other_shapes_match_oracle(r, N1):
+    # N1 != 128 batches run the CUDA-core scan (the tensor-core scan needs
+    # N1 = 128) with the batched baby-step shape; r = 1 has no packing level
+    n = 3
+    db = po.gen_db(170 + r + N1, r, N1)
+    clients = [po.gen_client(171 + i + N1, r, N1) for i in range(2)]
+    cl = np.array([0, 1, 0], dtype=np.int32)
+    queries = random_queries(13 + N1, n)
+    with make_ctx(r, N1, db, clients, max_inflight=4) as ctx:
+        got = ctx.answer_batch(cl, queries)
+        for i in range(n):
+            want = po.answer(db, r, N1, dict(clients[cl[i]], query=queries[i]))
+            assert (got[i] == want).all(), f"query {i}"
+            assert (ctx.answer(int(cl[i]), queries[i]) == want).all()
