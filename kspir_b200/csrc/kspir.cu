@@ -232,6 +232,7 @@ struct kspir_ctx {
     uint64_t* bq64 = nullptr;         // [slots][4][N] query words
     uint64_t* bresp = nullptr;        // [slots][2][N] response words
     int* errs = nullptr;              // [slots][kErrStride]
+    int* errs_host = nullptr;         // pinned copy read back by finish()
     int* client_of = nullptr;         // [slots]
     uint32_t* stage32 = nullptr;      // [r][4][N] residues for the staged entry points
     NttJob* jobs = nullptr;           // transform job lists of slot 0
@@ -450,6 +451,7 @@ int init_workspaces(kspir_ctx* c) {
     KS_CUDA(c, cudaMalloc(&c->bresp, (size_t)S * 2 * kN * 8));
     KS_CUDA(c, cudaMalloc(&c->errs, (size_t)S * kErrStride * 4));
     KS_CUDA(c, cudaMemsetAsync(c->errs, 0, (size_t)S * kErrStride * 4, c->stream));
+    KS_CUDA(c, cudaHostAlloc(&c->errs_host, (size_t)S * kErrStride * 4, cudaHostAllocDefault));
     KS_CUDA(c, cudaMalloc(&c->client_of, (size_t)S * 4));
     KS_CUDA(c, cudaMemsetAsync(c->client_of, 0, (size_t)S * 4, c->stream));
     KS_CUDA(c, cudaMalloc(&c->stage32, (size_t)r * 4 * P));
@@ -758,14 +760,18 @@ int check_ready(kspir_ctx* c, int client) {
 
 // Waits for the context stream and reports (then clears) the error words of
 // slots [slot0, slot0 + nq).
+// Waits for the work enqueued on the context stream and collects the error
+// words of slots [slot0, slot0 + nq) with it (one synchronisation).
 int finish(kspir_ctx* c, int slot0, int nq) {
+    const size_t bytes = (size_t)nq * kErrStride * 4;
+    KS_CUDA(c, cudaMemcpyAsync(c->errs_host + (size_t)slot0 * kErrStride, c->errs + (size_t)slot0 * kErrStride, bytes,
+                               cudaMemcpyDeviceToHost, c->stream));
     KS_CUDA(c, cudaStreamSynchronize(c->stream));
-    std::vector<int> e((size_t)nq * kErrStride);
-    KS_COPY(c, e.data(), c->errs + (size_t)slot0 * kErrStride, e.size() * 4, cudaMemcpyDeviceToHost);
+    const int* e = c->errs_host + (size_t)slot0 * kErrStride;
     int herr = 0;
     for (int q = 0; q < nq; q++) herr |= e[(size_t)q * kErrStride];
     if (herr) {
-        cudaMemsetAsync(c->errs + (size_t)slot0 * kErrStride, 0, e.size() * 4, c->stream);
+        cudaMemsetAsync(c->errs + (size_t)slot0 * kErrStride, 0, bytes, c->stream);
         cudaStreamSynchronize(c->stream);
         return set_err(c, KSPIR_ERR_TIMEOUT, "a bounded device wait gave up (code " + std::to_string(herr) + ")");
     }
@@ -892,6 +898,7 @@ int kspir_ctx_destroy(kspir_ctx* c) {
     cudaFree(c->bq64);
     cudaFree(c->bresp);
     cudaFree(c->errs);
+    if (c->errs_host) cudaFreeHost(c->errs_host);
     cudaFree(c->client_of);
     cudaFree(c->stage32);
     cudaFree(c->key_mem);
