@@ -22,6 +22,7 @@
 
 #include "ntt.cuh"
 #include "pipeline.cuh"
+#include "ptx.cuh"
 
 namespace kspir {
 
@@ -121,7 +122,7 @@ __device__ __forceinline__ void baby_bs_part(const BabyRot& R, const BabyArgs& a
             const uint32_t* kk = R.kbs + (size_t)(j * 2 + R.comp) * kN;
 #pragma unroll
             for (int it = 0; it < kPerThread; it++)
-                acc[it] += (uint64_t)__ldg(d + pk[it]) * __ldg(kk + tid + it * kNttThreads);
+                acc[it] += (uint64_t)__ldcg(d + pk[it]) * __ldg(kk + tid + it * kNttThreads);
         }
 #pragma unroll
         for (int it = 0; it < kPerThread; it++)
@@ -139,7 +140,7 @@ __device__ __forceinline__ void baby_bs_part(const BabyRot& R, const BabyArgs& a
             const int pk2 = pidx(tid) + it * kPadStep;
             bool neg;
             const int src = auto_src(k, ginv, &neg);
-            uint32_t v = __ldg(shifted(a.srcBbs, R.wo) + src);
+            uint32_t v = __ldcg(shifted(a.srcBbs, R.wo) + src);
             if (neg) v = negmod(v, qb);
             S[pk2] = addmod(S[pk2], v, qb);
         }
@@ -179,13 +180,13 @@ __device__ __forceinline__ void baby_crt_part(const BabyRot& R, const BabyArgs& 
         const uint32_t* kk = R.kcrt + (size_t)((j * 2 + comp) * 2 + ch) * kN;
 #pragma unroll
         for (int it = 0; it < kPerThread; it++)
-            acc[it] += (uint64_t)__ldg(d + pk[it]) * __ldg(kk + tid + it * kNttThreads);
+            acc[it] += (uint64_t)__ldcg(d + pk[it]) * __ldg(kk + tid + it * kNttThreads);
     }
 #pragma unroll
     for (int it = 0; it < kPerThread; it++) {
         const int k = tid + it * kNttThreads;
         uint32_t A = negmod(mod_crt(acc[it], ch), cc.q);
-        if (comp == 1) A = addmod(A, __ldg(shifted(a.srcB, R.wo) + ch * kN + sig[k]), cc.q);
+        if (comp == 1) A = addmod(A, __ldcg(shifted(a.srcB, R.wo) + ch * kN + sig[k]), cc.q);
         if (R.inter) inter_out[ch * kN + k] = A;
         const uint32_t r = shoup_mul(submod(A, S[pidx(tid) + it * kPadStep], cc.q), cc.bsinv, cc.bsinv_p, cc.q);
         if (a.cb_rm)
@@ -207,8 +208,10 @@ __global__ void __launch_bounds__(kNttThreads, MINB) k_baby_rot(BabyArgs a, Clie
     uint32_t* S = reinterpret_cast<uint32_t*>(smem_raw + kN * 8);
     const int ch = blockIdx.x & 1;
     BabyRot R;
+    pdl_launch_dependents();
     stage_twiddles(tws, tabs, CH_BS, NTT_INV);
     baby_setup<ELL>(R, a, keys, bt, blockIdx.x >> 2, (blockIdx.x >> 1) & 1);
+    pdl_wait();   // the digits come from the previous kernel
     baby_bs_part<ELL>(R, a, S, tws, ch == 0);
     baby_crt_part<ELL>(R, a, S, tws, tabs, ch);
 }
@@ -226,8 +229,10 @@ __global__ void __launch_bounds__(kNttThreads, MINB) k_baby_pair(BabyArgs a, Cli
     uint32_t* S = reinterpret_cast<uint32_t*>(smem_raw + kN * 8);
     uint32_t* S2 = S + kPadN;
     BabyRot R;
+    pdl_launch_dependents();
     stage_twiddles(tws, tabs, CH_BS, NTT_INV);
     baby_setup<ELL>(R, a, keys, bt, blockIdx.x >> 1, blockIdx.x & 1);
+    pdl_wait();   // the digits come from the previous kernel
     baby_bs_part<ELL>(R, a, S, tws, true);
     // the second prime transforms its own copy of x2 (each thread copies the
     // coefficients it wrote: no barrier needed)

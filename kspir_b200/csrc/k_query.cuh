@@ -2,6 +2,7 @@
 #pragma once
 
 #include "pipeline.cuh"
+#include "ptx.cuh"
 
 namespace kspir {
 
@@ -13,6 +14,8 @@ namespace kspir {
 //  * the RNS modswitch of the query itself, (x_crt - x_bs) * bsMod^-1 mod
 //    crtMod (twosteps.cpp:1073-1086), as residues before its transform.
 __global__ void k_query_prep(Workspace ws, GadgetBsgs g, Batch bt) {
+    pdl_launch_dependents();
+    pdl_wait();
     ws = ws_at(ws, bt);
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= kN) return;
@@ -42,11 +45,13 @@ __global__ void k_query_prep(Workspace ws, GadgetBsgs g, Batch bt) {
 // decompose_bsgs of its coefficient-form a (crt residues composed to the
 // canonical word) and its bsMod part.
 __global__ void k_inter_decomp(Workspace ws, GadgetBsgs g, Batch bt) {
+    pdl_launch_dependents();
+    pdl_wait();
     ws = ws_at(ws, bt);
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= kN) return;
-    const uint64_t a_crt = crt_compose_res(ws.inter_acoef[k], ws.inter_acoef[kN + k]);
-    const uint32_t a_bs = ws.inter_bs[k];
+    const uint64_t a_crt = crt_compose_res(__ldcg(ws.inter_acoef + k), __ldcg(ws.inter_acoef + kN + k));
+    const uint32_t a_bs = __ldcg(ws.inter_bs + k);
     int32_t dig[kMaxEll];
     decompose_bsgs(a_crt, a_bs, g, dig);
     for (int j = 0; j < g.ell; j++) {

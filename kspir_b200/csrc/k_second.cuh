@@ -12,6 +12,7 @@
 
 #include "ntt.cuh"
 #include "pipeline.cuh"
+#include "ptx.cuh"
 
 namespace kspir {
 
@@ -110,15 +111,17 @@ __global__ void __launch_bounds__(kNttThreads) k_giant_fused(uint32_t* sout, con
     const int tid = threadIdx.x;
     sout = shifted(sout, ws_off(bt));
     gkeys = shifted(gkeys, key_off(bt));
+    pdl_launch_dependents();
 
     // a of output[c], both primes, to coefficient form
 #pragma unroll
     for (int ch = 0; ch < 2; ch++) {
         stage_twiddles(tws, tabs, ch, NTT_INV);
+        pdl_wait();   // the scan output comes from the previous kernel
 #pragma unroll
         for (int k = tid; k < kN / 4; k += kNttThreads)
             *reinterpret_cast<uint4*>(P + ch * kPadN + pidx(4 * k)) =
-                *reinterpret_cast<const uint4*>(sout + sout_idx(row, 0 * 2 + ch, 4 * k, rows));
+                __ldcg(reinterpret_cast<const uint4*>(sout + sout_idx(row, 0 * 2 + ch, 4 * k, rows)));
         cta_ntt_inverse(P + ch * kPadN, tws, ch);
     }
     // X -> X^g, g = 5^(N1 c), then the digits (registers first: P is overwritten)
@@ -168,7 +171,7 @@ __global__ void __launch_bounds__(kNttThreads) k_giant_fused(uint32_t* sout, con
                 mad_wide(sa, d, __ldg(key + ((j * 2 + 0) * 2 + ch) * kN + k));
                 mad_wide(sb, d, __ldg(key + ((j * 2 + 1) * 2 + ch) * kN + k));
             }
-            const uint32_t bv = sout[sout_idx(row, 1 * 2 + ch, sig[k], rows)];
+            const uint32_t bv = __ldcg(sout + sout_idx(row, 1 * 2 + ch, sig[k], rows));
             cbv[it] = addmod(bv, negmod(mod_crt(sb, ch), cc.q), cc.q);
             sout[sout_idx(row, 0 * 2 + ch, k, rows)] = negmod(mod_crt(sa, ch), cc.q);
         }
@@ -182,6 +185,8 @@ __global__ void __launch_bounds__(kNttThreads) k_giant_fused(uint32_t* sout, con
 // mod q: the sum of the N2 rows of sub-database r after k_giant_fused.
 __global__ void k_giant_finish(const uint32_t* __restrict__ sout, uint32_t* __restrict__ result, int R, int N2,
                                Batch bt) {
+    pdl_launch_dependents();
+    pdl_wait();
     const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= (long)R * 4 * kN) return;
     sout = shifted(sout, ws_off(bt));
@@ -191,7 +196,7 @@ __global__ void k_giant_finish(const uint32_t* __restrict__ sout, uint32_t* __re
     const int r = (int)(idx / (4 * kN));
     const ChanConst q = c_dev.ch[cc_ & 1];
     uint64_t v = 0;
-    for (int c = 0; c < N2; c++) v += sout[sout_idx(r * N2 + c, cc_, k, R * N2)];
+    for (int c = 0; c < N2; c++) v += __ldcg(sout + sout_idx(r * N2 + c, cc_, k, R * N2));
     result[idx] = reduce64(v, q.q, q.barrett);
 }
 
@@ -228,12 +233,14 @@ __global__ void __launch_bounds__(kNttThreads) k_pack_fused(const uint32_t* __re
     const uint32_t* r0 = in + (size_t)j * 4 * kN;
     const uint32_t* cc = in + (size_t)(I + j) * 4 * kN;
     const uint32_t q = c_dev.ch[ch].q;
+    pdl_launch_dependents();
     stage_twiddles(tws, tabs, ch, NTT_FWD);
+    pdl_wait();   // the level input comes from the previous kernel
     // X^I c at position p of polynomial (comp, prime)
     auto cshift = [&](int comp, int pch, int p) -> uint32_t {
         const int s = p - I;
         const uint32_t qq = pch ? kQ2 : kQ1;
-        return s >= 0 ? __ldg(cc + (comp * 2 + pch) * kN + s) : negmod(__ldg(cc + (comp * 2 + pch) * kN + s + kN), qq);
+        return s >= 0 ? __ldcg(cc + (comp * 2 + pch) * kN + s) : negmod(__ldcg(cc + (comp * 2 + pch) * kN + s + kN), qq);
     };
     uint32_t c2v[kPerThreadG][2];
 #pragma unroll
@@ -241,14 +248,14 @@ __global__ void __launch_bounds__(kNttThreads) k_pack_fused(const uint32_t* __re
         const int k = tid + it * kNttThreads;
 #pragma unroll
         for (int comp = 0; comp < 2; comp++)
-            c2v[it][comp] = addmod(cshift(comp, ch, k), __ldg(r0 + (comp * 2 + ch) * kN + k), q);
+            c2v[it][comp] = addmod(cshift(comp, ch, k), __ldcg(r0 + (comp * 2 + ch) * kN + k), q);
         bool neg;
         const int src = auto_src(k, ginv, &neg);
         uint32_t ra[2];
 #pragma unroll
         for (int pch = 0; pch < 2; pch++) {
             const uint32_t qq = pch ? kQ2 : kQ1;
-            const uint32_t v = submod(__ldg(r0 + (0 * 2 + pch) * kN + src), cshift(0, pch, src), qq);
+            const uint32_t v = submod(__ldcg(r0 + (0 * 2 + pch) * kN + src), cshift(0, pch, src), qq);
             ra[pch] = neg ? negmod(v, qq) : v;
         }
         int32_t dig[kMaxEll];
@@ -256,7 +263,7 @@ __global__ void __launch_bounds__(kNttThreads) k_pack_fused(const uint32_t* __re
         const int pk = pidx(tid) + it * kPadStep;
 #pragma unroll
         for (int d = 0; d < ELL; d++) P[d * kPadN + pk] = signed_to_res(dig[d], q);
-        const uint32_t vb = submod(__ldg(r0 + (1 * 2 + ch) * kN + src), cshift(1, ch, src), q);
+        const uint32_t vb = submod(__ldcg(r0 + (1 * 2 + ch) * kN + src), cshift(1, ch, src), q);
         P[ELL * kPadN + pk] = neg ? negmod(vb, q) : vb;
     }
     cta_ntt_forward_m<ELL + 1>(P, kPadN, tws, ch);
@@ -318,11 +325,13 @@ __global__ void __launch_bounds__(kNttThreads) k_pack_split_fwd(const uint32_t* 
     const uint32_t* r0 = in + (size_t)j * 4 * kN;
     const uint32_t* cc = in + (size_t)(I + j) * 4 * kN;
     const uint32_t q = c_dev.ch[ch].q;
+    pdl_launch_dependents();
     stage_twiddles(tws, tabs, ch, NTT_FWD);
+    pdl_wait();   // the level input comes from the previous kernel
     auto cshift = [&](int comp, int pch, int p) -> uint32_t {   // (X^I c)[p]
         const int s = p - I;
         const uint32_t qq = pch ? kQ2 : kQ1;
-        return s >= 0 ? __ldg(cc + (comp * 2 + pch) * kN + s) : negmod(__ldg(cc + (comp * 2 + pch) * kN + s + kN), qq);
+        return s >= 0 ? __ldcg(cc + (comp * 2 + pch) * kN + s) : negmod(__ldcg(cc + (comp * 2 + pch) * kN + s + kN), qq);
     };
 #pragma unroll
     for (int it = 0; it < kPerThreadG; it++) {
@@ -335,14 +344,14 @@ __global__ void __launch_bounds__(kNttThreads) k_pack_split_fwd(const uint32_t* 
 #pragma unroll
             for (int pch = 0; pch < 2; pch++) {
                 const uint32_t qq = pch ? kQ2 : kQ1;
-                const uint32_t x = submod(__ldg(r0 + (0 * 2 + pch) * kN + src), cshift(0, pch, src), qq);
+                const uint32_t x = submod(__ldcg(r0 + (0 * 2 + pch) * kN + src), cshift(0, pch, src), qq);
                 ra[pch] = neg ? negmod(x, qq) : x;
             }
             int32_t dig[kMaxEll];
             decompose_b(crt_compose_res(ra[0], ra[1]), kCrtMod, g, dig);
             v = signed_to_res(dig[d], q);
         } else {
-            const uint32_t vb = submod(__ldg(r0 + (1 * 2 + ch) * kN + src), cshift(1, ch, src), q);
+            const uint32_t vb = submod(__ldcg(r0 + (1 * 2 + ch) * kN + src), cshift(1, ch, src), q);
             v = neg ? negmod(vb, q) : vb;
         }
         S[pidx(tid) + it * kPadStep] = v;
@@ -376,16 +385,18 @@ __global__ void __launch_bounds__(kNttThreads) k_pack_split_inv(const uint32_t* 
     const int comp = blockIdx.x & 1, ch = (blockIdx.x >> 1) & 1, j = blockIdx.x >> 2;
     const int tid = threadIdx.x;
     const uint32_t q = c_dev.ch[ch].q;
+    pdl_launch_dependents();
     stage_twiddles(tws, tabs, ch, NTT_INV);
+    pdl_wait();   // the terms come from the previous kernel
     const uint32_t* pj = part + ((size_t)j * 2 + ch) * (ELL + 1) * 2 * kN;
 #pragma unroll
     for (int it = 0; it < kPerThreadG; it++) {
         const int k = tid + it * kNttThreads;
         uint32_t sum = 0;
 #pragma unroll
-        for (int d = 0; d < ELL; d++) sum = addmod(sum, __ldg(pj + ((size_t)d * 2 + comp) * kN + k), q);
+        for (int d = 0; d < ELL; d++) sum = addmod(sum, __ldcg(pj + ((size_t)d * 2 + comp) * kN + k), q);
         // a' = -sum_d dig_d key[d].a ;  b' = NTT(temp.b) - sum_d dig_d key[d].b
-        S[pidx(tid) + it * kPadStep] = comp == 0 ? negmod(sum, q) : submod(__ldg(pj + (size_t)ELL * 2 * kN + k), sum, q);
+        S[pidx(tid) + it * kPadStep] = comp == 0 ? negmod(sum, q) : submod(__ldcg(pj + (size_t)ELL * 2 * kN + k), sum, q);
     }
     cta_ntt_inverse(S, tws, ch);
     const uint32_t* r0 = in + (size_t)j * 4 * kN;
@@ -394,8 +405,8 @@ __global__ void __launch_bounds__(kNttThreads) k_pack_split_inv(const uint32_t* 
     for (int it = 0; it < kPerThreadG; it++) {
         const int k = tid + it * kNttThreads;
         const int s = k - I;
-        const uint32_t sh = s >= 0 ? __ldg(cc + s) : negmod(__ldg(cc + s + kN), q);
-        const uint32_t c2 = addmod(sh, __ldg(r0 + (comp * 2 + ch) * kN + k), q);
+        const uint32_t sh = s >= 0 ? __ldcg(cc + s) : negmod(__ldcg(cc + s + kN), q);
+        const uint32_t c2 = addmod(sh, __ldcg(r0 + (comp * 2 + ch) * kN + k), q);
         out[((size_t)j * 4 + comp * 2 + ch) * kN + k] = addmod(S[pidx(tid) + it * kPadStep], c2, q);
     }
 }
@@ -427,11 +438,13 @@ __global__ void __launch_bounds__(kNttThreads) k_ext_fused(const uint32_t* __res
     const int r = blockIdx.x >> 1, ch = blockIdx.x & 1;
     const int tid = threadIdx.x;
     const uint32_t* fd = first_dim + (size_t)r * 4 * kN;          // [comp][prime][N]
+    pdl_launch_dependents();
     // first_dim to coefficient form, all four polynomials (P[comp * 2 + prime])
 #pragma unroll
     for (int pch = 0; pch < 2; pch++) {
         if (pch) __syncthreads();
         stage_twiddles(tws, tabs, pch, NTT_INV);
+        pdl_wait();   // the first-dimension results come from the previous kernel
 #pragma unroll
         for (int comp = 0; comp < 2; comp++) {
             poly_to_smem(P + (comp * 2 + pch) * kPadN, fd + (comp * 2 + pch) * kN);
@@ -475,7 +488,7 @@ __global__ void __launch_bounds__(kNttThreads) k_ext_fused(const uint32_t* __res
             for (int row = 0; row < 2 * ELL; row++)
                 mad_wide(s, P[row * kPadN + pidx(tid) + it * kPadStep], __ldg(rgsw + ((row * 2 + comp) * 2 + ch) * kN + k));
             const uint32_t m = mod_crt(s, ch);
-            outv[it][comp] = init ? addmod(__ldg(init + ((size_t)r * 4 + comp * 2 + ch) * kN + k), m, cq.q) : m;
+            outv[it][comp] = init ? addmod(__ldcg(init + ((size_t)r * 4 + comp * 2 + ch) * kN + k), m, cq.q) : m;
         }
     }
 #pragma unroll

@@ -5,6 +5,7 @@
 #include "common.cuh"
 #include "ntt.cuh"
 #include "pipeline.cuh"
+#include "ptx.cuh"
 
 namespace kspir {
 
@@ -25,10 +26,12 @@ __global__ void __launch_bounds__(kNttThreads) k_ntt_jobs(const NttJob* __restri
     extern __shared__ __align__(16) uint8_t smem_raw[];
     uint2* tws = reinterpret_cast<uint2*>(smem_raw);
     uint32_t* s = reinterpret_cast<uint32_t*>(smem_raw + kN * 8);
+    pdl_launch_dependents();
     NttJob jb = jobs[blockIdx.x];
     jb.src = shifted(jb.src, ws_off(bt));   // job lists address workspace slot 0
     jb.dst = shifted(jb.dst, ws_off(bt));
     stage_twiddles(tws, tabs, jb.ch, INVERSE ? NTT_INV : NTT_FWD);
+    pdl_wait();
     poly_to_smem(s, jb.src);
     if (INVERSE) cta_ntt_inverse(s, tws, jb.ch);
     else cta_ntt_forward(s, tws, jb.ch);
@@ -52,11 +55,13 @@ __global__ void k_compose_words(const uint32_t* __restrict__ res, uint64_t* __re
 // Response words of every query of a batch: resp64 of its slot = canonical
 // words of the two residue polynomials `res` (a workspace pointer of slot 0).
 __global__ void k_compose_resp(const uint32_t* __restrict__ res, Workspace w, Batch bt) {
+    pdl_launch_dependents();
+    pdl_wait();
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= 2 * kN) return;
     const uint32_t* r = shifted(res, ws_off(bt)) + (size_t)(idx / kN) * 2 * kN;
     const int k = idx % kN;
-    w.resp64[(size_t)batch_slot(bt) * 2 * kN + idx] = crt_compose_res(r[k], r[kN + k]);
+    w.resp64[(size_t)batch_slot(bt) * 2 * kN + idx] = crt_compose_res(__ldcg(r + k), __ldcg(r + kN + k));
 }
 
 // res[p][ch][k] = words[p][k] mod q_ch (ch = q1, q2) for `polys` polynomials.

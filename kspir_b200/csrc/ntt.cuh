@@ -226,11 +226,14 @@ __device__ __forceinline__ void cta_ntt_inverse(uint32_t* s, const uint2* tws, i
 }
 
 // Copies of whole polynomials between global memory (natural order) and a
-// padded shared-memory polynomial; 16-byte vectors.
+// padded shared-memory polynomial; 16-byte vectors.  The loads bypass L1
+// (ld.global.cg): the source is usually the previous kernel's output, and a
+// kernel started early by programmatic dependent launch must not hit lines
+// an overlapping kernel left in L1.
 __device__ __forceinline__ void poly_to_smem(uint32_t* s, const uint32_t* __restrict__ g) {
     const uint4* g4 = reinterpret_cast<const uint4*>(g);
 #pragma unroll
-    for (int k = threadIdx.x; k < kN / 4; k += kNttThreads) *reinterpret_cast<uint4*>(s + pidx(4 * k)) = __ldg(g4 + k);
+    for (int k = threadIdx.x; k < kN / 4; k += kNttThreads) *reinterpret_cast<uint4*>(s + pidx(4 * k)) = __ldcg(g4 + k);
 }
 __device__ __forceinline__ void poly_from_smem(uint32_t* __restrict__ g, const uint32_t* s) {
     uint4* g4 = reinterpret_cast<uint4*>(g);

@@ -69,4 +69,19 @@ __device__ __forceinline__ void bulk_g2s(void* dst_smem, const void* src_gmem, u
         : "memory");
 }
 
+// Programmatic dependent launch (sm_90+).  A kernel launched with the
+// programmatic-serialization attribute may start while the previous kernel in
+// its stream still runs: it does its independent prologue (staging
+// twiddles), then pdl_wait() blocks until the previous grid has completed and
+// its memory is visible.  Every kernel of such a chain calls pdl_wait(), so
+// completion stays transitive.  Data written inside a chain is read with
+// ld.global.cg (L2, not L1): the kernel's CTAs were launched -- and the SM's
+// L1 invalidated -- before the previous kernel finished, so an L1 line that
+// kernel loaded and then overwrote could otherwise be read stale (measured:
+// the in-place transforms of k_ntt_jobs read back by the baby steps).  pdl_launch_dependents() lets the next grid
+// start launching once every CTA of this one has issued it.  Both are no-ops
+// for kernels launched without the attribute.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 }  // namespace kspir
