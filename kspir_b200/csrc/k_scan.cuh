@@ -84,6 +84,7 @@ __global__ void __launch_bounds__(ScanCfg<N1>::THREADS, 1)
     if (warp == C::CONS) {
         // producer
         if (lane == 0) {
+            const uint64_t pol_db = l2_policy_evict_first(), pol_cb = l2_policy_evict_last();
             long issued = 0;
             for (long j = 0; j < nloc; j++) {
                 const int s = (int)(j % C::NST);
@@ -98,8 +99,10 @@ __global__ void __launch_bounds__(ScanCfg<N1>::THREADS, 1)
                 const long r = it / kN, z = it % kN;
                 uint8_t* st = smem + (size_t)s * C::STAGE;
                 mbar_arrive_expect_tx(&full[s], C::STAGE);
-                bulk_g2s(st, db + ((size_t)r * kN + z) * (kN / 2), C::SLAB, &full[s]);
-                bulk_g2s(st + C::SLAB, cbuf + (size_t)z * 2 * N1, C::QSLAB, &full[s]);
+                // the database streams through L2 once (evict first); the 8 MiB
+                // cipherbuf is read again for every sub-database (evict last)
+                bulk_g2s_hint(st, db + ((size_t)r * kN + z) * (kN / 2), C::SLAB, &full[s], pol_db);
+                bulk_g2s_hint(st + C::SLAB, cbuf + (size_t)z * 2 * N1, C::QSLAB, &full[s], pol_cb);
                 issued = j + 1;
             }
             // never leave the CTA with copies in flight into its shared memory
