@@ -1580,14 +1580,18 @@ int kspir_answer(kspir_ctx* c, int client, const uint64_t* query, uint64_t* resp
     int rc = check_ready(c, client);
     if (rc) return rc;
     if (!query || !response) return KSPIR_ERR_INVALID_ARG;
-    if (!canonical(query, 2 * kN, kCrtMod) || !canonical(query + 2 * kN, 2 * kN, kBsMod))
-        return set_err(c, KSPIR_ERR_INVALID_ARG, "query word not canonical");
     std::lock_guard<std::mutex> lk(c->mu);
     KS_CUDA(c, cudaSetDevice(c->device));
     KS_CUDA(c, cudaMemcpyAsync(c->bq64, query, 4 * kN * 8, cudaMemcpyHostToDevice, c->stream));
     rc = enqueue_answer(c, 0, 1, &client, c->stream);
     if (rc) return rc;
     KS_CUDA(c, cudaGetLastError());
+    // the query is validated while the device answers it; a non-canonical one
+    // is reported before anything reaches the caller's response buffer
+    if (!canonical(query, 2 * kN, kCrtMod) || !canonical(query + 2 * kN, 2 * kN, kBsMod)) {
+        KS_CUDA(c, cudaStreamSynchronize(c->stream));
+        return set_err(c, KSPIR_ERR_INVALID_ARG, "query word not canonical");
+    }
     KS_CUDA(c, cudaMemcpyAsync(response, c->bresp, 2 * kN * 8, cudaMemcpyDeviceToHost, c->stream));
     return finish(c, 0, 1);
 }
