@@ -1620,18 +1620,23 @@ int kspir_answer_batch(kspir_ctx* c, int n, const int32_t* clients, const uint64
     if (rc) return rc;
     if (n < 1 || n > c->p.max_inflight || n > kMaxBatch || !clients || !queries || !responses)
         return set_err(c, KSPIR_ERR_INVALID_ARG, "batch size out of range or null pointer");
-    for (int i = 0; i < n; i++) {
+    for (int i = 0; i < n; i++)
         if ((rc = check_client(c, clients[i]))) return rc;
-        const uint64_t* q = queries + (size_t)i * 4 * kN;
-        if (!canonical(q, 2 * kN, kCrtMod) || !canonical(q + 2 * kN, 2 * kN, kBsMod))
-            return set_err(c, KSPIR_ERR_INVALID_ARG, "query word not canonical");
-    }
     std::lock_guard<std::mutex> lk(c->mu);
     KS_CUDA(c, cudaSetDevice(c->device));
     KS_CUDA(c, cudaMemcpyAsync(c->bq64, queries, (size_t)n * 4 * kN * 8, cudaMemcpyHostToDevice, c->stream));
     rc = enqueue_answer(c, 0, n, clients, c->stream);
     if (rc) return rc;
     KS_CUDA(c, cudaGetLastError());
+    // the queries are validated while the device answers them; a
+    // non-canonical word is reported before anything reaches `responses`
+    for (int i = 0; i < n; i++) {
+        const uint64_t* q = queries + (size_t)i * 4 * kN;
+        if (!canonical(q, 2 * kN, kCrtMod) || !canonical(q + 2 * kN, 2 * kN, kBsMod)) {
+            KS_CUDA(c, cudaStreamSynchronize(c->stream));
+            return set_err(c, KSPIR_ERR_INVALID_ARG, "query word not canonical");
+        }
+    }
     KS_CUDA(c, cudaMemcpyAsync(responses, c->bresp, (size_t)n * 2 * kN * 8, cudaMemcpyDeviceToHost, c->stream));
     return finish(c, 0, n);
 }
