@@ -379,6 +379,10 @@ def run_gpu(args, rank, world, local_rank):
                          "algorithmic_bytes_per_launch": db_bytes, "traffic": read_traffic(r)},
             "e2e": {"value": world * args.steps / e2e_s, "unit": "queries/s",
                     "h2d_bytes_per_step": 4 * N * 8, "d2h_bytes_per_step": 2 * N * 8},
+            # the whole answer against the bytes it must touch: the database,
+            # one client's keys and the 8 MiB rotated-query buffer
+            "answer_gbs": (db_bytes + ctx.lib.kspir_client_key_bytes(ctx.handle) + N * N1 * 2 * 8)
+                          / (ms / args.steps * 1e-3) / 1e9,
             "gpu_launches": int(launches) * world,
             "clocks": clocks.summary(),
         }
@@ -392,6 +396,10 @@ def run_gpu(args, rank, world, local_rank):
             out["cpu_baseline"] = {"value": rate, "unit": "queries/s", "cores": th, "kind": kind,
                                    "sample": f"{n} full answers (r={r}, N1={N1}) in ~{args.cpu_seconds:.0f} s, "
                                              f"one independent query per thread"}
+            # the reference's path is single-threaded: its latency on one core
+            rate1, kind1, n1, _ = cpu_answer_rate(db, cl, perms, r, N1, min(3.0, args.cpu_seconds), 1)
+            out["cpu_baseline_1core"] = {"ms_per_query": 1e3 / rate1, "kind": kind1,
+                                         "sample": f"{n1} answers on one thread"}
         print(json.dumps(out), flush=True)
     ctx.close()
     if dist:
