@@ -176,6 +176,16 @@ def cpu_answer_rate(db, client, perms, r, N1, seconds, threads):
     return n / t_end[0], kind, n, threads
 
 
+def host_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
 def host_threads():
     try:
         return len(os.sched_getaffinity(0))
@@ -393,7 +403,7 @@ def run_gpu(args, rank, world, local_rank):
         if world == 1 and not args.no_cpu_baseline:
             threads = host_threads()
             rate, kind, n, th = cpu_answer_rate(db, cl, perms, r, N1, args.cpu_seconds, threads)
-            out["cpu_baseline"] = {"value": rate, "unit": "queries/s", "cores": th, "kind": kind,
+            out["cpu_baseline"] = {"value": rate, "unit": "queries/s", "cores": th, "kind": kind, "host": host_model(),
                                    "sample": f"{n} full answers (r={r}, N1={N1}) in ~{args.cpu_seconds:.0f} s, "
                                              f"one independent query per thread"}
             # the reference's path is single-threaded: its latency on one core
