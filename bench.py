@@ -215,7 +215,7 @@ def read_int8_peak():
 
 def read_traffic(r):
     """DRAM bytes per scan launch from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", "k_scan_single_query_r4.md")
+    p = os.path.join(ROOT, "profiles", "k_scan_single_query_8192_records.md")
     if not os.path.exists(p):
         return None
     for line in open(p):
