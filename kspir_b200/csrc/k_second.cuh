@@ -327,6 +327,16 @@ __global__ void __launch_bounds__(kNttThreads) k_pack_split_fwd(const uint32_t* 
     const uint32_t q = c_dev.ch[ch].q;
     pdl_launch_dependents();
     stage_twiddles(tws, tabs, ch, NTT_FWD);
+    // the key words of this digit, loaded while the previous kernel finishes
+    // (keys are never written by the answer), used after the transform
+    uint32_t ka[kPerThreadG], kb[kPerThreadG];
+    if (d < ELL) {
+#pragma unroll
+        for (int it = 0; it < kPerThreadG; it++) {
+            ka[it] = __ldg(key + ((d * 2 + 0) * 2 + ch) * kN + tid + it * kNttThreads);
+            kb[it] = __ldg(key + ((d * 2 + 1) * 2 + ch) * kN + tid + it * kNttThreads);
+        }
+    }
     pdl_wait();   // the level input comes from the previous kernel
     auto cshift = [&](int comp, int pch, int p) -> uint32_t {   // (X^I c)[p]
         const int s = p - I;
@@ -363,8 +373,8 @@ __global__ void __launch_bounds__(kNttThreads) k_pack_split_fwd(const uint32_t* 
         const int k = tid + it * kNttThreads;
         const uint32_t dv = S[pidx(tid) + it * kPadStep];
         if (d < ELL) {
-            pa[k] = mod_crt((uint64_t)dv * __ldg(key + ((d * 2 + 0) * 2 + ch) * kN + k), ch);
-            pa[kN + k] = mod_crt((uint64_t)dv * __ldg(key + ((d * 2 + 1) * 2 + ch) * kN + k), ch);
+            pa[k] = mod_crt((uint64_t)dv * ka[it], ch);
+            pa[kN + k] = mod_crt((uint64_t)dv * kb[it], ch);
         } else {
             pa[k] = dv;   // NTT(temp.b)
         }
@@ -398,16 +408,22 @@ __global__ void __launch_bounds__(kNttThreads) k_pack_split_inv(const uint32_t* 
         // a' = -sum_d dig_d key[d].a ;  b' = NTT(temp.b) - sum_d dig_d key[d].b
         S[pidx(tid) + it * kPadStep] = comp == 0 ? negmod(sum, q) : submod(__ldcg(pj + (size_t)ELL * 2 * kN + k), sum, q);
     }
-    cta_ntt_inverse(S, tws, ch);
+    // c2 = X^I c + r of the level input, loaded ahead of the transform
     const uint32_t* r0 = in + (size_t)j * 4 * kN;
     const uint32_t* cc = in + (size_t)(I + j) * 4 * kN + (comp * 2 + ch) * kN;
+    uint32_t c2[kPerThreadG];
 #pragma unroll
     for (int it = 0; it < kPerThreadG; it++) {
         const int k = tid + it * kNttThreads;
         const int s = k - I;
         const uint32_t sh = s >= 0 ? __ldcg(cc + s) : negmod(__ldcg(cc + s + kN), q);
-        const uint32_t c2 = addmod(sh, __ldcg(r0 + (comp * 2 + ch) * kN + k), q);
-        out[((size_t)j * 4 + comp * 2 + ch) * kN + k] = addmod(S[pidx(tid) + it * kPadStep], c2, q);
+        c2[it] = addmod(sh, __ldcg(r0 + (comp * 2 + ch) * kN + k), q);
+    }
+    cta_ntt_inverse(S, tws, ch);
+#pragma unroll
+    for (int it = 0; it < kPerThreadG; it++) {
+        const int k = tid + it * kNttThreads;
+        out[((size_t)j * 4 + comp * 2 + ch) * kN + k] = addmod(S[pidx(tid) + it * kPadStep], c2[it], q);
     }
 }
 
