@@ -264,18 +264,22 @@ def bench_client(ctx, n=128, reps=5):
     sec = np.where(sec < 0, sec + CRTMOD, sec).astype(np.uint64)
     rows = rng.integers(0, N // 2, size=n).astype(np.uint32)
     q = ctx.client_queries(sec, rows, seed=1)          # warm-up (tables, allocation)
-    t0 = time.perf_counter()
+    tq = []
     for i in range(reps):
+        t0 = time.perf_counter()
         q = ctx.client_queries(sec, rows, seed=2 + i)
-    tq = (time.perf_counter() - t0) / reps
+        tq.append(time.perf_counter() - t0)
     resp = np.ascontiguousarray(q[:, :2 * N])          # any canonical crtMod words
     ctx.client_decrypt(sec, resp, 16)
-    t0 = time.perf_counter()
+    td = []
     for _ in range(reps):
+        t0 = time.perf_counter()
         ctx.client_decrypt(sec, resp, 16)
-    td = (time.perf_counter() - t0) / reps
-    return {"batch": n, "queries_per_s": n / tq, "decrypts_per_s": n / td,
-            "note": "end to end through kspir_client_queries / kspir_client_decrypt with host buffers"}
+        td.append(time.perf_counter() - t0)
+    return {"batch": n, "queries_per_s": n / float(np.median(tq)), "decrypts_per_s": n / float(np.median(td)),
+            "calls_ms": {"queries": [round(t * 1e3, 3) for t in tq], "decrypts": [round(t * 1e3, 3) for t in td]},
+            "note": "end to end through kspir_client_queries / kspir_client_decrypt with host buffers; "
+                    f"median of {reps} calls"}
 
 
 def run_gpu(args, rank, world, local_rank):

@@ -214,6 +214,10 @@ struct kspir_ctx {
     // client-side helpers: query_encode [N] int32, the message scaling table [p]
     int32_t* cl_qenc = nullptr;
     uint64_t* cl_dm = nullptr;
+    // device buffers of the client calls, kept between calls (grown on
+    // demand): a cudaFree per call would synchronise the whole device
+    uint8_t* cl_scratch = nullptr;
+    size_t cl_scratch_bytes = 0;
     uint8_t* dbop = nullptr;          // its database operand [N][2][G] tiles
     int G = 0;
     uint8_t* qop = nullptr;           // its query operand: launch at slot0 uses qop_at(slot0)
@@ -942,6 +946,7 @@ int kspir_ctx_destroy(kspir_ctx* c) {
     cudaFree(c->prep_dev);
     cudaFree(c->cl_qenc);
     cudaFree(c->cl_dm);
+    cudaFree(c->cl_scratch);
     if (c->prep_host) cudaFreeHost(c->prep_host);
     cudaFree(c->dbop);
     cudaFree(c->qop);
@@ -1157,6 +1162,20 @@ struct Carve {
         return p;
     }
 };
+
+// The context's client scratch, at least `bytes` long (caller holds c->mu).
+int client_scratch(kspir_ctx* c, size_t bytes, uint8_t** out) {
+    if (c->cl_scratch_bytes < bytes) {
+        KS_CUDA(c, cudaStreamSynchronize(c->stream));
+        cudaFree(c->cl_scratch);
+        c->cl_scratch = nullptr;
+        c->cl_scratch_bytes = 0;
+        KS_CUDA(c, cudaMalloc(&c->cl_scratch, bytes));
+        c->cl_scratch_bytes = bytes;
+    }
+    *out = c->cl_scratch;
+    return KSPIR_OK;
+}
 }  // namespace
 
 extern "C" {
@@ -1173,7 +1192,7 @@ int kspir_client_queries(kspir_ctx* c, int n, const uint64_t* secrets, const uin
     if (rc) return rc;
     const size_t sw = (size_t)n * kN, qw = (size_t)n * 4 * kN, rw = (size_t)n * 6 * kN;
     Carve cv;
-    KS_CUDA(c, cudaMalloc(&cv.base, sw * 8 + qw * 8 + rw * 4 + (size_t)n * 4 + 1024));
+    if ((rc = client_scratch(c, sw * 8 + qw * 8 + rw * 4 + (size_t)n * 4 + 1024, &cv.base))) return rc;
     uint64_t* d_s = cv.take<uint64_t>(sw);
     uint64_t* d_q = cv.take<uint64_t>(qw);
     uint32_t* d_res = cv.take<uint32_t>(rw);
@@ -1188,7 +1207,6 @@ int kspir_client_queries(kspir_ctx* c, int n, const uint64_t* secrets, const uin
         if (e != cudaSuccess) rc = set_err(c, KSPIR_ERR_CUDA, std::string("client query: ") + cudaGetErrorString(e));
     }
     if (!rc) rc = copy_sync(c, queries, d_q, qw * 8, cudaMemcpyDeviceToHost);
-    cudaFree(cv.base);
     return rc;
 }
 
@@ -1205,12 +1223,13 @@ int kspir_client_decrypt(kspir_ctx* c, int n, const uint64_t* secrets, const uin
     const uint64_t qinv = (uint64_t)h_invmod((uint64_t)r % kCrtMod, kCrtMod);
     const size_t sw = (size_t)n * kN, rw = (size_t)n * 2 * kN;
     Carve cv;
-    KS_CUDA(c, cudaMalloc(&cv.base, sw * 8 + rw * 8 + rw * 4 + sw * 8 + 1024));
+    int rc = client_scratch(c, sw * 8 + rw * 8 + rw * 4 + sw * 8 + 1024, &cv.base);
+    if (rc) return rc;
     uint64_t* d_s = cv.take<uint64_t>(sw);
     uint64_t* d_r = cv.take<uint64_t>(rw);
     uint32_t* d_res = cv.take<uint32_t>(rw);
     uint64_t* d_m = cv.take<uint64_t>(sw);
-    int rc = copy_sync(c, d_s, secrets, sw * 8, cudaMemcpyHostToDevice);
+    rc = copy_sync(c, d_s, secrets, sw * 8, cudaMemcpyHostToDevice);
     if (!rc) rc = copy_sync(c, d_r, responses, rw * 8, cudaMemcpyHostToDevice);
     if (!rc) {
         k_client_decrypt<<<dim3(2, n), kNttThreads, kClientSmem, c->stream>>>(d_s, d_r, qinv, d_res, c->ntabs);
@@ -1219,7 +1238,6 @@ int kspir_client_decrypt(kspir_ctx* c, int n, const uint64_t* secrets, const uin
         if (e != cudaSuccess) rc = set_err(c, KSPIR_ERR_CUDA, std::string("client decrypt: ") + cudaGetErrorString(e));
     }
     if (!rc) rc = copy_sync(c, messages, d_m, sw * 8, cudaMemcpyDeviceToHost);
-    cudaFree(cv.base);
     return rc;
 }
 
