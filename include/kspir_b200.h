@@ -44,7 +44,7 @@ extern "C" {
 #define KSPIR_ERR_NOT_READY -3     /* database, permutations or client keys missing */
 #define KSPIR_ERR_OOM -4           /* device allocation failed */
 #define KSPIR_ERR_TIMEOUT -5       /* a bounded device-side wait gave up */
-#define KSPIR_ERR_BUSY -6          /* no free slot (serving admission) */
+#define KSPIR_ERR_BUSY -6          /* the server cannot take the call now (client has requests in flight) */
 #define KSPIR_ERR_IO -7            /* file error, or a malformed / corrupted container */
 
 #define KSPIR_N 4096

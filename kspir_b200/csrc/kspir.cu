@@ -849,7 +849,7 @@ const char* kspir_strerror(int code) {
         case KSPIR_ERR_NOT_READY: return "database, permutations or keys missing";
         case KSPIR_ERR_OOM: return "out of device memory";
         case KSPIR_ERR_TIMEOUT: return "device-side wait timed out";
-        case KSPIR_ERR_BUSY: return "no free slot";
+        case KSPIR_ERR_BUSY: return "busy: requests in flight";
         case KSPIR_ERR_IO: return "file or format error";
         default: return "unknown error";
     }

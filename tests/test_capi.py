@@ -52,6 +52,6 @@ def test_invalid_params_rejected_before_device(lib):
 
 
 def test_strerror(lib):
-    for code in (0, -1, -2, -3, -4, -5, -6):
+    for code in (0, -1, -2, -3, -4, -5, -6, -7):
         assert lib.kspir_strerror(code)
     assert lib.kspir_answer(None, 0, None, None) == native.ERR_INVALID_ARG
