@@ -55,3 +55,29 @@ def test_strerror(lib):
     for code in (0, -1, -2, -3, -4, -5, -6, -7):
         assert lib.kspir_strerror(code)
     assert lib.kspir_answer(None, 0, None, None) == native.ERR_INVALID_ARG
+
+
+@pytest.mark.parametrize("N1", [64, 128, 256])
+def test_permutation_matrix_is_the_references(lib, N1):
+    """kspir_permutation_matrix is host code: it must equal the oracle's
+    compute_permutation_matrix (utils.cpp:1591-1619) and, where the reference
+    is built here, the reference's own."""
+    import numpy as np
+
+    from oracle import pyoracle as po
+
+    got = native.permutation_matrix(N1)
+    assert (got == po.permutation_matrix(N1)).all()
+    if po.ref_available():
+        want = np.zeros(N1 * native.N, np.int32)
+        po.ref().ref_permutation_matrix(po._p(want), N1)
+        assert (got == want).all()
+
+
+def test_permutation_matrix_rejects_bad_shapes(lib):
+    import numpy as np
+
+    out = np.zeros(128 * native.N, np.int32)   # rejected shapes write nothing
+    for N1 in (0, -1, native.N // 2 + 1, 8192):
+        assert lib.kspir_permutation_matrix(native.ptr(out), N1) == native.ERR_INVALID_ARG
+    assert lib.kspir_permutation_matrix(None, 128) == native.ERR_INVALID_ARG
