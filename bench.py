@@ -62,6 +62,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batches", default="1,8,32,64,128", help="batch sizes of the batched sweep ('' = none)")
     ap.add_argument("--clients", type=int, default=128, help="distinct client key sets of the batched sweep")
+    ap.add_argument("--no-extras", dest="extras", action="store_false",
+                    help="skip the 1 GB database and the serving run")
+    ap.add_argument("--serving-rates", default="1000,4000", help="offered queries/s of the serving run")
     return ap.parse_args()
 
 
@@ -364,7 +367,18 @@ def run_gpu(args, rank, world, local_rank):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms, e2e_s = float(t[0]), float(t[1])
 
-    batched = run_batched(args, ctx, batches, nclients, rank, dist, torch) if batches else None
+    clients16 = [cl]
+    batched = run_batched(args, ctx, batches, nclients, rank, dist, torch, clients16) if batches else None
+    rotating = bench_rotating(args, ctx, nclients, torch) if nclients >= 16 else None
+    extra = {}
+    if args.extras and world == 1 and len(clients16) >= 32:
+        ctx64, clients64 = None, None
+        try:
+            ctx64, clients64, extra["db_1gb"] = bench_1gb(args, torch)
+            extra["serving"] = bench_serving(args, ctx, clients16, ctx64, clients64)
+        finally:
+            if ctx64 is not None:
+                ctx64.close()
 
     if rank == 0:
         db_bytes = r * N * N // 2 * 8
@@ -402,6 +416,9 @@ def run_gpu(args, rank, world, local_rank):
         }
         if batched:
             out["batched"] = batched
+        if rotating:
+            out["single_rotating_clients"] = rotating
+        out.update(extra)
         out["db_preprocess"] = prep
         out["client"] = bench_client(ctx)
         if world == 1 and not args.no_cpu_baseline:
@@ -420,15 +437,18 @@ def run_gpu(args, rank, world, local_rank):
         dist.destroy_process_group()
 
 
-def run_batched(args, ctx, batches, nclients, rank, dist, torch):
+def run_batched(args, ctx, batches, nclients, rank, dist, torch, keep):
     """Batched answers of distinct clients at each batch size (the answer of
-    every query equals its single-query answer; tests/test_gpu_batch.py)."""
+    every query equals its single-query answer; tests/test_gpu_batch.py).
+    Client key sets 1..31 are appended to `keep` (for the serving run)."""
     import kspir_b200 as kb
     from kspir_b200 import synth
     r, N1 = args.r, args.N1
     for i in range(1, nclients):
         c = synth.gen_client(args.seed + 1000 * (rank + 1) + i, r, N1)
         ctx.upload_client(i, c["baby"], c["giant"], c["packing"], c["rgsw"])
+        if i < 32:
+            keep.append(c)
     rng = np.random.default_rng(args.seed + 77 + rank)
     bmax = max(batches)
     qall = np.empty((bmax, 4 * N), np.uint64)
@@ -505,6 +525,155 @@ def run_batched(args, ctx, batches, nclients, rank, dist, torch):
         for k, v in res.items():
             v["speedup_vs_batch1"] = v["queries_per_s"] / base
     return res
+
+
+def bench_rotating(args, ctx, nclients, torch):
+    """Single-query answers cycling through 16+ clients' keys (22 MiB each, so
+    a client's keys are not left in the 126 MB L2 by its previous answer, as
+    they are when one client asks repeatedly): device-timed."""
+    rng = np.random.default_rng(args.seed + 5)
+    q = np.empty(4 * N, np.uint64)
+    q[:2 * N] = rng.integers(0, CRTMOD, 2 * N, dtype=np.uint64)
+    q[2 * N:] = rng.integers(0, 16760833, 2 * N, dtype=np.uint64)
+    dq = torch.from_numpy(q.view(np.int64).copy()).cuda()
+    dr = torch.empty(2 * N, dtype=torch.int64, device="cuda")
+    stream = torch.cuda.Stream()
+    n = max(args.steps, 2 * nclients)
+    for i in range(nclients):
+        ctx.answer_device(i, dq.data_ptr(), dr.data_ptr(), stream.cuda_stream)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(n):
+        ctx.answer_device(i % nclients, dq.data_ptr(), dr.data_ptr(), stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ctx.sync()
+    ms = e0.elapsed_time(e1)
+    return {"queries_per_s": n / (ms * 1e-3), "ms_per_answer": ms / n, "answers": n, "clients": nclients,
+            "note": "one query at a time, client i % clients, keys of 22 MiB per client (not L2-resident)"}
+
+
+def bench_1gb(args, torch):
+    """The 1 GB database (131072 records x 8 KB: r = 64, N1 = 128, 4 GiB
+    preprocessed): the raw database is drawn on the device and preprocessed
+    there; single answers (device-timed) and a batch of 32 distinct clients."""
+    import kspir_b200 as kb
+    from kspir_b200 import synth
+    r, N1, B = 64, args.N1, 32
+    ctx = kb.Context(r, N1, max_clients=B, max_inflight=B)
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(args.seed + 64)
+    raw = torch.randint(0, 65537, (r * N * N // 2,), dtype=torch.int64, device="cuda", generator=gen)
+    prep_ms = ctx.preprocess_db_device(raw.data_ptr(), raw.numel())
+    del raw
+    ctx.upload_perms(kb.permutation_matrix(N1))
+    clients = []
+    for i in range(B):
+        c = synth.gen_client(args.seed + 6400 + i, r, N1)
+        ctx.upload_client(i, c["baby"], c["giant"], c["packing"], c["rgsw"])
+        clients.append(c)
+    qs = np.stack([c["query"] for c in clients])
+    dq = torch.from_numpy(qs.view(np.int64).copy()).cuda()
+    dr = torch.empty((B, 2 * N), dtype=torch.int64, device="cuda")
+    stream = torch.cuda.Stream()
+    for _ in range(3):
+        ctx.answer_device(0, dq[0].data_ptr(), dr[0].data_ptr(), stream.cuda_stream)
+    torch.cuda.synchronize()
+    ctx.timing_reset()
+    reps = 20
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(reps):
+        ctx.answer_device(i % B, dq[i % B].data_ptr(), dr[0].data_ptr(), stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms1 = e0.elapsed_time(e1) / reps
+    n1, _, _, ph1 = ctx.timing_summary()
+    ctx.sync()
+    cl = np.arange(B, dtype=np.int32)
+    kind, _ = ctx.tune_batch(B)
+    for _ in range(3):
+        ctx.answer_batch_device(cl, dq.data_ptr(), dr.data_ptr(), stream.cuda_stream)
+    torch.cuda.synchronize()
+    ctx.timing_reset()
+    reps_b = 5
+    e0.record(stream)
+    for _ in range(reps_b):
+        ctx.answer_batch_device(cl, dq.data_ptr(), dr.data_ptr(), stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    msb = e0.elapsed_time(e1) / reps_b
+    nb, _, _, phb = ctx.timing_summary()
+    ctx.sync()
+    db_bytes = r * N * N // 2 * 8
+    names = ("baby_steps", "db_scan", "giant_steps", "external_products", "packing")
+    out = {"workload": f"1 GB database: 131072 x 8 KB records, r={r} N1={N1}, {db_bytes >> 30} GiB preprocessed",
+           "preprocess_device_ms": prep_ms,
+           "single": {"ms_per_answer": ms1, "queries_per_s": 1e3 / ms1,
+                      "scan_gbs": db_bytes / (ph1[1] / n1 * 1e-3) / 1e9,
+                      "phases_ms": {k: v / n1 for k, v in zip(names, ph1)},
+                      "note": "device-timed, clients rotating over 32 key sets"},
+           "batch32": {"ms_per_batch": msb, "queries_per_s": B / (msb * 1e-3), "scan_kind": kb.SCAN_NAMES[kind],
+                       "phases_ms": {k: v / reps_b for k, v in zip(names, phb)}}}
+    return ctx, clients, out
+
+
+def bench_serving(args, ctx16, clients16, ctx64, clients64):
+    """Serving with the 256 MB and the 1 GB databases resident together
+    (kspir_server_*: continuous batching over lanes, client keys in device
+    slots): seeded compound-Poisson arrivals (bursts of 1..64 queries, 3:1
+    between the databases) at each offered rate; served queries/s and
+    submit-to-response p50/p95/p99, beside the plain per-query path through
+    the same servers (one request at a time)."""
+    import types
+
+    import kspir_b200 as kb
+    from kspir_b200 import serving
+    lanes = {16: (2, 64), 64: (1, 32)}
+    deps = []
+    for r, ctx, keys in ((16, ctx16, clients16), (64, ctx64, clients64)):
+        nl, ls = lanes[r]
+        srv = kb.Server(ctx, lanes=nl, lane_size=ls)
+        n_cl = len(keys)
+        for i, c in enumerate(keys):
+            srv.register(i, c["baby"], c["giant"], c["packing"], c["rgsw"])
+        deps.append(types.SimpleNamespace(r=r, server=srv, clients=list(range(n_cl))))
+    try:
+        plain = {}
+        q1 = serving.random_queries(np.random.default_rng(1), 1)[0]
+        for d in deps:
+            d.server.wait(d.server.submit(0, q1))
+            d.server.reset_stats()
+            for _ in range(20):
+                d.server.wait(d.server.submit(0, q1))
+            lat = d.server.latencies_us()
+            plain[f"r{d.r}"] = {"p50_us": float(np.percentile(lat, 50)), "queries_per_s": 1e6 / float(np.mean(lat))}
+        serving.drive(deps, [3, 1], serving.poisson_schedule(1000, 0.5, args.seed + 99, 64), args.seed + 98)
+        rows = []
+        for rate in [float(x) for x in args.serving_rates.split(",") if x.strip()]:
+            for d in deps:
+                d.server.reset_stats()
+            wall, nq = serving.drive(deps, [3, 1], serving.poisson_schedule(rate, 1.5, args.seed + int(rate), 64),
+                                     args.seed + 7 * int(rate))
+            lat = np.concatenate([d.server.latencies_us() for d in deps])
+            row = {"offered_qps": rate, "queries": nq, "served_qps": nq / wall,
+                   "p50_ms": float(np.percentile(lat, 50)) / 1e3, "p95_ms": float(np.percentile(lat, 95)) / 1e3,
+                   "p99_ms": float(np.percentile(lat, 99)) / 1e3, "per_db": {}}
+            for d in deps:
+                st = d.server.stats()
+                row["per_db"][f"r{d.r}"] = {"served": st["served"], "mean_batch": st["mean_batch"],
+                                            "p50_ms": st["p50_us"] / 1e3, "p99_ms": st["p99_us"] / 1e3,
+                                            "max_running_lanes": st["max_running_lanes"]}
+            rows.append(row)
+    finally:
+        for d in deps:
+            d.server.close()
+    return {"workload": "256 MB (r=16) and 1 GB (r=64) databases resident together; 32 clients each; "
+                        "lanes 2 x 64 (256 MB) and 1 x 32 (1 GB); bursts of 1..64, 3:1 between the databases",
+            "plain_per_query": plain, "rates": rows}
 
 
 def run_reference(args, rank, world):

@@ -228,8 +228,11 @@ int kspir_external_product(kspir_ctx* ctx, int client, uint64_t* result, uint64_
 
 /* Reference packingRLWEs (answer.h:79-80, answer.cpp:800-835): packs r
  * coefficient-form RLWEs ([r][2][N]) into response ([2][N], coefficient
- * form).  Host buffers; rlwes is read only. */
-int kspir_packing_rlwes(kspir_ctx* ctx, int client, const uint64_t* rlwes, uint64_t* response);
+ * form).  Host buffers.  rlwes is overwritten as the reference overwrites it
+ * (answer.cpp:821-828): rlwes[0] becomes the response and, for each merge of
+ * rlwes[j] with rlwes[I + j] (I = r/2, ..., 1; j < I), rlwes[I + j] becomes
+ * X^I rlwes[I + j] + rlwes[j] of that level's inputs. */
+int kspir_packing_rlwes(kspir_ctx* ctx, int client, uint64_t* rlwes, uint64_t* response);
 
 /* No counterpart in the reference.  The external product of
  * kspir_external_product (reference externalProduct, lwe.cpp:761-808, with
@@ -246,7 +249,9 @@ int kspir_packing_rlwes(kspir_ctx* ctx, int client, const uint64_t* rlwes, uint6
  * count <= KSPIR_NOALLOC_MAX_COUNT; larger counts are rejected with
  * KSPIR_ERR_INVALID_ARG, as are non-canonical words (outputs then untouched).
  * Work is enqueued on `stream` (a cudaStream_t, NULL = the legacy default
- * stream) and the call returns after it completes.
+ * stream); the call then waits for that stream (cudaStreamSynchronize) and
+ * reads a validation word back, so it returns only after its work is done
+ * and blocks the calling thread until then.
  * Scratch: a fixed file-scope device array of about 6.3 MiB (plus 192 KiB of
  * transform tables) that every GPU loading this library holds until the
  * process exits.  All calls on a device share it, so calls that overlap on
@@ -292,6 +297,17 @@ int kspir_fetch_stage(kspir_ctx* ctx, int stage, uint64_t* out, size_t words);
 /* Same for the query that ran in workspace slot `slot` (query i of the last
  * batch ran in slot i). */
 int kspir_fetch_stage_slot(kspir_ctx* ctx, int slot, int stage, uint64_t* out, size_t words);
+
+/* Failure injection, for tests of the device-side failure detection.  Every
+ * wait of the database scan on the device is bounded: a wait that runs out
+ * records an error word and the kernel returns, and the call that collects
+ * the launch reports KSPIR_ERR_TIMEOUT; the context stays usable.  This sets
+ * the limit of those waits (wait_limit_ns <= 0: the default of 2 s) and makes
+ * the next CUDA-core database scan (the one of a single answer) skip the copy
+ * of local work item `skip_item` of its first CTA (-1: none), so that the
+ * wait for it runs out.  No GPU fault is involved: the kernel only waits for
+ * bytes that were never requested. */
+int kspir_debug_scan_fault(kspir_ctx* ctx, int64_t wait_limit_ns, long skip_item);
 
 /* Bytes of one client's keys in a device key slot (for sizing max_clients
  * from an HBM budget). */

@@ -34,7 +34,7 @@ __all__ = [
     "STAGE_CIPHERBUF", "STAGE_SCAN", "STAGE_RESULT", "STAGE_EXT",
     "SCAN_CUDA", "SCAN_MMA4", "SCAN_MMA8", "SCAN_MMA16", "SCAN_MMA32", "SCAN_NAMES",
     "AutoKeyBSGSRNS", "AutoKey", "RGSWCiphertext",
-    "matrix_vector_mul_bsgs_rns_crt_large", "externalProduct", "packingRLWEs",
+    "matrix_vector_mul_bsgs_rns_crt_large", "externalProduct", "packingRLWEs", "invalidate",
     "key_bundle_bytes", "key_bundle_write", "key_bundle_read", "query_pack", "query_unpack", "response_pack",
     "response_unpack", "QUERY_WIRE_BYTES", "RESPONSE_WIRE_BYTES",
 ]
@@ -64,14 +64,24 @@ class RGSWCiphertext:
 
 
 class _Session:
-    """Device context reused across mirror calls; re-uploads only what changed."""
+    """Device context reused across mirror calls; uploads only what changed.
+
+    Key parts and permutations are compared word for word with the copies
+    last uploaded, so an object rewritten in place, or a new object at a
+    freed one's address, is uploaded again.  The database (1 GiB at r = 16) is
+    recognised by its address, size and a fingerprint of 4096 words spread
+    over it: a caller that edits a few words of the same array in place calls
+    :func:`invalidate` (or passes a new array) before the next answer."""
+
+    PARTS = ("baby", "giant", "packing", "rgsw")
 
     def __init__(self):
         self.ctx = None
         self.key = None
         self.db_id = None
-        self.perm_id = None
-        self.client_ids = None
+        self.perms = None
+        self.parts = {}
+        self.uploaded = False
 
     def get(self, r: int, N1: int) -> Context:
         if self.ctx is None or self.key != (r, N1):
@@ -79,28 +89,54 @@ class _Session:
                 self.ctx.close()
             self.ctx = Context(r, N1)
             self.key = (r, N1)
-            self.db_id = self.perm_id = self.client_ids = None
+            self.invalidate()
         return self.ctx
 
-    def ensure(self, ctx: Context, data=None, perms=None, baby=None, giant=None, packing=None, rgsw=None):
-        if data is not None and self.db_id != _ident(data):
+    def current(self, r: int | None = None, N1: int | None = None) -> Context:
+        """The session's context, or a new one of (r, N1) (defaults r = 1, N1 = 128)."""
+        if self.ctx is not None and (r is None or r == self.key[0]) and (N1 is None or N1 == self.key[1]):
+            return self.ctx
+        return self.get(r if r is not None else (self.key[0] if self.key else 1),
+                        N1 if N1 is not None else (self.key[1] if self.key else 128))
+
+    def ensure(self, ctx: Context, data=None, perms=None, **keys):
+        if data is not None and self.db_id != _db_fingerprint(data):
             ctx.upload_db(data)
-            self.db_id = _ident(data)
-        if perms is not None and self.perm_id != _ident(perms):
-            ctx.upload_perms(perms)
-            self.perm_id = _ident(perms)
-        ids = tuple(_ident(a) for a in (baby, giant, packing, rgsw))
-        if self.client_ids != ids:
-            ctx.upload_client(0, *_fill_keys(ctx, baby, giant, packing, rgsw))
-            self.client_ids = ids
+            self.db_id = _db_fingerprint(data)
+        if perms is not None:
+            p = np.asarray(perms, dtype=np.int32).reshape(-1)
+            if self.perms is None or not np.array_equal(self.perms, p):
+                ctx.upload_perms(p)
+                self.perms = p.copy()
+        changed = False
+        for name in self.PARTS:
+            a = keys.get(name)
+            if a is None:
+                continue
+            a = np.asarray(a, dtype=np.uint64).reshape(-1)
+            cur = self.parts.get(name)
+            if cur is None or not np.array_equal(cur, a):
+                self.parts[name] = a.copy()
+                changed = True
+        if changed or not self.uploaded:
+            ctx.upload_client(0, *_fill_keys(ctx, *(self.parts.get(n) for n in self.PARTS)))
+            self.uploaded = True
+
+    def invalidate(self):
+        self.db_id = None
+        self.perms = None
+        self.parts = {}
+        self.uploaded = False
 
 
-def _ident(a):
-    return None if a is None else (a.ctypes.data, a.nbytes, a.__array_interface__["data"][0])
+def _db_fingerprint(a):
+    flat = np.asarray(a).reshape(-1)
+    idx = np.linspace(0, flat.size - 1, num=min(4096, flat.size), dtype=np.int64)
+    return (flat.ctypes.data, flat.nbytes, flat[idx].tobytes())
 
 
 def _fill_keys(ctx: Context, baby, giant, packing, rgsw):
-    """Zero-filled stand-ins for key parts a staged call does not use."""
+    """Zero-filled stand-ins for key parts no call has supplied yet."""
     if baby is None:
         baby = np.zeros((ctx.N1 // 2) * 6 * 2 * N, dtype=np.uint64)
     if giant is None:
@@ -110,6 +146,12 @@ def _fill_keys(ctx: Context, baby, giant, packing, rgsw):
     if rgsw is None:
         rgsw = np.zeros(4 * 2 * N, dtype=np.uint64)
     return baby, giant, packing, rgsw
+
+
+def invalidate() -> None:
+    """Forget what the reference-named mirror uploaded: the next call uploads
+    its database, permutations and keys again."""
+    _session.invalidate()
 
 
 _session = _Session()
@@ -128,20 +170,23 @@ def matrix_vector_mul_bsgs_rns_crt_large(result: np.ndarray, input: np.ndarray, 
     input.reshape(-1)[:] = q
 
 
-def externalProduct(result: np.ndarray, firstDim: np.ndarray, query: RGSWCiphertext, r: int = 1,
-                    N1: int = 128) -> None:
+def externalProduct(result: np.ndarray, firstDim: np.ndarray, query: RGSWCiphertext, r: int | None = None,
+                    N1: int | None = None) -> None:
     """Reference lwe.cpp:761-808: result ([2][N]) += g^-1(firstDim) x query,
-    returned in coefficient form; firstDim (NTT form) becomes coefficient form."""
-    ctx = _session.get(r, N1)
-    _session.ensure(ctx, rgsw=query.rows, baby=None, giant=None, packing=None)
+    returned in coefficient form; firstDim (NTT form) becomes coefficient form.
+    Runs in the session's current context unless r / N1 name another one."""
+    ctx = _session.current(r, N1)
+    _session.ensure(ctx, rgsw=query.rows)
     res, fd = ctx.external_product(0, result, firstDim)
     result.reshape(-1)[:] = res
     firstDim.reshape(-1)[:] = fd
 
 
-def packingRLWEs(result: np.ndarray, rlwes: np.ndarray, autokey: AutoKey, N1: int = 128) -> None:
-    """Reference answer.cpp:800-835: packs rlwes ([r][2][N], coefficient form) into result ([2][N])."""
+def packingRLWEs(result: np.ndarray, rlwes: np.ndarray, autokey: AutoKey, N1: int | None = None) -> None:
+    """Reference answer.cpp:800-835: packs rlwes ([r][2][N], coefficient form)
+    into result ([2][N]) and leaves rlwes as the reference does (rlwes[0] =
+    the result, rlwes[I + j] = X^I rlwes[I + j] + rlwes[j] of each merge)."""
     r = rlwes.reshape(-1).size // (2 * N)
-    ctx = _session.get(r, N1)
+    ctx = _session.current(r, N1)
     _session.ensure(ctx, packing=autokey.keys)
-    result.reshape(-1)[:] = ctx.packing(0, rlwes)
+    result.reshape(-1)[:] = ctx.packing(0, rlwes, rlwes_out=rlwes)

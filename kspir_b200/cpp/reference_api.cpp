@@ -15,12 +15,17 @@
 // input[0] is modswitched in place to NTT form and result[j] comes back in NTT
 // form; externalProduct accumulates into `result` and returns both `result`
 // and `firstDim` in coefficient form; packingRLWEs writes the packed response
-// in coefficient form.  One difference: packingRLWEs leaves `rlwes` as it was
-// (the reference overwrites it with the packing tree's intermediates).
+// in coefficient form and leaves `rlwes` as the reference does (rlwes[0] =
+// the response, rlwes[I + j] = X^I rlwes[I + j] + rlwes[j] of each merge).
 //
-// The database, permutations and key objects are uploaded to the device the
-// first time they are seen and stay resident; an object at an address already
-// uploaded is assumed unchanged (the reference's callers build them once).
+// The database, permutations and key words stay resident on the device
+// between calls.  Every call gathers the words of the key objects and of the
+// permutations and compares them with the resident copy, so an object
+// rewritten in place, or a new one built where a freed one lived, is uploaded
+// again.  The database (1 GiB at r = 16) is recognised by its address and a
+// fingerprint of 4096 words spread over it, which any re-preprocessing
+// changes; a caller that edits a few datacrt words in place calls
+// kspir_dropin_invalidate() before the next answer.
 // The reference's functions return void and check only with assert; an error
 // of the library here prints its message and aborts likewise.
 //
@@ -46,13 +51,27 @@ struct Session {
     kspir_ctx* ctx = nullptr;
     int r = 0, N1 = 0;
     const uint64_t* db = nullptr;
-    const void* perms = nullptr;
-    const void* bsgs = nullptr;   // key objects whose words are resident
-    const void* gsw = nullptr;
-    const void* pack = nullptr;
+    std::vector<uint64_t> db_sample;   // fingerprint of the resident database
+    std::vector<int32_t> perms;        // resident permutations (empty: none)
     std::vector<uint64_t> baby, giant, packing, rgsw;   // words of client slot 0
+    bool keys_uploaded = false;
 };
 Session g;
+
+constexpr size_t kDbSample = 4096;
+
+std::vector<uint64_t> db_fingerprint(const uint64_t* data, size_t words) {
+    std::vector<uint64_t> f(kDbSample);
+    for (size_t i = 0; i < kDbSample; i++) f[i] = data[i * (words - 1) / (kDbSample - 1)];
+    return f;
+}
+
+// dst (the resident copy) := src; true if any word differed
+bool gather(uint64_t* dst, const uint64_t* src, size_t words) {
+    if (memcmp(dst, src, words * 8) == 0) return false;
+    memcpy(dst, src, words * 8);
+    return true;
+}
 
 void check(const char* what, int rc) {
     if (rc == KSPIR_OK) return;
@@ -82,6 +101,12 @@ void put_rlwe(uint64_t* dst, const RlweCiphertext& c) {
     memcpy(dst + kPoly, c.b.data(), kPoly * 8);
 }
 
+bool gather_rlwe(uint64_t* dst, const RlweCiphertext& c) {
+    const bool ca = gather(dst, c.a.data(), kPoly);
+    const bool cb = gather(dst + kPoly, c.b.data(), kPoly);
+    return ca || cb;
+}
+
 void get_rlwe(RlweCiphertext& c, const uint64_t* src) {
     c.a.assign(src, src + kPoly);
     c.b.assign(src + kPoly, src + 2 * kPoly);
@@ -107,10 +132,12 @@ void ensure(int r, int N1) {
     g.rgsw.assign((size_t)4 * 2 * kPoly, 0);
 }
 
-void upload_keys() {
+void upload_keys(bool changed) {
+    if (!changed && g.keys_uploaded) return;
     check("kspir_client_keys_upload",
           kspir_client_keys_upload(g.ctx, 0, g.baby.data(), g.giant.empty() ? nullptr : g.giant.data(),
                                    g.packing.empty() ? nullptr : g.packing.data(), g.rgsw.data()));
+    g.keys_uploaded = true;
 }
 
 // The preprocessing runs in a context of its own (one sub-database at a time,
@@ -176,30 +203,32 @@ void matrix_vector_mul_bsgs_rns_crt_large(std::vector<RlweCiphertext>& result, s
                                           std::vector<std::vector<int32_t> >& permutations, int32_t r) {
     ensure(r, N1);
     const int N2 = kPoly / 2 / N1;
-    if (g.db != data) {
-        check("kspir_db_upload", kspir_db_upload(g.ctx, data, (size_t)r * kPoly * (kPoly / 2)));
+    const size_t db_words = (size_t)r * kPoly * (kPoly / 2);
+    std::vector<uint64_t> fp = db_fingerprint(data, db_words);
+    if (g.db != data || g.db_sample != fp) {
+        check("kspir_db_upload", kspir_db_upload(g.ctx, data, db_words));
         g.db = data;
+        g.db_sample.swap(fp);
     }
-    if (g.perms != (const void*)&permutations) {
-        std::vector<int32_t> flat((size_t)N1 * kPoly);
-        for (int i = 0; i < N1; i++) memcpy(flat.data() + (size_t)i * kPoly, permutations[i].data(), kPoly * 4);
+    std::vector<int32_t> flat((size_t)N1 * kPoly);
+    for (int i = 0; i < N1; i++) memcpy(flat.data() + (size_t)i * kPoly, permutations[i].data(), kPoly * 4);
+    if (flat != g.perms) {
         check("kspir_perms_upload", kspir_perms_upload(g.ctx, flat.data(), flat.size()));
-        g.perms = &permutations;
+        g.perms.swap(flat);
     }
-    if (g.bsgs != (const void*)&autoKey) {
-        // baby keys keyMap[5^i], i = 1..N1/2 (six RLWEs each: crtMod rows, then bsMod
-        // rows); giant keys keyMap[5^(N1 c)], c = 1..N2-1 (two RLWEs each)
-        for (int i = 1; i <= N1 / 2; i++) {
-            const std::vector<RlweCiphertext>& v = autoKey.keyMap.at((int32_t)pow5_mod2n(i));
-            for (int j = 0; j < 6; j++) put_rlwe(g.baby.data() + ((size_t)(i - 1) * 6 + j) * 2 * kPoly, v[j]);
-        }
-        for (int c = 1; c < N2; c++) {
-            const std::vector<RlweCiphertext>& v = autoKey.keyMap.at((int32_t)pow5_mod2n((long)N1 * c));
-            for (int j = 0; j < 2; j++) put_rlwe(g.giant.data() + ((size_t)(c - 1) * 2 + j) * 2 * kPoly, v[j]);
-        }
-        upload_keys();
-        g.bsgs = &autoKey;
+    // baby keys keyMap[5^i], i = 1..N1/2 (six RLWEs each: crtMod rows, then bsMod
+    // rows); giant keys keyMap[5^(N1 c)], c = 1..N2-1 (two RLWEs each)
+    bool changed = false;
+    for (int i = 1; i <= N1 / 2; i++) {
+        const std::vector<RlweCiphertext>& v = autoKey.keyMap.at((int32_t)pow5_mod2n(i));
+        for (int j = 0; j < 6; j++)
+            changed |= gather_rlwe(g.baby.data() + ((size_t)(i - 1) * 6 + j) * 2 * kPoly, v[j]);
     }
+    for (int c = 1; c < N2; c++) {
+        const std::vector<RlweCiphertext>& v = autoKey.keyMap.at((int32_t)pow5_mod2n((long)N1 * c));
+        for (int j = 0; j < 2; j++) changed |= gather_rlwe(g.giant.data() + ((size_t)(c - 1) * 2 + j) * 2 * kPoly, v[j]);
+    }
+    upload_keys(changed);
     std::vector<uint64_t> q(4 * kPoly), res((size_t)r * 2 * kPoly);
     put_rlwe(q.data(), input[0]);
     put_rlwe(q.data() + 2 * kPoly, input[1]);
@@ -215,14 +244,12 @@ void matrix_vector_mul_bsgs_rns_crt_large(std::vector<RlweCiphertext>& result, s
 
 void externalProduct(RlweCiphertext& result, RlweCiphertext& firstDim, const RGSWCiphertext& query) {
     if (!g.ctx) ensure(1, 128);
-    if (g.gsw != (const void*)&query) {
-        for (int j = 0; j < 4; j++) {
-            memcpy(g.rgsw.data() + (size_t)j * 2 * kPoly, query.a[j].data(), kPoly * 8);
-            memcpy(g.rgsw.data() + (size_t)j * 2 * kPoly + kPoly, query.b[j].data(), kPoly * 8);
-        }
-        upload_keys();
-        g.gsw = &query;
+    bool changed = false;
+    for (int j = 0; j < 4; j++) {
+        changed |= gather(g.rgsw.data() + (size_t)j * 2 * kPoly, query.a[j].data(), kPoly);
+        changed |= gather(g.rgsw.data() + (size_t)j * 2 * kPoly + kPoly, query.b[j].data(), kPoly);
     }
+    upload_keys(changed);
     std::vector<uint64_t> acc(2 * kPoly), fd(2 * kPoly);
     put_rlwe(acc.data(), result);
     put_rlwe(fd.data(), firstDim);
@@ -236,18 +263,31 @@ void externalProduct(RlweCiphertext& result, RlweCiphertext& firstDim, const RGS
 void packingRLWEs(RlweCiphertext& result, std::vector<RlweCiphertext>& rlwes, const AutoKey& autokey) {
     const int r = (int)rlwes.size();
     if (!g.ctx || g.r != r) ensure(r, g.N1 ? g.N1 : 128);
-    if (g.pack != (const void*)&autokey) {
-        // keyMap[N/2^l + 1], l = 0..log2 r - 1, four RLWEs each
-        for (int l = 0; l < log2i(r); l++) {
-            const std::vector<RlweCiphertext>& v = autokey.keyMap.at(kPoly / (1 << l) + 1);
-            for (int j = 0; j < 4; j++) put_rlwe(g.packing.data() + ((size_t)l * 4 + j) * 2 * kPoly, v[j]);
-        }
-        upload_keys();
-        g.pack = &autokey;
+    // keyMap[N/2^l + 1], l = 0..log2 r - 1, four RLWEs each
+    bool changed = false;
+    for (int l = 0; l < log2i(r); l++) {
+        const std::vector<RlweCiphertext>& v = autokey.keyMap.at(kPoly / (1 << l) + 1);
+        for (int j = 0; j < 4; j++) changed |= gather_rlwe(g.packing.data() + ((size_t)l * 4 + j) * 2 * kPoly, v[j]);
     }
+    upload_keys(changed);
     std::vector<uint64_t> in((size_t)r * 2 * kPoly), out(2 * kPoly);
     for (int j = 0; j < r; j++) put_rlwe(in.data() + (size_t)j * 2 * kPoly, rlwes[j]);
     check("kspir_packing_rlwes", kspir_packing_rlwes(g.ctx, 0, in.data(), out.data()));
     get_rlwe(result, out.data());
     result.setIsNtt(false);
+    // rlwes left as the reference's packing tree leaves them (answer.cpp:821-828)
+    for (int j = 0; j < r; j++) {
+        get_rlwe(rlwes[j], in.data() + (size_t)j * 2 * kPoly);
+        rlwes[j].setIsNtt(false);
+    }
+}
+
+// Not a reference function: forgets the resident database fingerprint, the
+// permutations and the key words, so the next call uploads them again (for a
+// caller that edited a few datacrt words in place).
+extern "C" void kspir_dropin_invalidate(void) {
+    g.db = nullptr;
+    g.db_sample.clear();
+    g.perms.clear();
+    g.keys_uploaded = false;
 }

@@ -59,10 +59,16 @@ struct ScanCfg {
     static_assert(RPL >= 2 && CPL >= 1, "N1 must be in [64, 256]");
 };
 
+// Failure injection for the tests of the bounded waits (kspir_debug_scan_fault):
+// `limit_ns` replaces the 2 s limit of every wait, and CTA 0's producer
+// issues no copy for its local item `skip` (-1: none), so the consumer of that
+// stage waits for bytes that never come, gives up after limit_ns, records the
+// error and stops; the producer then gives up waiting for the stage to be
+// released, and drains the copies it did issue before the CTA exits.
 template <int N1>
 __global__ void __launch_bounds__(ScanCfg<N1>::THREADS, 1)
     k_scan(const uint64_t* __restrict__ db, const uint64_t* __restrict__ cbuf, uint32_t* __restrict__ sout,
-           int R, int* __restrict__ err) {
+           int R, int* __restrict__ err, uint64_t limit_ns, long skip) {
     using C = ScanCfg<N1>;
     extern __shared__ __align__(128) uint8_t smem[];
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + C::NST * C::STAGE);
@@ -85,16 +91,19 @@ __global__ void __launch_bounds__(ScanCfg<N1>::THREADS, 1)
         // producer
         if (lane == 0) {
             const uint64_t pol_db = l2_policy_evict_first(), pol_cb = l2_policy_evict_last();
+            const long skip_j = blockIdx.x == 0 ? skip : -1;
             long issued = 0;
             for (long j = 0; j < nloc; j++) {
                 const int s = (int)(j % C::NST);
                 if (j >= C::NST) {
                     const uint32_t par = (uint32_t)((j / C::NST - 1) & 1);
-                    if (!mbar_wait_bounded(&empty[s], par, kWaitLimitNs)) {
+                    if (!mbar_wait_bounded(&empty[s], par, limit_ns)) {
                         atomicOr(err, 1);
                         break;
                     }
                 }
+                issued = j + 1;
+                if (j == skip_j) continue;   // injected failure: nothing arrives on full[s]
                 const long it = blockIdx.x + j * gridDim.x;
                 const long r = it / kN, z = it % kN;
                 uint8_t* st = smem + (size_t)s * C::STAGE;
@@ -103,12 +112,11 @@ __global__ void __launch_bounds__(ScanCfg<N1>::THREADS, 1)
                 // cipherbuf is read again for every sub-database (evict last)
                 bulk_g2s_hint(st, db + ((size_t)r * kN + z) * (kN / 2), C::SLAB, &full[s], pol_db);
                 bulk_g2s_hint(st + C::SLAB, cbuf + (size_t)z * 2 * N1, C::QSLAB, &full[s], pol_cb);
-                issued = j + 1;
             }
             // never leave the CTA with copies in flight into its shared memory
             const long first = issued > C::NST ? issued - C::NST : 0;
             for (long j = first; j < issued; j++)
-                if (!mbar_wait_bounded(&full[j % C::NST], (uint32_t)((j / C::NST) & 1), kWaitLimitNs))
+                if (j != skip_j && !mbar_wait_bounded(&full[j % C::NST], (uint32_t)((j / C::NST) & 1), limit_ns))
                     atomicOr(err, 4);
         }
         return;
@@ -119,7 +127,7 @@ __global__ void __launch_bounds__(ScanCfg<N1>::THREADS, 1)
     const int lc = lane & 7;     // chunk lane 0..7
     for (long j = warp; j < nloc; j += C::CONS) {
         const int s = (int)(j % C::NST);
-        if (!mbar_wait_bounded(&full[s], (uint32_t)((j / C::NST) & 1), kWaitLimitNs)) {
+        if (!mbar_wait_bounded(&full[s], (uint32_t)((j / C::NST) & 1), limit_ns)) {
             atomicOr(err, 2);
             break;
         }

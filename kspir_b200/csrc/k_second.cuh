@@ -381,15 +381,19 @@ __global__ void __launch_bounds__(kNttThreads) k_pack_split_fwd(const uint32_t* 
     }
 }
 
+// c2out (or null): the reference's packingRLWEs leaves c2 = X^I c + r of the
+// merge of (j, I + j) in rlwes[I + j] (answer.cpp:727-731, 821-828); the
+// staged entry point returns it there, as [r][comp][ch][N] residues.
 template <int ELL>
 __global__ void __launch_bounds__(kNttThreads) k_pack_split_inv(const uint32_t* __restrict__ in,
                                                                 const uint32_t* __restrict__ part,
                                                                 uint32_t* __restrict__ out, int I, NttTables tabs,
-                                                                Batch bt) {
+                                                                Batch bt, uint32_t* __restrict__ c2out) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
     in = shifted(in, ws_off(bt));
     part = shifted(part, ws_off(bt));
     out = shifted(out, ws_off(bt));
+    c2out = shifted(c2out, ws_off(bt));
     uint2* tws = reinterpret_cast<uint2*>(smem_raw);
     uint32_t* S = reinterpret_cast<uint32_t*>(smem_raw + kN * 8);
     const int comp = blockIdx.x & 1, ch = (blockIdx.x >> 1) & 1, j = blockIdx.x >> 2;
@@ -418,6 +422,7 @@ __global__ void __launch_bounds__(kNttThreads) k_pack_split_inv(const uint32_t* 
         const int s = k - I;
         const uint32_t sh = s >= 0 ? __ldcg(cc + s) : negmod(__ldcg(cc + s + kN), q);
         c2[it] = addmod(sh, __ldcg(r0 + (comp * 2 + ch) * kN + k), q);
+        if (c2out) c2out[((size_t)(I + j) * 4 + comp * 2 + ch) * kN + k] = c2[it];
     }
     cta_ntt_inverse(S, tws, ch);
 #pragma unroll

@@ -261,6 +261,11 @@ struct kspir_ctx {
     long answers = 0;         // queries of those launches
     long launches = 0;        // kernels launched by them
     int last_slot = -1;
+    // failure injection of the tests (kspir_debug_scan_fault): the limit of
+    // every bounded wait of the database scan, and a local item of CTA 0 whose
+    // copy the next CUDA-core scan does not issue (-1: none)
+    uint64_t wait_limit_ns = kWaitLimitNs;
+    long scan_skip = -1;
     std::mutex mu;            // serialises enqueues from several host threads
 };
 
@@ -629,11 +634,13 @@ void enqueue_scan(kspir_ctx* c, int slot0, int nq, int kind, cudaStream_t st) {
             switch (c->N1) {
 #define KS_SCAN(n)                                                                                           \
     case n:                                                                                                  \
-        k_scan<n><<<c->nsm, ScanCfg<n>::THREADS, ScanCfg<n>::SMEM, st>>>(c->db, w.cipherbuf, w.sout, R, w.err); \
+        k_scan<n><<<c->nsm, ScanCfg<n>::THREADS, ScanCfg<n>::SMEM, st>>>(c->db, w.cipherbuf, w.sout, R, w.err, \
+                                                                         c->wait_limit_ns, c->scan_skip);        \
         break;
                 KS_SCAN(64) KS_SCAN(128) KS_SCAN(256)
 #undef KS_SCAN
             }
+            c->scan_skip = -1;   // an injected failure applies to one scan launch
         }
         return;
     }
@@ -667,7 +674,9 @@ void enqueue_ext(kspir_ctx* c, int slot0, int nq, int count, const uint32_t* ini
            (const uint32_t*)c->keys0.rgsw, init, w.ext, coef_out, c->ntabs, c->gad.ext, batch_of(c, slot0));
 }
 
-void enqueue_packing(kspir_ctx* c, int slot0, int nq, cudaStream_t st) {
+// c2out (or null; split kernels only): receives each merge's X^I c + r, the
+// words the reference's packingRLWEs leaves in rlwes[I + j]
+void enqueue_packing(kspir_ctx* c, int slot0, int nq, cudaStream_t st, uint32_t* c2out = nullptr) {
     const Workspace& w = c->ws0;
     const Batch bt = batch_of(c, slot0);
     const int pe = c->gad.pack.ell;
@@ -681,7 +690,7 @@ void enqueue_packing(kspir_ctx* c, int slot0, int nq, cudaStream_t st) {
             launch(c, true, k_pack_split_fwd<4>, dim3(I * 2 * 5, nq), kNttThreads, kPackSplitSmem, st, cur, w.pkpart, key, I,
                    ginv, c->ntabs, c->gad.pack, bt);
             launch(c, true, k_pack_split_inv<4>, dim3(I * 4, nq), kNttThreads, kPackSplitSmem, st, cur,
-                   (const uint32_t*)w.pkpart, out, I, c->ntabs, bt);
+                   (const uint32_t*)w.pkpart, out, I, c->ntabs, bt, c2out);
         } else {                          // throughput: the whole level per CTA pair
             launch(c, false, k_pack_fused<4>, dim3(I * 2, nq), kNttThreads, kPackSmem, st, cur, out, key, I, ginv, c->ntabs,
                    c->gad.pack, bt);
@@ -1594,6 +1603,14 @@ int kspir_sync(kspir_ctx* c) {
     return finish(c, 0, c->p.max_inflight);
 }
 
+int kspir_debug_scan_fault(kspir_ctx* c, int64_t wait_limit_ns, long skip_item) {
+    if (!c || skip_item < -1) return KSPIR_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->wait_limit_ns = wait_limit_ns > 0 ? (uint64_t)wait_limit_ns : kWaitLimitNs;
+    c->scan_skip = skip_item;
+    return KSPIR_OK;
+}
+
 int kspir_answer(kspir_ctx* c, int client, const uint64_t* query, uint64_t* response) {
     int rc = check_ready(c, client);
     if (rc) return rc;
@@ -1819,12 +1836,13 @@ int kspir_external_product(kspir_ctx* c, int client, uint64_t* result, uint64_t*
     return finish(c, 0, 1);
 }
 
-int kspir_packing_rlwes(kspir_ctx* c, int client, const uint64_t* rlwes, uint64_t* response) {
+int kspir_packing_rlwes(kspir_ctx* c, int client, uint64_t* rlwes, uint64_t* response) {
     if (!c) return KSPIR_ERR_INVALID_ARG;
     int rc = check_client(c, client);
     if (rc) return rc;
     if (!rlwes || !response) return KSPIR_ERR_INVALID_ARG;
-    const size_t n = (size_t)c->p.r * 2 * kN;
+    const int R = c->p.r;
+    const size_t n = (size_t)R * 2 * kN;
     if (!canonical(rlwes, n, kCrtMod)) return set_err(c, KSPIR_ERR_INVALID_ARG, "ciphertext word not canonical");
     std::lock_guard<std::mutex> lk(c->mu);
     const Workspace w = ws_host(c, 0);
@@ -1833,11 +1851,24 @@ int kspir_packing_rlwes(kspir_ctx* c, int client, const uint64_t* rlwes, uint64_
     k_set_clients<<<1, 32, 0, st>>>(c->client_of, 0, ClientList{1, {client}});
     uint64_t* words = reinterpret_cast<uint64_t*>(c->stage32);
     KS_CUDA(c, cudaMemcpyAsync(words, rlwes, n * 8, cudaMemcpyHostToDevice, st));
-    k_split_words<<<blocks_for((long)n, 256), 256, 0, st>>>(words, w.ext, c->p.r * 2);
-    enqueue_packing(c, 0, 1, st);
+    k_split_words<<<blocks_for((long)n, 256), 256, 0, st>>>(words, w.ext, R * 2);
+    // rlwes[I + j] of every merge, as the reference leaves them (residues in
+    // the scan-output region, which the packing does not use)
+    uint32_t* c2 = w.sout;
+    enqueue_packing(c, 0, 1, st, c2);
     KS_CUDA(c, cudaGetLastError());
     KS_CUDA(c, cudaMemcpyAsync(response, c->bresp, 2 * kN * 8, cudaMemcpyDeviceToHost, st));
-    return finish(c, 0, 1);
+    if (R > 1) {
+        k_compose_words<<<blocks_for((long)(R - 1) * 2 * kN, 256), 256, 0, st>>>(c2 + 4 * kN, words + 2 * kN,
+                                                                                (R - 1) * 2);
+        KS_CUDA(c, cudaGetLastError());
+        KS_CUDA(c, cudaMemcpyAsync(rlwes + 2 * kN, words + 2 * kN, (size_t)(R - 1) * 2 * kN * 8, cudaMemcpyDeviceToHost,
+                                   st));
+    }
+    rc = finish(c, 0, 1);
+    if (rc) return rc;
+    memcpy(rlwes, response, 2 * kN * 8);   // rlwes[0] ends as the packed result
+    return KSPIR_OK;
 }
 
 int kspir_permutation_matrix(int32_t* perms, int N1) {

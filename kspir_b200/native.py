@@ -79,6 +79,7 @@ SIGNATURES = {
     "kspir_get_scan_kind": (_i, [_vp, _i]),
     "kspir_fetch_stage_slot": (_i, [_vp, _i, _i, _vp, _sz]),
     "kspir_client_key_bytes": (_sz, [_vp]),
+    "kspir_debug_scan_fault": (_i, [_vp, ctypes.c_int64, ctypes.c_long]),
     "kspir_server_create": (_i, [_vp, _vp, _vp]),
     "kspir_server_destroy": (_i, [_vp]),
     "kspir_server_register_client": (_i, [_vp, ctypes.c_int64, _vp, _vp, _vp, _vp]),
@@ -371,6 +372,11 @@ class Context:
     def sync(self):
         self._check(self.lib.kspir_sync(self._h))
 
+    def debug_scan_fault(self, wait_limit_ns: int = 0, skip_item: int = -1):
+        """Test hook (kspir_debug_scan_fault): the limit of the database scan's
+        bounded device waits, and a work item the next single-answer scan skips."""
+        self._check(self.lib.kspir_debug_scan_fault(self._h, wait_limit_ns, skip_item))
+
     def answer_batch(self, clients, queries, out: np.ndarray | None = None) -> np.ndarray:
         """Responses [n][2][N] of n queries ([n][2][2][N]) of the given client slots."""
         cl = np.ascontiguousarray(clients, dtype=np.int32).reshape(-1)
@@ -434,10 +440,14 @@ class Context:
         self._check(self.lib.kspir_external_product(self._h, client, ptr(res), ptr(fd), count))
         return res, fd
 
-    def packing(self, client: int, rlwes):
-        rl = _u64(rlwes).reshape(-1)
+    def packing(self, client: int, rlwes, rlwes_out: np.ndarray | None = None):
+        """The packed response of rlwes ([r][2][N]); rlwes_out (or None)
+        receives rlwes as the reference's packingRLWEs leaves them."""
+        rl = _u64(rlwes).reshape(-1).copy()
         out = np.empty(2 * N, dtype=np.uint64)
         self._check(self.lib.kspir_packing_rlwes(self._h, client, ptr(rl), ptr(out)))
+        if rlwes_out is not None:
+            rlwes_out.reshape(-1)[:] = rl
         return out
 
     def fetch_stage(self, stage: int, slot: int = 0) -> np.ndarray:

@@ -188,12 +188,16 @@ def external_product(first_dim, rgsw, ext=None):
     return e, fd
 
 
-def packing(rlwes, r, keys):
+def packing(rlwes, r, keys, rlwes_out=None):
+    """Packed response; rlwes_out (or None) receives rlwes as the reference's
+    packingRLWEs leaves them."""
     rl = rlwes.copy()
     resp = np.zeros(2 * N, dtype=np.uint64)
     rc = lib().ko_packing(_p(rl), r, _p(keys), _p(resp))
     if rc:
         raise RuntimeError(f"ko_packing rc={rc}")
+    if rlwes_out is not None:
+        rlwes_out.reshape(-1)[:] = rl
     return resp
 
 

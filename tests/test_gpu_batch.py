@@ -107,6 +107,29 @@ def test_batch_full_size_alone_equals_in_batch():
             assert (got5[i] == ctx.answer(int(cl[i]), queries[-5 + i])).all()
 
 
+def test_batch_128_full_size():
+    # the largest batch of the benchmark: 128 queries of 8 distinct clients at
+    # r = 16 (256 MB of records), slots 0..127 of one launch, with the scan
+    # variant the autotuner picks and with tcgen05 query tiles of 32 forced;
+    # every query equals its single answer, four of them the oracle
+    r, N1, n = 16, 128, 128
+    db = po.gen_db(181, r, N1)
+    clients = [po.gen_client(190 + i, r, N1) for i in range(8)]
+    cl = np.array([(3 * i + i // 16) % 8 for i in range(n)], dtype=np.int32)
+    queries = random_queries(18, n)
+    with make_ctx(r, N1, db, clients, max_inflight=n) as ctx:
+        alone = np.stack([ctx.answer(int(cl[i]), queries[i]) for i in range(n)])
+        tuned, _ = ctx.tune_batch(n)
+        for kind in dict.fromkeys((tuned, kb.SCAN_MMA32)):
+            ctx.set_scan_kind(n, kind)
+            got = ctx.answer_batch(cl, queries)
+            bad = [i for i in range(n) if not np.array_equal(got[i], alone[i])]
+            assert not bad, f"{kb.SCAN_NAMES[kind]}: queries {bad[:8]} differ from their single answers"
+        for i in (0, 63, 64, 127):
+            want = po.answer(db, r, N1, dict(clients[cl[i]], query=queries[i]))
+            assert np.array_equal(alone[i], want), f"query {i} against the oracle"
+
+
 def test_batch_rejects_bad_input():
     r, N1 = 2, 128
     clients = [po.gen_client(161, r, N1)]

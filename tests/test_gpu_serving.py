@@ -109,3 +109,76 @@ def test_serving_rejects_unknown_client_and_bad_query():
         out = srv.wait(srv.submit(0, keys["query"]))
     assert np.array_equal(out, po.answer(po.gen_db(231, r, N1), r, N1, keys))
     ctx.close()
+
+
+def _rolled_db(seed, r, N1):
+    """r sub-databases: one seeded sub-database, rotated by a different word
+    count in each (cheap to build at r = 64, every word canonical)."""
+    base = po.gen_db(seed, 1, N1)
+    num = base.size
+    out = np.empty(r * num, np.uint64)
+    for k in range(r):
+        out[k * num:(k + 1) * num] = np.roll(base, 4099 * k + 17)
+    return out
+
+
+def test_serving_256mb_and_1gb_resident_together():
+    # the serving configuration of the benchmark: the 256 MB (r = 16) and the
+    # 1 GB (r = 64) databases resident at once, each behind its own server,
+    # lanes of 128 queries, bursts of 1..128 arriving while other batches run,
+    # fewer key slots than clients (evictions); every response must equal the
+    # same query answered alone
+    N1 = 128
+    spec = {16: dict(lanes=2, lane_size=128, slots=3, clients=5),
+            64: dict(lanes=1, lane_size=128, slots=2, clients=3)}
+    deps = {}
+    for r, sp in spec.items():
+        db = _rolled_db(400 + r, r, N1)
+        keys = [po.gen_client(410 + 10 * r + i, r, N1) for i in range(sp["clients"])]
+        ctx = kb.Context(r, N1, max_clients=sp["slots"], max_inflight=128 * (sp["lanes"] - 1) + sp["lane_size"])
+        ctx.upload_db(db)
+        ctx.upload_perms(keys[0]["perms"])
+        srv = kb.Server(ctx, lanes=sp["lanes"], lane_size=sp["lane_size"],
+                        key_budget_bytes=sp["slots"] * ctx.lib.kspir_client_key_bytes(ctx.handle))
+        for i, c in enumerate(keys):
+            srv.register(i, c["baby"], c["giant"], c["packing"], c["rgsw"])
+        deps[r] = dict(db=db, keys=keys, ctx=ctx, srv=srv, reqs=[])
+    rng = np.random.default_rng(6)
+    pool = serving.random_queries(rng, 64)
+    total = 0
+    while total < 420:
+        r = 16 if rng.random() < 0.7 else 64
+        d = deps[r]
+        for _ in range(int(rng.integers(1, 129))):
+            cl, qi = int(rng.integers(0, spec[r]["clients"])), int(rng.integers(0, len(pool)))
+            out = np.zeros(2 * N, np.uint64)
+            d["reqs"].append((cl, qi, out, d["srv"].submit(cl, pool[qi], out=out)))
+            total += 1
+        time.sleep(0.001 * int(rng.integers(0, 6)))
+    stats = {}
+    for r, d in deps.items():
+        for _, _, _, t in d["reqs"]:
+            d["srv"].wait(t)
+        stats[r] = d["srv"].stats()
+        d["srv"].close()
+    for r, d in deps.items():
+        st = stats[r]
+        assert st["served"] == len(d["reqs"]), (r, st)
+        assert st["batches"] < st["served"], (r, st)               # arrivals were batched
+        assert st["evictions"] > 0 and st["key_uploads"] > spec[r]["clients"] - 1, (r, st)
+        # the same queries answered alone, client by client, in the same context
+        ctx = d["ctx"]
+        for cl in range(spec[r]["clients"]):
+            c = d["keys"][cl]
+            ctx.upload_client(0, c["baby"], c["giant"], c["packing"], c["rgsw"])
+            alone = {}
+            for j, (rc, qi, out, _) in enumerate(d["reqs"]):
+                if rc != cl:
+                    continue
+                if qi not in alone:
+                    alone[qi] = ctx.answer(0, pool[qi])
+                assert np.array_equal(out, alone[qi]), f"r={r} request {j}"
+        cl, qi, out, _ = d["reqs"][0]
+        want = po.answer(d["db"], r, N1, dict(d["keys"][cl], query=pool[qi]))
+        assert np.array_equal(out, want), f"r={r}: first request against the oracle"
+        ctx.close()

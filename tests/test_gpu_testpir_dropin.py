@@ -23,3 +23,16 @@ def test_unmodified_testpir_recovers_the_record_through_the_gpu():
     assert want in out.stdout, out.stdout[-2000:]
     assert "online server response costs" in out.stdout
     assert "server preprocessing costs" in out.stdout
+
+
+INPLACE = os.path.join(ROOT, "oracle", "_ref", "dropin-inplace")
+
+
+@pytest.mark.skipif(not os.path.exists(INPLACE), reason="oracle/_ref/dropin-inplace not built (needs the reference tree)")
+def test_dropin_follows_objects_rewritten_in_place():
+    # tests/dropin_inplace.cpp: the RGSW query re-keyed in place and the
+    # database rebuilt in place (same addresses) must change the answer, and
+    # packingRLWEs leaves rlwes[0] equal to the response, as the reference does
+    out = subprocess.run([INPLACE], capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stdout[-2000:] + out.stderr[-2000:]
+    assert "dropin-inplace: ok" in out.stdout

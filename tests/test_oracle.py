@@ -203,6 +203,25 @@ def test_oracle_equals_reference_live():
 
 
 @needs_ref
+@pytest.mark.parametrize("r", [1, 2, 8])
+def test_packing_leaves_rlwes_like_the_reference(r):
+    # packingRLWEs overwrites its input vector (answer.cpp:821-828): rlwes[0]
+    # ends as the response, rlwes[I + j] as X^I c + r of each merge
+    rng = np.random.default_rng(30 + r)
+    keys = rng.integers(0, po.CRTMOD, max(r.bit_length() - 1, 0) * 4 * 2 * N, dtype=np.uint64)
+    rl = rng.integers(0, po.CRTMOD, r * 2 * N, dtype=np.uint64)
+    rl[5 * 2 * N % rl.size: 5 * 2 * N % rl.size + 64] = 0   # zeros: the multConst negation quirk
+    got_rl = np.empty_like(rl)
+    got = po.packing(rl, r, keys, rlwes_out=got_rl)
+    ref_rl = rl.copy()
+    ref_resp = np.zeros(2 * N, np.uint64)
+    po.ref().ref_packing(po._p(ref_rl), r, po._p(keys), po._p(ref_resp))
+    assert (got == ref_resp).all()
+    assert (got_rl == ref_rl).all()
+    assert (got_rl[:2 * N] == got).all()
+
+
+@needs_ref
 def test_testpir_replay_known_answer():
     g = GOLDEN["testpir"]
     seed, r, N1 = g["seed"], g["r"], g["N1"]

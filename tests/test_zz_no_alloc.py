@@ -63,6 +63,27 @@ def test_noalloc_matches_context_path_twice():
         assert np.array_equal(got_fd, want_fd), f"call {call}: first_dim differs"
 
 
+def test_noalloc_full_scratch_and_oracle():
+    # count = KSPIR_NOALLOC_MAX_COUNT fills the whole static scratch and job
+    # list; every ciphertext equals the context path, and two of them the
+    # oracle's externalProduct (lwe.cpp:761-808) directly
+    torch = pytest.importorskip("torch")
+    from oracle import pyoracle as po
+    lib = native.load()
+    count = 16
+    rgsw, acc, fd = _inputs(14, count)
+    rc, got_res, got_fd = _noalloc(lib, torch, rgsw, acc, fd, count, 0)
+    assert rc == native.OK
+    want_res, want_fd = _existing(rgsw, acc, fd, count)
+    assert np.array_equal(got_res, want_res)
+    assert np.array_equal(got_fd, want_fd)
+    for j in (0, count - 1):
+        s = slice(j * 2 * N, (j + 1) * 2 * N)
+        e, f = po.external_product(fd[s], rgsw, ext=acc[s])
+        assert np.array_equal(got_res[s], e), f"ciphertext {j}: result"
+        assert np.array_equal(got_fd[s], f), f"ciphertext {j}: first_dim"
+
+
 def test_noalloc_rejects_oversize_and_bad_words():
     torch = pytest.importorskip("torch")
     lib = native.load()
