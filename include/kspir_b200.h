@@ -309,6 +309,18 @@ int kspir_fetch_stage_slot(kspir_ctx* ctx, int slot, int stage, uint64_t* out, s
  * bytes that were never requested. */
 int kspir_debug_scan_fault(kspir_ctx* ctx, int64_t wait_limit_ns, long skip_item);
 
+/* The single answer as one kernel (kspir_answer and kspir_answer_device on
+ * contexts with N1 = 128): one cooperative launch of one CTA per SM in which
+ * a 512-thread warp group runs the key switches from a dependency-ordered task
+ * queue while the other warps stream the database, so the giant steps,
+ * external products and packing merges of sub-databases already scanned
+ * overlap the scan of the rest.  Same words as the separate kernels.
+ * kspir_set_fused turns it on (1) or off (0): KSPIR_ERR_NOT_READY when the
+ * context cannot run it; the environment variable KSPIR_FUSED=1 turns it on
+ * at context creation.  kspir_get_fused: 1 on, 0 off. */
+int kspir_set_fused(kspir_ctx* ctx, int enable);
+int kspir_get_fused(const kspir_ctx* ctx);
+
 /* Bytes of one client's keys in a device key slot (for sizing max_clients
  * from an HBM budget). */
 size_t kspir_client_key_bytes(const kspir_ctx* ctx);

@@ -105,7 +105,7 @@ __device__ __forceinline__ void baby_setup(BabyRot& R, const BabyArgs& a, const 
 //   INTT_bs(-sum_j d_j[perm] * key_j) (+ auto_g(b mod bsMod) for comp 1).
 // The caller has staged the bsMod inverse twiddles into tws (unsynchronised).
 // export_inter: this CTA writes the intermediate rotation's x2.
-template <int ELL>
+template <int ELL, class Sync = CtaSync>
 __device__ __forceinline__ void baby_bs_part(const BabyRot& R, const BabyArgs& a, uint32_t* S, const uint2* tws,
                                              bool export_inter) {
     const int tid = R.tid;
@@ -128,7 +128,7 @@ __device__ __forceinline__ void baby_bs_part(const BabyRot& R, const BabyArgs& a
         for (int it = 0; it < kPerThread; it++)
             S[pidx(tid) + it * kPadStep] = negmod(reduce64(acc[it], cb.q, cb.barrett), cb.q);
     }
-    cta_ntt_inverse(S, tws, CH_BS);
+    cta_ntt_inverse<Sync>(S, tws, CH_BS);
 
     if (R.comp == 1) {
         // x2b += auto_g(b mod bsMod)   (automorphic_rns, twosteps.cpp:1045-1048)
@@ -157,16 +157,16 @@ __device__ __forceinline__ void baby_bs_part(const BabyRot& R, const BabyArgs& a
 // Prime ch of the rotation: NTT_ch(x2) from S (in place), the crt
 // multiply-accumulate, the modswitch, and the cipherbuf store.  Starts with
 // a barrier (x2 complete, tws free) and stages the forward twiddles itself.
-template <int ELL>
+template <int ELL, class Sync = CtaSync>
 __device__ __forceinline__ void baby_crt_part(const BabyRot& R, const BabyArgs& a, uint32_t* S, uint2* tws,
                                               const NttTables& tabs, int ch) {
     const int tid = R.tid, comp = R.comp;
     const uint16_t* __restrict__ sig = a.sigma + (size_t)R.ki * kN;
     uint32_t* cb32 = reinterpret_cast<uint32_t*>(shifted(a.cipherbuf, R.wo));
     uint32_t* inter_out = shifted(comp == 0 ? a.interA : a.interB, R.wo);
-    __syncthreads();   // x2 complete and the previous twiddles no longer read
+    Sync::sync();   // x2 complete and the previous twiddles no longer read
     stage_twiddles(tws, tabs, ch, NTT_FWD);
-    cta_ntt_forward(S, tws, ch);   // NTT_ch(x2), x2 < bsMod < q
+    cta_ntt_forward<Sync>(S, tws, ch);   // NTT_ch(x2), x2 < bsMod < q
 
     const ChanConst cc = c_dev.ch[ch];
     int pk[kPerThread];

@@ -13,12 +13,8 @@ namespace kspir {
 //  * query b as residues (its crt transform feeds the hoisted b terms);
 //  * the RNS modswitch of the query itself, (x_crt - x_bs) * bsMod^-1 mod
 //    crtMod (twosteps.cpp:1073-1086), as residues before its transform.
-__global__ void k_query_prep(Workspace ws, GadgetBsgs g, Batch bt) {
-    pdl_launch_dependents();
-    pdl_wait();
-    ws = ws_at(ws, bt);
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= kN) return;
+// k < N; ws is already the query's workspace slot.
+__device__ __forceinline__ void query_prep_one(const Workspace& ws, const GadgetBsgs& g, int k) {
     const uint64_t a_crt = ws.q64[k], b_crt = ws.q64[kN + k];
     const uint32_t a_bs = (uint32_t)ws.q64[2 * kN + k], b_bs = (uint32_t)ws.q64[3 * kN + k];
     int32_t dig[kMaxEll];
@@ -41,15 +37,18 @@ __global__ void k_query_prep(Workspace ws, GadgetBsgs g, Batch bt) {
     ws.col0[3 * kN + k] = shoup_mul(submod(bq2, b_bs, kQ2), c2.bsinv, c2.bsinv_p, kQ2);
 }
 
-// Digits of the intermediate rotation (evalAutoSRNSSecond, twosteps.cpp:1109-1120):
-// decompose_bsgs of its coefficient-form a (crt residues composed to the
-// canonical word) and its bsMod part.
-__global__ void k_inter_decomp(Workspace ws, GadgetBsgs g, Batch bt) {
+__global__ void k_query_prep(Workspace ws, GadgetBsgs g, Batch bt) {
     pdl_launch_dependents();
     pdl_wait();
     ws = ws_at(ws, bt);
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= kN) return;
+    if (k < kN) query_prep_one(ws, g, k);
+}
+
+// Digits of the intermediate rotation (evalAutoSRNSSecond, twosteps.cpp:1109-1120):
+// decompose_bsgs of its coefficient-form a (crt residues composed to the
+// canonical word) and its bsMod part.
+__device__ __forceinline__ void inter_decomp_one(const Workspace& ws, const GadgetBsgs& g, int k) {
     const uint64_t a_crt = crt_compose_res(__ldcg(ws.inter_acoef + k), __ldcg(ws.inter_acoef + kN + k));
     const uint32_t a_bs = __ldcg(ws.inter_bs + k);
     int32_t dig[kMaxEll];
@@ -59,6 +58,14 @@ __global__ void k_inter_decomp(Workspace ws, GadgetBsgs g, Batch bt) {
         ws.dig1[(j * 3 + CH_Q2) * kN + k] = signed_to_res(dig[j], kQ2);
         ws.dig1[(j * 3 + CH_BS) * kN + k] = signed_to_res(dig[j], kBsMod);
     }
+}
+
+__global__ void k_inter_decomp(Workspace ws, GadgetBsgs g, Batch bt) {
+    pdl_launch_dependents();
+    pdl_wait();
+    ws = ws_at(ws, bt);
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < kN) inter_decomp_one(ws, g, k);
 }
 
 }  // namespace kspir

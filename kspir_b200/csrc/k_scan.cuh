@@ -59,6 +59,69 @@ struct ScanCfg {
     static_assert(RPL >= 2 && CPL >= 1, "N1 must be in [64, 256]");
 };
 
+// The multiply-accumulate of one work item by one warp: the slab DB[r][z]
+// and cipherbuf row z in shared memory at `st` -> the lane's 4 * RPL partial
+// sums v[o], o = 4 * rr + comp_ch (0 = a q1 (lo), 1 = a q2 (hi), 2 = b q1,
+// 3 = b q2) of rows lr + 4 rr.
+template <int N1>
+__device__ __forceinline__ void scan_item_mac(const uint8_t* st, int lane, uint64_t* v) {
+    using C = ScanCfg<N1>;
+    const int lr = lane >> 3;    // row lane 0..3
+    const int lc = lane & 7;     // chunk lane 0..7
+    const uint4* D4 = reinterpret_cast<const uint4*>(st);             // [N2][CHUNKS] chunks of 2 words
+    const uint4* Q4 = reinterpret_cast<const uint4*>(st + C::SLAB);   // [N1] (a_k, b_k) pairs
+#pragma unroll
+    for (int o = 0; o < C::NV; o++) v[o] = 0;
+#pragma unroll
+    for (int cc = 0; cc < C::CPL; cc++) {
+        const int kc = lc + 8 * cc;                   // chunk = words 2kc, 2kc+1
+        const uint4 qa = Q4[2 * kc];                  // (a_2kc, b_2kc)
+        const uint4 qb = Q4[2 * kc + 1];              // (a_2kc+1, b_2kc+1)
+#pragma unroll
+        for (int rr = 0; rr < C::RPL; rr++) {
+            const uint4 w = D4[(lr + 4 * rr) * C::CHUNKS + kc];
+            mad_wide(v[4 * rr + 0], w.x, qa.x);
+            mad_wide(v[4 * rr + 0], w.z, qb.x);
+            mad_wide(v[4 * rr + 1], w.y, qa.y);
+            mad_wide(v[4 * rr + 1], w.w, qb.y);
+            mad_wide(v[4 * rr + 2], w.x, qa.z);
+            mad_wide(v[4 * rr + 2], w.z, qb.z);
+            mad_wide(v[4 * rr + 3], w.y, qa.w);
+            mad_wide(v[4 * rr + 3], w.w, qb.w);
+        }
+    }
+}
+
+// Transpose-reduce over the chunk lanes (offsets 4, 2, 1: at each level the
+// lane keeps the half of its values selected by its lane bit and adds the
+// partner's copy of that half), then the residues of the lane's finished
+// outputs into the scan output of sub-database r, slot z.
+template <int N1>
+__device__ __forceinline__ void scan_item_store(uint64_t* v, int lane, int r, int z, int R, uint32_t* sout) {
+    using C = ScanCfg<N1>;
+    const int lr = lane >> 3, lc = lane & 7;
+#pragma unroll
+    for (int lvl = 0; lvl < 3; lvl++) {
+        const int d = 4 >> lvl;
+        const int hs = C::NV >> (lvl + 1);
+        const bool upper = (lc & d) != 0;
+#pragma unroll
+        for (int i = 0; i < hs; i++) {
+            const uint64_t send = upper ? v[i] : v[i + hs];
+            const uint64_t keep = upper ? v[i + hs] : v[i];
+            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, d);
+        }
+    }
+    // lane lc now holds outputs o = NOUT * lc + t
+#pragma unroll
+    for (int t = 0; t < C::NOUT; t++) {
+        const int o = C::NOUT * lc + t;
+        const int i = lr + 4 * (o >> 2), cv = o & 3;
+        const uint32_t res = (cv & 1) ? mod_q2(v[t]) : mod_q1(v[t]);
+        sout[sout_idx(r * C::N2 + i, cv, z, R * C::N2)] = res;
+    }
+}
+
 // Failure injection for the tests of the bounded waits (kspir_debug_scan_fault):
 // `limit_ns` replaces the 2 s limit of every wait, and CTA 0's producer
 // issues no copy for its local item `skip` (-1: none), so the consumer of that
@@ -123,66 +186,18 @@ __global__ void __launch_bounds__(ScanCfg<N1>::THREADS, 1)
     }
 
     // consumers
-    const int lr = lane >> 3;    // row lane 0..3
-    const int lc = lane & 7;     // chunk lane 0..7
     for (long j = warp; j < nloc; j += C::CONS) {
         const int s = (int)(j % C::NST);
         if (!mbar_wait_bounded(&full[s], (uint32_t)((j / C::NST) & 1), limit_ns)) {
             atomicOr(err, 2);
             break;
         }
-        const uint8_t* st = smem + (size_t)s * C::STAGE;
-        const uint4* D4 = reinterpret_cast<const uint4*>(st);             // [N2][CHUNKS] chunks of 2 words
-        const uint4* Q4 = reinterpret_cast<const uint4*>(st + C::SLAB);   // [N1] (a_k, b_k) pairs
-        // v[o], o = 4 * rr + comp_ch: 0 = a q1 (lo), 1 = a q2 (hi), 2 = b q1, 3 = b q2
         uint64_t v[C::NV];
-#pragma unroll
-        for (int o = 0; o < C::NV; o++) v[o] = 0;
-#pragma unroll
-        for (int cc = 0; cc < C::CPL; cc++) {
-            const int kc = lc + 8 * cc;                   // chunk = words 2kc, 2kc+1
-            const uint4 qa = Q4[2 * kc];                  // (a_2kc, b_2kc)
-            const uint4 qb = Q4[2 * kc + 1];              // (a_2kc+1, b_2kc+1)
-#pragma unroll
-            for (int rr = 0; rr < C::RPL; rr++) {
-                const uint4 w = D4[(lr + 4 * rr) * C::CHUNKS + kc];
-                mad_wide(v[4 * rr + 0], w.x, qa.x);
-                mad_wide(v[4 * rr + 0], w.z, qb.x);
-                mad_wide(v[4 * rr + 1], w.y, qa.y);
-                mad_wide(v[4 * rr + 1], w.w, qb.y);
-                mad_wide(v[4 * rr + 2], w.x, qa.z);
-                mad_wide(v[4 * rr + 2], w.z, qb.z);
-                mad_wide(v[4 * rr + 3], w.y, qa.w);
-                mad_wide(v[4 * rr + 3], w.w, qb.w);
-            }
-        }
+        scan_item_mac<N1>(smem + (size_t)s * C::STAGE, lane, v);
         __syncwarp();
         if (lane == 0) mbar_arrive(&empty[s]);
-        // transpose-reduce over the chunk lanes (offsets 4, 2, 1): at each level
-        // the lane keeps the half of its values selected by its lane bit and
-        // adds the partner's copy of that half
-#pragma unroll
-        for (int lvl = 0; lvl < 3; lvl++) {
-            const int d = 4 >> lvl;
-            const int hs = C::NV >> (lvl + 1);
-            const bool upper = (lc & d) != 0;
-#pragma unroll
-            for (int i = 0; i < hs; i++) {
-                const uint64_t send = upper ? v[i] : v[i + hs];
-                const uint64_t keep = upper ? v[i + hs] : v[i];
-                v[i] = keep + __shfl_xor_sync(0xffffffffu, send, d);
-            }
-        }
-        // lane lc now holds outputs o = NOUT * lc + t
         const long it = blockIdx.x + j * gridDim.x;
-        const long r = it / kN, z = it % kN;
-#pragma unroll
-        for (int t = 0; t < C::NOUT; t++) {
-            const int o = C::NOUT * lc + t;
-            const int i = lr + 4 * (o >> 2), cv = o & 3;
-            const uint32_t res = (cv & 1) ? mod_q2(v[t]) : mod_q1(v[t]);
-            sout[sout_idx((int)r * C::N2 + i, cv, (int)z, R * C::N2)] = res;
-        }
+        scan_item_store<N1>(v, lane, (int)(it / kN), (int)(it % kN), R, sout);
     }
 }
 

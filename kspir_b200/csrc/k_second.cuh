@@ -308,19 +308,17 @@ __global__ void __launch_bounds__(kNttThreads) k_pack_fused(const uint32_t* __re
 constexpr int kPackPartPolys = 2 * 5 * 2;   // per pair: [prime][ELL + 1][comp]
 constexpr int kPackSplitSmem = kN * 8 + kPadN * 4;
 
-template <int ELL>
-__global__ void __launch_bounds__(kNttThreads) k_pack_split_fwd(const uint32_t* __restrict__ in,
-                                                                uint32_t* __restrict__ part,
-                                                                const uint32_t* __restrict__ key, int I,
-                                                                uint32_t ginv, NttTables tabs, GadgetB g, Batch bt) {
+// One split forward task, pair j, prime ch, digit d (d = ELL: temp.b); in,
+// part and key already point at the query's workspace and key slot.  Shared
+// with the fused answer kernel (Sync = its named barrier).
+template <int ELL, class Sync>
+__device__ __forceinline__ void pack_split_fwd_body(const uint32_t* __restrict__ in, uint32_t* __restrict__ part,
+                                                    const uint32_t* __restrict__ key, int I, uint32_t ginv,
+                                                    const NttTables& tabs, const GadgetB& g, int j, int ch, int d,
+                                                    uint8_t* smem_raw) {
     static_assert(2 * (ELL + 1) * 2 <= kPackPartPolys, "term buffer");
-    extern __shared__ __align__(16) uint8_t smem_raw[];
-    in = shifted(in, ws_off(bt));
-    part = shifted(part, ws_off(bt));
-    key = shifted(key, key_off(bt));
     uint2* tws = reinterpret_cast<uint2*>(smem_raw);
     uint32_t* S = reinterpret_cast<uint32_t*>(smem_raw + kN * 8);
-    const int d = blockIdx.x % (ELL + 1), ch = (blockIdx.x / (ELL + 1)) & 1, j = blockIdx.x / (ELL + 1) / 2;
     const int tid = threadIdx.x;
     const uint32_t* r0 = in + (size_t)j * 4 * kN;
     const uint32_t* cc = in + (size_t)(I + j) * 4 * kN;
@@ -366,7 +364,7 @@ __global__ void __launch_bounds__(kNttThreads) k_pack_split_fwd(const uint32_t* 
         }
         S[pidx(tid) + it * kPadStep] = v;
     }
-    cta_ntt_forward(S, tws, ch);
+    cta_ntt_forward<Sync>(S, tws, ch);
     uint32_t* pa = part + (((size_t)j * 2 + ch) * (ELL + 1) + d) * 2 * kN;
 #pragma unroll
     for (int it = 0; it < kPerThreadG; it++) {
@@ -381,22 +379,27 @@ __global__ void __launch_bounds__(kNttThreads) k_pack_split_fwd(const uint32_t* 
     }
 }
 
+template <int ELL>
+__global__ void __launch_bounds__(kNttThreads) k_pack_split_fwd(const uint32_t* __restrict__ in,
+                                                                uint32_t* __restrict__ part,
+                                                                const uint32_t* __restrict__ key, int I,
+                                                                uint32_t ginv, NttTables tabs, GadgetB g, Batch bt) {
+    extern __shared__ __align__(16) uint8_t smem_raw[];
+    const int d = blockIdx.x % (ELL + 1), ch = (blockIdx.x / (ELL + 1)) & 1, j = blockIdx.x / (ELL + 1) / 2;
+    pack_split_fwd_body<ELL, CtaSync>(shifted(in, ws_off(bt)), shifted(part, ws_off(bt)), shifted(key, key_off(bt)), I,
+                                      ginv, tabs, g, j, ch, d, smem_raw);
+}
+
 // c2out (or null): the reference's packingRLWEs leaves c2 = X^I c + r of the
 // merge of (j, I + j) in rlwes[I + j] (answer.cpp:727-731, 821-828); the
 // staged entry point returns it there, as [r][comp][ch][N] residues.
-template <int ELL>
-__global__ void __launch_bounds__(kNttThreads) k_pack_split_inv(const uint32_t* __restrict__ in,
-                                                                const uint32_t* __restrict__ part,
-                                                                uint32_t* __restrict__ out, int I, NttTables tabs,
-                                                                Batch bt, uint32_t* __restrict__ c2out) {
-    extern __shared__ __align__(16) uint8_t smem_raw[];
-    in = shifted(in, ws_off(bt));
-    part = shifted(part, ws_off(bt));
-    out = shifted(out, ws_off(bt));
-    c2out = shifted(c2out, ws_off(bt));
+template <int ELL, class Sync>
+__device__ __forceinline__ void pack_split_inv_body(const uint32_t* __restrict__ in, const uint32_t* __restrict__ part,
+                                                    uint32_t* __restrict__ out, int I, const NttTables& tabs, int j,
+                                                    int ch, int comp, uint32_t* __restrict__ c2out,
+                                                    uint8_t* smem_raw) {
     uint2* tws = reinterpret_cast<uint2*>(smem_raw);
     uint32_t* S = reinterpret_cast<uint32_t*>(smem_raw + kN * 8);
-    const int comp = blockIdx.x & 1, ch = (blockIdx.x >> 1) & 1, j = blockIdx.x >> 2;
     const int tid = threadIdx.x;
     const uint32_t q = c_dev.ch[ch].q;
     pdl_launch_dependents();
@@ -424,11 +427,85 @@ __global__ void __launch_bounds__(kNttThreads) k_pack_split_inv(const uint32_t* 
         c2[it] = addmod(sh, __ldcg(r0 + (comp * 2 + ch) * kN + k), q);
         if (c2out) c2out[((size_t)(I + j) * 4 + comp * 2 + ch) * kN + k] = c2[it];
     }
-    cta_ntt_inverse(S, tws, ch);
+    cta_ntt_inverse<Sync>(S, tws, ch);
 #pragma unroll
     for (int it = 0; it < kPerThreadG; it++) {
         const int k = tid + it * kNttThreads;
         out[((size_t)j * 4 + comp * 2 + ch) * kN + k] = addmod(S[pidx(tid) + it * kPadStep], c2[it], q);
+    }
+}
+
+template <int ELL>
+__global__ void __launch_bounds__(kNttThreads) k_pack_split_inv(const uint32_t* __restrict__ in,
+                                                                const uint32_t* __restrict__ part,
+                                                                uint32_t* __restrict__ out, int I, NttTables tabs,
+                                                                Batch bt, uint32_t* __restrict__ c2out) {
+    extern __shared__ __align__(16) uint8_t smem_raw[];
+    const int comp = blockIdx.x & 1, ch = (blockIdx.x >> 1) & 1, j = blockIdx.x >> 2;
+    pack_split_inv_body<ELL, CtaSync>(shifted(in, ws_off(bt)), shifted(part, ws_off(bt)), shifted(out, ws_off(bt)), I,
+                                      tabs, j, ch, comp, shifted(c2out, ws_off(bt)), smem_raw);
+}
+
+// The external product after first_dim is in coefficient form in P[comp * 2 +
+// prime] (both primes, as the decomposition needs the composed word): signed
+// digits of a and b, their transforms on prime ch, init (or 0) + sum_row
+// row * rgsw[row], inverse transform, into ext [comp][ch][N].  rgsw, init and
+// ext point at the query's key slot and its polynomial r.
+template <int ELL, class Sync>
+__device__ __forceinline__ void ext_tail(uint32_t* P, uint2* tws, const uint32_t* __restrict__ rgsw,
+                                         const uint32_t* __restrict__ init, uint32_t* __restrict__ ext,
+                                         const NttTables& tabs, const GadgetS& g, int ch) {
+    const int tid = threadIdx.x;
+    // signed digits of a and b (rows comp * ELL + t), residues of this prime
+    uint32_t dres[kPerThreadG][2 * ELL];
+#pragma unroll
+    for (int it = 0; it < kPerThreadG; it++) {
+#pragma unroll
+        for (int comp = 0; comp < 2; comp++) {
+            int32_t dig[kMaxEll];
+            const int pk = pidx(tid) + it * kPadStep;
+            decompose_signed(crt_compose_res(P[(comp * 2 + 0) * kPadN + pk], P[(comp * 2 + 1) * kPadN + pk]), kCrtMod, g,
+                             dig);
+#pragma unroll
+            for (int t = 0; t < ELL; t++) dres[it][comp * ELL + t] = signed_to_res(dig[t], ch ? kQ2 : kQ1);
+        }
+    }
+    Sync::sync();
+#pragma unroll
+    for (int it = 0; it < kPerThreadG; it++)
+#pragma unroll
+        for (int row = 0; row < 2 * ELL; row++) P[row * kPadN + pidx(tid) + it * kPadStep] = dres[it][row];
+    stage_twiddles(tws, tabs, ch, NTT_FWD);
+    cta_ntt_forward_m<2 * ELL, Sync>(P, kPadN, tws, ch);
+    const ChanConst cq = c_dev.ch[ch];
+    uint32_t outv[kPerThreadG][2];
+#pragma unroll
+    for (int it = 0; it < kPerThreadG; it++) {
+        const int k = tid + it * kNttThreads;
+#pragma unroll
+        for (int comp = 0; comp < 2; comp++) {
+            uint64_t s = 0;
+#pragma unroll
+            for (int row = 0; row < 2 * ELL; row++)
+                mad_wide(s, P[row * kPadN + pidx(tid) + it * kPadStep], __ldg(rgsw + ((row * 2 + comp) * 2 + ch) * kN + k));
+            const uint32_t m = mod_crt(s, ch);
+            outv[it][comp] = init ? addmod(__ldcg(init + (size_t)(comp * 2 + ch) * kN + k), m, cq.q) : m;
+        }
+    }
+#pragma unroll
+    for (int it = 0; it < kPerThreadG; it++) {
+        const int pk = pidx(tid) + it * kPadStep;
+        P[pk] = outv[it][0];        // only this thread reads this slot of rows 0, 1
+        P[kPadN + pk] = outv[it][1];
+    }
+    stage_twiddles(tws, tabs, ch, NTT_INV);   // the forward transforms ended with a barrier
+    cta_ntt_inverse_m<2, Sync>(P, kPadN, tws, ch);
+#pragma unroll
+    for (int it = 0; it < kPerThreadG; it++) {
+        const int k = tid + it * kNttThreads;
+#pragma unroll
+        for (int comp = 0; comp < 2; comp++)
+            ext[(size_t)(comp * 2 + ch) * kN + k] = P[comp * kPadN + pidx(tid) + it * kPadStep];
     }
 }
 
@@ -457,7 +534,6 @@ __global__ void __launch_bounds__(kNttThreads) k_ext_fused(const uint32_t* __res
     uint2* tws = reinterpret_cast<uint2*>(smem_raw);
     uint32_t* P = reinterpret_cast<uint32_t*>(smem_raw + kN * 8);   // [4][N]
     const int r = blockIdx.x >> 1, ch = blockIdx.x & 1;
-    const int tid = threadIdx.x;
     const uint32_t* fd = first_dim + (size_t)r * 4 * kN;          // [comp][prime][N]
     pdl_launch_dependents();
     // first_dim to coefficient form, all four polynomials (P[comp * 2 + prime])
@@ -476,57 +552,8 @@ __global__ void __launch_bounds__(kNttThreads) k_ext_fused(const uint32_t* __res
 #pragma unroll
         for (int i = 0; i < 4; i++) poly_from_smem(coef_out + ((size_t)r * 4 + i) * kN, P + i * kPadN);
     }
-    // signed digits of a and b (rows comp * ELL + t), residues of this prime
-    uint32_t dres[kPerThreadG][2 * ELL];
-#pragma unroll
-    for (int it = 0; it < kPerThreadG; it++) {
-#pragma unroll
-        for (int comp = 0; comp < 2; comp++) {
-            int32_t dig[kMaxEll];
-            const int pk = pidx(tid) + it * kPadStep;
-            decompose_signed(crt_compose_res(P[(comp * 2 + 0) * kPadN + pk], P[(comp * 2 + 1) * kPadN + pk]), kCrtMod, g,
-                             dig);
-#pragma unroll
-            for (int t = 0; t < ELL; t++) dres[it][comp * ELL + t] = signed_to_res(dig[t], ch ? kQ2 : kQ1);
-        }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int it = 0; it < kPerThreadG; it++)
-#pragma unroll
-        for (int row = 0; row < 2 * ELL; row++) P[row * kPadN + pidx(tid) + it * kPadStep] = dres[it][row];
-    stage_twiddles(tws, tabs, ch, NTT_FWD);
-    cta_ntt_forward_m<2 * ELL>(P, kPadN, tws, ch);
-    const ChanConst cq = c_dev.ch[ch];
-    uint32_t outv[kPerThreadG][2];
-#pragma unroll
-    for (int it = 0; it < kPerThreadG; it++) {
-        const int k = tid + it * kNttThreads;
-#pragma unroll
-        for (int comp = 0; comp < 2; comp++) {
-            uint64_t s = 0;
-#pragma unroll
-            for (int row = 0; row < 2 * ELL; row++)
-                mad_wide(s, P[row * kPadN + pidx(tid) + it * kPadStep], __ldg(rgsw + ((row * 2 + comp) * 2 + ch) * kN + k));
-            const uint32_t m = mod_crt(s, ch);
-            outv[it][comp] = init ? addmod(__ldcg(init + ((size_t)r * 4 + comp * 2 + ch) * kN + k), m, cq.q) : m;
-        }
-    }
-#pragma unroll
-    for (int it = 0; it < kPerThreadG; it++) {
-        const int pk = pidx(tid) + it * kPadStep;
-        P[pk] = outv[it][0];        // only this thread reads this slot of rows 0, 1
-        P[kPadN + pk] = outv[it][1];
-    }
-    stage_twiddles(tws, tabs, ch, NTT_INV);   // the forward transforms ended with a barrier
-    cta_ntt_inverse_m<2>(P, kPadN, tws, ch);
-#pragma unroll
-    for (int it = 0; it < kPerThreadG; it++) {
-        const int k = tid + it * kNttThreads;
-#pragma unroll
-        for (int comp = 0; comp < 2; comp++)
-            ext[((size_t)r * 4 + comp * 2 + ch) * kN + k] = P[comp * kPadN + pidx(tid) + it * kPadStep];
-    }
+    ext_tail<ELL, CtaSync>(P, tws, rgsw, init ? init + (size_t)r * 4 * kN : nullptr, ext + (size_t)r * 4 * kN, tabs, g,
+                           ch);
 }
 
 }  // namespace kspir

@@ -21,6 +21,20 @@ struct NttJob {
 // dynamic shared memory: 32 KiB twiddles + one padded polynomial
 constexpr int kNttJobSmem = kN * 8 + kPadN * 4;
 
+// The transform of one job whose twiddles are staged in tws (the caller
+// synchronises nothing: the transform starts with a barrier).
+template <bool INVERSE, class Sync>
+__device__ __forceinline__ void ntt_job_run(const NttJob& jb, const uint2* tws, uint32_t* s) {
+    poly_to_smem(s, jb.src);
+    if (INVERSE) cta_ntt_inverse<Sync>(s, tws, jb.ch);
+    else cta_ntt_forward<Sync>(s, tws, jb.ch);
+    if (jb.dst_stride == 1) {
+        poly_from_smem(jb.dst, s);
+    } else {
+        for (int k = threadIdx.x; k < kN; k += kNttThreads) jb.dst[(size_t)k * jb.dst_stride] = s[pidx(k)];
+    }
+}
+
 template <bool INVERSE>
 __global__ void __launch_bounds__(kNttThreads) k_ntt_jobs(const NttJob* __restrict__ jobs, NttTables tabs, Batch bt) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
@@ -32,14 +46,7 @@ __global__ void __launch_bounds__(kNttThreads) k_ntt_jobs(const NttJob* __restri
     jb.dst = shifted(jb.dst, ws_off(bt));
     stage_twiddles(tws, tabs, jb.ch, INVERSE ? NTT_INV : NTT_FWD);
     pdl_wait();
-    poly_to_smem(s, jb.src);
-    if (INVERSE) cta_ntt_inverse(s, tws, jb.ch);
-    else cta_ntt_forward(s, tws, jb.ch);
-    if (jb.dst_stride == 1) {
-        poly_from_smem(jb.dst, s);
-    } else {
-        for (int k = threadIdx.x; k < kN; k += kNttThreads) jb.dst[(size_t)k * jb.dst_stride] = s[pidx(k)];
-    }
+    ntt_job_run<INVERSE, CtaSync>(jb, tws, s);
 }
 
 // words[p][k] = canonical crtMod value of residues (res[p][0][k], res[p][1][k])

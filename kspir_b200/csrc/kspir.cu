@@ -28,6 +28,7 @@
 #include "k_scan_mma.cuh"
 #include "k_second.cuh"
 #include "k_util.cuh"
+#include "k_answer.cuh"
 #include "ntt.cuh"
 #include "pipeline.cuh"
 
@@ -266,6 +267,16 @@ struct kspir_ctx {
     // copy the next CUDA-core scan does not issue (-1: none)
     uint64_t wait_limit_ns = kWaitLimitNs;
     long scan_skip = -1;
+    // the fused single answer (k_answer.cuh): task list, counters, giant-step
+    // accumulators and per-launch device timestamps ([kTimingRing][8])
+    bool fused_ok = false;    // built for this context
+    bool fused = false;       // single answers use it
+    FaTask* fa_tasks = nullptr;
+    int fa_ntasks = 0;
+    int* fa_cnt = nullptr;
+    uint32_t* fa_acc = nullptr;
+    unsigned long long* fa_times = nullptr;
+    std::vector<char> ring_fused;
     std::mutex mu;            // serialises enqueues from several host threads
 };
 
@@ -735,15 +746,95 @@ int build_graphs(kspir_ctx* c, int slot0, int nq, bool rm, kspir_ctx::PhaseGraph
     return KSPIR_OK;
 }
 
-int enqueue_answer(kspir_ctx* c, int slot0, int nq, const int* clients, cudaStream_t st) {
+// The fused single answer of workspace slot 0 (k_answer.cuh): reset of its
+// counters, then one cooperative launch of one CTA per SM.
+FaArgs fa_args(const kspir_ctx* c, int ring_slot) {
+    FaArgs A{};
+    const Workspace& w = c->ws0;
+    A.w = w;
+    A.keys = c->keys0;
+    A.bt = batch_of(c, 0);
+    A.tabs = c->ntabs;
+    A.gad = c->gad;
+    BabyArgs a1{};
+    a1.cb_rm = 0;
+    a1.dig = w.dig0; a1.srcB = w.qbn; a1.srcBbs = w.qbbs; a1.perms = c->perms; a1.sigma = c->sigma_baby;
+    a1.cipherbuf = w.cipherbuf; a1.interA = w.interA; a1.interB = w.interB; a1.inter_bs = w.inter_bs;
+    a1.N1 = c->N1; a1.col_base = 1; a1.inter_idx = c->N1h - 2;
+    BabyArgs a2 = a1;
+    a2.dig = w.dig1; a2.srcB = w.interB; a2.srcBbs = w.inter_bs + kN;
+    a2.col_base = c->N1h; a2.inter_idx = -1;
+    A.a1 = a1;
+    A.a2 = a2;
+    A.jobs = c->jobs;
+    A.seg_q = c->seg_q;
+    A.n_q = c->n_q;
+    A.seg_inter = c->seg_inter;
+    A.seg_dig1 = c->seg_dig1;
+    A.inter_idx = c->N1h - 2;
+    A.sigma_giant = c->sigma_giant;
+    A.db = c->db;
+    A.R = c->p.r;
+    A.N1 = c->N1;
+    A.levels = c->levels;
+    A.tasks = c->fa_tasks;
+    A.ntasks = c->fa_ntasks;
+    A.cnt = c->fa_cnt;
+    A.acc = c->fa_acc;
+    A.times = c->fa_times + (size_t)ring_slot * FT_T_COUNT;
+    A.limit_ns = c->wait_limit_ns;
+    A.skip = c->scan_skip;
+    A.err = c->errs;
+    return A;
+}
+
+constexpr int kFaScanWarps = 6;
+
+int enqueue_fused(kspir_ctx* c, int client, cudaStream_t st, int ring_slot) {
+    k_fa_reset<<<1, 256, 0, st>>>(c->client_of, 0, client, c->fa_cnt, fa_counter_words(c->p.r),
+                                  c->fa_times + (size_t)ring_slot * FT_T_COUNT);
+    const FaArgs A = fa_args(c, ring_slot);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(c->nsm);
+    cfg.blockDim = dim3(FaCfg<128, kFaScanWarps>::THREADS);
+    cfg.dynamicSmemBytes = FaCfg<128, kFaScanWarps>::SMEM;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    KS_CUDA(c, cudaLaunchKernelEx(&cfg, k_answer<128, kFaScanWarps>, A));
+    c->scan_skip = -1;   // an injected failure applies to one launch
+    return KSPIR_OK;
+}
+
+// allow_fused: a single answer of slot 0 through the public single-answer
+// calls may run as the fused kernel (batches and serving lanes never do)
+int enqueue_answer(kspir_ctx* c, int slot0, int nq, const int* clients, cudaStream_t st, bool allow_fused = false) {
+    const int slot = (int)(c->enqueues % kTimingRing);
+    auto& ev = c->ring[slot];
+    if (allow_fused && c->fused && nq == 1 && slot0 == 0) {
+        c->last_kind = SCAN_CUDA;
+        cudaEventRecord(ev[0], st);
+        int rc = enqueue_fused(c, clients[0], st, slot);
+        if (rc) return rc;
+        for (int i = 1; i < 6; i++) cudaEventRecord(ev[i], st);
+        c->ring_nq[slot] = 1;
+        c->ring_fused[slot] = 1;
+        c->enqueues++;
+        c->answers += 1;
+        c->launches += 2;
+        c->last_slot = slot;
+        return KSPIR_OK;
+    }
+    c->ring_fused[slot] = 0;
     ClientList cl;
     cl.n = nq;
     for (int i = 0; i < nq; i++) cl.id[i] = clients[i];
     k_set_clients<<<1, kMaxBatch, 0, st>>>(c->client_of, slot0, cl);
     const int kind = scan_kind_for(c, nq);
     c->last_kind = kind;
-    const int slot = (int)(c->enqueues % kTimingRing);
-    auto& ev = c->ring[slot];
     if (c->use_graphs) {
         kspir_ctx::PhaseGraphs* pg = nullptr;
         int rc = build_graphs(c, slot0, nq, kind != SCAN_CUDA, &pg);
@@ -833,6 +924,113 @@ int build_dbop(kspir_ctx* c) {
                                                                                         c->G);
     KS_CUDA(c, cudaGetLastError());
     KS_CUDA(c, cudaStreamSynchronize(c->stream));
+    return KSPIR_OK;
+}
+
+// The task queue of the fused answer (k_answer.cuh).  Every task comes after
+// the tasks it depends on; the tail (giant steps, external products, packing
+// merges) is sorted by when its inputs complete: the scan position of the
+// last sub-database it needs (the scan runs in fa_scan_order), then its depth.
+std::vector<FaTask> build_fa_tasks(const kspir_ctx* c) {
+    std::vector<FaTask> t;
+    auto add = [&](int type, int a, int b, int cc = 0, int d = 0) {
+        FaTask x;
+        x.type = (uint8_t)type; x.a = (uint8_t)a; x.b = (uint16_t)b; x.c = (uint16_t)cc; x.d = (uint16_t)d;
+        t.push_back(x);
+    };
+    const int R = c->p.r, N2 = c->N2, L = c->levels, N1h = c->N1h, inter = N1h - 2;
+    for (int b = 0; b < kFaPrepChunks; b++) add(FT_PREP, 0, b);
+    for (int b = 0; b < c->n_q; b++) add(FT_QNTT, 0, b);
+    for (int comp = 0; comp < 2; comp++) add(FT_ROT1, comp, inter);
+    for (int b = 0; b < 2; b++) add(FT_INTER_NTT, 0, b);
+    for (int b = 0; b < kFaPrepChunks; b++) add(FT_INTER_DEC, 0, b);
+    for (int b = 0; b < 9; b++) add(FT_DIG1, 0, b);
+    for (int ki = 0; ki < N1h - 1; ki++)
+        if (ki != inter)
+            for (int comp = 0; comp < 2; comp++) add(FT_ROT1, comp, ki);
+    for (int ki = 0; ki < N1h; ki++)
+        for (int comp = 0; comp < 2; comp++) add(FT_ROT2, comp, ki);
+    std::vector<int> pos(R);
+    for (int x = 0; x < R; x++) pos[fa_scan_order(x, L)] = x;   // pos[sub-database] = scan position
+    struct Keyed { int k0, k1, k2; FaTask task; };
+    std::vector<Keyed> tail;
+    auto push = [&](int k0, int k1, int k2, int type, int a, int b, int cc = 0, int d = 0) {
+        FaTask x;
+        x.type = (uint8_t)type; x.a = (uint8_t)a; x.b = (uint16_t)b; x.c = (uint16_t)cc; x.d = (uint16_t)d;
+        tail.push_back(Keyed{k0, k1, k2, x});
+    };
+    for (int r = 0; r < R; r++) {
+        for (int cg = 1; cg < N2; cg++) push(pos[r], 0, cg, FT_GIANT, 0, r, cg);
+        for (int ch = 0; ch < 2; ch++) push(pos[r], 1, ch, FT_EXT, ch, r);
+    }
+    for (int lv = L - 1; lv >= 0; lv--) {
+        const int I = 1 << lv;
+        for (int j = 0; j < I; j++) {
+            int last = 0;
+            for (int x = j; x < R; x += I) last = std::max(last, pos[x]);
+            const int depth = 2 + 2 * (L - 1 - lv);
+            for (int ch = 0; ch < 2; ch++)
+                for (int d = 0; d <= 4; d++) push(last, depth, ch * 8 + d, FT_PFWD, lv, j, ch, d);
+            for (int ch = 0; ch < 2; ch++)
+                for (int comp = 0; comp < 2; comp++) push(last, depth + 1, ch * 2 + comp, FT_PINV, lv, j, ch, comp);
+        }
+    }
+    std::stable_sort(tail.begin(), tail.end(), [](const Keyed& x, const Keyed& y) {
+        return x.k0 != y.k0 ? x.k0 < y.k0 : x.k1 != y.k1 ? x.k1 < y.k1 : x.k2 < y.k2;
+    });
+    for (auto& k : tail) t.push_back(k.task);
+    add(FT_COMPOSE, 0, 0);
+    return t;
+}
+
+// Runs the queue in order on the host with the kernel's own dependency rules
+// (the scan completes once every rotation has): every task must find its
+// inputs complete when it is dequeued, so no wait of the kernel can depend on
+// a task behind it.  Returns the index of the first task that fails, or -1.
+int fa_check_order(const std::vector<FaTask>& tasks, const FaShape& sh) {
+    std::vector<int> cnt(fa_counter_words(sh.R), 0);
+    cnt[FC_ZERO] = sh.ctas;
+    for (size_t i = 0; i < tasks.size(); i++) {
+        int idx[2], target[2];
+        const int n = fa_deps(sh, tasks[i], idx, target);
+        for (int d = 0; d < n; d++)
+            if (idx[d] < 0 || idx[d] >= (int)cnt.size() || cnt[idx[d]] < target[d]) return (int)i;
+        int second;
+        const int c = fa_done(sh, tasks[i], &second);
+        cnt[c]++;
+        if (second >= 0) cnt[second]++;
+        if (cnt[FC_QNTT] >= sh.n_q && cnt[FC_ROT1] >= 2 * (sh.N1 / 2 - 1) && cnt[FC_ROT2] >= sh.N1)
+            for (int r = 0; r < sh.R; r++) cnt[FC_PER_R + r] = kN;
+    }
+    return cnt[FC_COMPOSE] == 1 ? -1 : (int)tasks.size();
+}
+
+// The fused single answer needs N1 = 128, a device that launches cooperative
+// kernels, and one CTA of k_answer per SM.  Single answers use it when
+// KSPIR_FUSED=1 or kspir_set_fused turns it on.
+int init_fused(kspir_ctx* c) {
+    if (c->N1 != 128) return KSPIR_OK;
+    int coop = 0;
+    KS_CUDA(c, cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c->device));
+    if (!coop) return KSPIR_OK;
+    using F = FaCfg<128, kFaScanWarps>;
+    KS_CUDA(c, cudaFuncSetAttribute(k_answer<128, kFaScanWarps>, cudaFuncAttributeMaxDynamicSharedMemorySize, F::SMEM));
+    int per_sm = 0;
+    KS_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_answer<128, kFaScanWarps>, F::THREADS, F::SMEM));
+    if (per_sm < 1) return KSPIR_OK;
+    const std::vector<FaTask> tasks = build_fa_tasks(c);
+    const int bad = fa_check_order(tasks, FaShape{c->p.r, c->N1, c->levels, c->n_q, c->N1h - 2, c->nsm});
+    if (bad >= 0)
+        return set_err(c, KSPIR_ERR_INVALID_ARG, "fused answer: task " + std::to_string(bad) + " out of order");
+    c->fa_ntasks = (int)tasks.size();
+    KS_CUDA(c, cudaMalloc(&c->fa_tasks, tasks.size() * sizeof(FaTask)));
+    KS_COPY(c, c->fa_tasks, tasks.data(), tasks.size() * sizeof(FaTask), cudaMemcpyHostToDevice);
+    KS_CUDA(c, cudaMalloc(&c->fa_cnt, (size_t)fa_counter_words(c->p.r) * 4));
+    KS_CUDA(c, cudaMalloc(&c->fa_acc, (size_t)c->p.r * 4 * kN * 4));
+    KS_CUDA(c, cudaMalloc(&c->fa_times, (size_t)kTimingRing * FT_T_COUNT * 8));
+    KS_CUDA(c, cudaMemsetAsync(c->fa_times, 0, (size_t)kTimingRing * FT_T_COUNT * 8, c->stream));
+    c->fused_ok = true;
+    if (const char* e = getenv("KSPIR_FUSED")) c->fused = e[0] == '1';
     return KSPIR_OK;
 }
 
@@ -926,6 +1124,9 @@ int kspir_ctx_create(int device, const kspir_params* params, kspir_ctx** out) {
     if (rc) return rc;
     rc = init_workspaces(c.get());
     if (rc) return rc;
+    c->ring_fused.assign(kTimingRing, 0);
+    rc = init_fused(c.get());
+    if (rc) return rc;
     KS_CUDA(c.get(), cudaStreamSynchronize(c->stream));
     *out = c.release();
     return KSPIR_OK;
@@ -959,6 +1160,10 @@ int kspir_ctx_destroy(kspir_ctx* c) {
     if (c->prep_host) cudaFreeHost(c->prep_host);
     cudaFree(c->dbop);
     cudaFree(c->qop);
+    cudaFree(c->fa_tasks);
+    cudaFree(c->fa_cnt);
+    cudaFree(c->fa_acc);
+    cudaFree(c->fa_times);
     cudaFree(c->perms);
     cudaFree(c->tw);
     cudaFree(c->sigma_baby);
@@ -1590,7 +1795,7 @@ int kspir_answer_device(kspir_ctx* c, int client, const uint64_t* d_query, uint6
     cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
     KS_CUDA(c, cudaSetDevice(c->device));
     KS_CUDA(c, cudaMemcpyAsync(c->bq64, d_query, 4 * kN * 8, cudaMemcpyDeviceToDevice, st));
-    rc = enqueue_answer(c, 0, 1, &client, st);
+    rc = enqueue_answer(c, 0, 1, &client, st, true);
     if (rc) return rc;
     KS_CUDA(c, cudaMemcpyAsync(d_response, c->bresp, 2 * kN * 8, cudaMemcpyDeviceToDevice, st));
     KS_CUDA(c, cudaGetLastError());
@@ -1618,7 +1823,7 @@ int kspir_answer(kspir_ctx* c, int client, const uint64_t* query, uint64_t* resp
     std::lock_guard<std::mutex> lk(c->mu);
     KS_CUDA(c, cudaSetDevice(c->device));
     KS_CUDA(c, cudaMemcpyAsync(c->bq64, query, 4 * kN * 8, cudaMemcpyHostToDevice, c->stream));
-    rc = enqueue_answer(c, 0, 1, &client, c->stream);
+    rc = enqueue_answer(c, 0, 1, &client, c->stream, true);
     if (rc) return rc;
     KS_CUDA(c, cudaGetLastError());
     // the query is validated while the device answers it; a non-canonical one
@@ -1723,6 +1928,37 @@ int kspir_set_scan_kind(kspir_ctx* c, int n, int kind) {
 
 int kspir_get_scan_kind(kspir_ctx* c, int n) { return c ? scan_kind_for(c, n) : KSPIR_ERR_INVALID_ARG; }
 
+namespace {
+// Phase split of a fused answer from its device timestamps: the segments of its
+// critical path (query side up to the scan start or the last rotation, the
+// scan, and what the giant steps, external products and packing add after
+// the scan ends).
+void fused_phases(const unsigned long long* t, float* ph) {
+    const double start = (double)~t[FT_T_START], scan0 = (double)~t[FT_T_SCAN0];
+    const double head = (double)t[FT_T_HEAD], scan1 = (double)t[FT_T_SCAN1], giant = (double)t[FT_T_GIANT],
+                 ext = (double)t[FT_T_EXT], end = (double)t[FT_T_END];
+    auto ms = [](double a, double b) { return (float)(b > a ? (b - a) * 1e-6 : 0.0); };
+    ph[0] = ms(start, std::min(head, scan0));
+    ph[1] = ms(scan0, scan1);
+    ph[2] = ms(scan1, giant);
+    ph[3] = ms(std::max(scan1, giant), ext);
+    ph[4] = ms(std::max(scan1, ext), end);
+}
+
+int phases_of(kspir_ctx* c, int slot, float* ph) {
+    auto& ev = c->ring[slot];
+    KS_CUDA(c, cudaEventSynchronize(ev[5]));
+    if (!c->ring_fused[slot]) {
+        for (int i = 0; i < 5; i++) KS_CUDA(c, cudaEventElapsedTime(&ph[i], ev[i], ev[i + 1]));
+        return KSPIR_OK;
+    }
+    unsigned long long t[FT_T_COUNT];
+    KS_CUDA(c, cudaMemcpy(t, c->fa_times + (size_t)slot * FT_T_COUNT, sizeof(t), cudaMemcpyDeviceToHost));
+    fused_phases(t, ph);
+    return KSPIR_OK;
+}
+}  // namespace
+
 int kspir_last_timing(kspir_ctx* c, float* total_ms, float* phase_ms) {
     if (!c || c->last_slot < 0) return KSPIR_ERR_NOT_READY;
     auto& ev = c->ring[c->last_slot];
@@ -1730,10 +1966,19 @@ int kspir_last_timing(kspir_ctx* c, float* total_ms, float* phase_ms) {
     float t = 0;
     KS_CUDA(c, cudaEventElapsedTime(&t, ev[0], ev[5]));
     if (total_ms) *total_ms = t;
-    if (phase_ms)
-        for (int i = 0; i < 5; i++) KS_CUDA(c, cudaEventElapsedTime(&phase_ms[i], ev[i], ev[i + 1]));
+    if (phase_ms) return phases_of(c, c->last_slot, phase_ms);
     return KSPIR_OK;
 }
+
+int kspir_set_fused(kspir_ctx* c, int enable) {
+    if (!c) return KSPIR_ERR_INVALID_ARG;
+    if (enable && !c->fused_ok) return set_err(c, KSPIR_ERR_NOT_READY, "fused answer not available on this context");
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->fused = enable != 0;
+    return KSPIR_OK;
+}
+
+int kspir_get_fused(const kspir_ctx* c) { return c ? (c->fused ? 1 : 0) : KSPIR_ERR_INVALID_ARG; }
 
 int kspir_timing_reset(kspir_ctx* c) {
     if (!c) return KSPIR_ERR_INVALID_ARG;
@@ -1756,10 +2001,10 @@ int kspir_timing_summary(kspir_ctx* c, int* answers, long* launches, float* tota
         KS_CUDA(c, cudaEventElapsedTime(&t, ev[0], ev[5]));
         tot += t;
         queries += c->ring_nq[k];
-        for (int i = 0; i < 5; i++) {
-            KS_CUDA(c, cudaEventElapsedTime(&t, ev[i], ev[i + 1]));
-            ph[i] += t;
-        }
+        float p[5];
+        int rc = phases_of(c, k, p);
+        if (rc) return rc;
+        for (int i = 0; i < 5; i++) ph[i] += p[i];
     }
     if (answers) *answers = queries;
     if (launches) *launches = c->launches;

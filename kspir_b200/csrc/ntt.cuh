@@ -53,6 +53,14 @@ struct NttTables {
     const uint2* tw[CH_COUNT];   // [2][N] per channel
 };
 
+// Barrier of the 512 threads that run a transform.  A stand-alone kernel
+// synchronises its whole CTA; the fused answer kernel (k_answer.cuh) runs its
+// transforms in a 512-thread warp group beside the scan warps and uses a named
+// barrier (KsSync there).
+struct CtaSync {
+    __device__ __forceinline__ static void sync() { __syncthreads(); }
+};
+
 enum NttDir : int { NTT_FWD = 0, NTT_INV = 1 };
 
 // Copies the twiddles of (channel, direction) into shared memory.  The caller
@@ -185,44 +193,46 @@ __device__ __forceinline__ void inv_pass(uint32_t* s, int stride, const uint2* t
 // lockstep (one barrier per pass for all of them); input in [0, 4q)
 // (canonical inputs are fine), output canonical.  tws holds the forward
 // twiddles of ch.
-template <int M>
+template <int M, class Sync = CtaSync>
 __device__ __forceinline__ void cta_ntt_forward_m(uint32_t* s, int stride, const uint2* tws, int ch) {
     const uint32_t q = c_dev.ch[ch].q, q2 = c_dev.ch[ch].two_q;
     const int u = threadIdx.x;
-    __syncthreads();
+    Sync::sync();
     fwd_pass<0, M>(s, stride, tws, q, q2, u);
-    __syncthreads();
+    Sync::sync();
     fwd_pass<1, M>(s, stride, tws, q, q2, u);
-    __syncthreads();
+    Sync::sync();
     fwd_pass<2, M>(s, stride, tws, q, q2, u);
-    __syncthreads();
+    Sync::sync();
     fwd_pass<3, M>(s, stride, tws, q, q2, u);
-    __syncthreads();
+    Sync::sync();
 }
 
 // Inverse transforms (include N^-1); input in [0, 2q) (canonical inputs are
 // fine), output canonical.  tws holds the inverse twiddles of ch.
-template <int M>
+template <int M, class Sync = CtaSync>
 __device__ __forceinline__ void cta_ntt_inverse_m(uint32_t* s, int stride, const uint2* tws, int ch) {
     const uint32_t q = c_dev.ch[ch].q, q2 = c_dev.ch[ch].two_q;
     const uint32_t ni = c_dev.ch[ch].ninv, nip = c_dev.ch[ch].ninv_p;
     const int u = threadIdx.x;
-    __syncthreads();
+    Sync::sync();
     inv_pass<3, M>(s, stride, tws, q, q2, ni, nip, u);
-    __syncthreads();
+    Sync::sync();
     inv_pass<2, M>(s, stride, tws, q, q2, ni, nip, u);
-    __syncthreads();
+    Sync::sync();
     inv_pass<1, M>(s, stride, tws, q, q2, ni, nip, u);
-    __syncthreads();
+    Sync::sync();
     inv_pass<0, M>(s, stride, tws, q, q2, ni, nip, u);
-    __syncthreads();
+    Sync::sync();
 }
 
+template <class Sync = CtaSync>
 __device__ __forceinline__ void cta_ntt_forward(uint32_t* s, const uint2* tws, int ch) {
-    cta_ntt_forward_m<1>(s, kPadN, tws, ch);
+    cta_ntt_forward_m<1, Sync>(s, kPadN, tws, ch);
 }
+template <class Sync = CtaSync>
 __device__ __forceinline__ void cta_ntt_inverse(uint32_t* s, const uint2* tws, int ch) {
-    cta_ntt_inverse_m<1>(s, kPadN, tws, ch);
+    cta_ntt_inverse_m<1, Sync>(s, kPadN, tws, ch);
 }
 
 // Copies of whole polynomials between global memory (natural order) and a

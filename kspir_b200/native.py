@@ -80,6 +80,8 @@ SIGNATURES = {
     "kspir_fetch_stage_slot": (_i, [_vp, _i, _i, _vp, _sz]),
     "kspir_client_key_bytes": (_sz, [_vp]),
     "kspir_debug_scan_fault": (_i, [_vp, ctypes.c_int64, ctypes.c_long]),
+    "kspir_set_fused": (_i, [_vp, _i]),
+    "kspir_get_fused": (_i, [_vp]),
     "kspir_server_create": (_i, [_vp, _vp, _vp]),
     "kspir_server_destroy": (_i, [_vp]),
     "kspir_server_register_client": (_i, [_vp, ctypes.c_int64, _vp, _vp, _vp, _vp]),
@@ -371,6 +373,14 @@ class Context:
 
     def sync(self):
         self._check(self.lib.kspir_sync(self._h))
+
+    def set_fused(self, enable: bool):
+        """Single answers as the one fused kernel (kspir_set_fused)."""
+        self._check(self.lib.kspir_set_fused(self._h, 1 if enable else 0))
+
+    @property
+    def fused(self) -> bool:
+        return self.lib.kspir_get_fused(self._h) == 1
 
     def debug_scan_fault(self, wait_limit_ns: int = 0, skip_item: int = -1):
         """Test hook (kspir_debug_scan_fault): the limit of the database scan's

@@ -1,7 +1,8 @@
 """The answer is the same in every launch mode: CUDA graphs on or off
-(KSPIR_NO_GRAPHS), programmatic dependent launch on or off (KSPIR_NO_PDL).
-The modes only change how the same kernels are launched, and each context
-reads them when it is created."""
+(KSPIR_NO_GRAPHS), programmatic dependent launch on or off (KSPIR_NO_PDL),
+and single answers as separate kernels or as the one fused kernel
+(KSPIR_FUSED).  The modes only change how the same arithmetic is launched,
+and each context reads them when it is created."""
 import os
 
 import numpy as np
@@ -14,8 +15,8 @@ pytestmark = pytest.mark.gpu
 
 
 @pytest.mark.parametrize("env", [{}, {"KSPIR_NO_GRAPHS": "1"}, {"KSPIR_NO_PDL": "1"},
-                                 {"KSPIR_NO_GRAPHS": "1", "KSPIR_NO_PDL": "1"}],
-                         ids=["default", "no-graphs", "no-pdl", "neither"])
+                                 {"KSPIR_NO_GRAPHS": "1", "KSPIR_NO_PDL": "1"}, {"KSPIR_FUSED": "1"}],
+                         ids=["default", "no-graphs", "no-pdl", "neither", "fused"])
 def test_launch_modes_answer_alike(env, monkeypatch):
     for k, v in env.items():
         monkeypatch.setenv(k, v)
