@@ -159,6 +159,34 @@ int kspir_client_queries(kspir_ctx* ctx, int n, const uint64_t* secrets, const u
 int kspir_client_decrypt(kspir_ctx* ctx, int n, const uint64_t* secrets, const uint64_t* responses, int r,
                          uint64_t* messages);
 
+/* ------------------------------------------------------------------------
+ * Offline key derivation, reference genAutoKeyFromOffline (twosteps.h,
+ * twosteps.cpp:1749-1864) with its key switch evalAutoRNSKey
+ * (twosteps.cpp:1587-1743), as tests/test-two-steps-key.cpp:140-175 runs it:
+ * offline keys offlineKey1 (crtMod, crtBaMod = bsMod * auxMod, ell 5, base
+ * 2^18, Bg 2^18) and offlineKey2 (crtMod, auxMod, ell 5, base 2^14, Bg 2^14),
+ * automorphism keys autoKey1 (crtMod, crtBaMod) and autoKey2 (crtMod, auxMod),
+ * N1 and N2 of the context.  Host buffers of u64 words, NTT form as keyGen
+ * leaves the inputs:
+ *   offline1  [10][2][N]  offlineKey1.keyMap[5]: rows 0-4 mod crtMod, 5-9 mod crtBaMod
+ *   offline2  [10][2][N]  offlineKey2.keyMap[5^N1]: rows 0-4 mod crtMod, 5-9 mod auxMod
+ *   auto1     [6][2][N]   autoKey1.keyMap[5]: rows 0-2 mod crtMod, 3-5 mod crtBaMod
+ *   auto2     [6][2][N]   autoKey2.keyMap[5^N1]: rows 0-2 mod crtMod, 3-5 mod auxMod
+ * Outputs (each may be NULL), word for word the reference's key maps after
+ * the call:
+ *   chain1    [N1-2][6][2][N]  autoKey1.keyMap[5^i], i = 2..N1-1 (coefficient form)
+ *   chain2    [N2-2][6][2][N]  autoKey2.keyMap[5^(N1 i)], i = 2..N2-1
+ *   baby_out  [N1-1][6][2][N]  result.keyMap[5^i], i = 1..N1-1 (NTT form)
+ *   giant_out [N2-1][3][2][N]  result.keyMap[5^(N1 i)], i = 1..N2-1
+ * The reference reads the crtBaMod rows through EltwiseReduceMod with factors
+ * (1, 1), which leaves them unreduced, so rows 3-5 of every baby_out key are
+ * zero; these are the reference's words, not keys the answer can use.
+ * device_ms (or NULL) receives the device time.  Non-canonical input words:
+ * KSPIR_ERR_INVALID_ARG. */
+int kspir_gen_autokey_from_offline(kspir_ctx* ctx, const uint64_t* offline1, const uint64_t* offline2,
+                                   const uint64_t* auto1, const uint64_t* auto2, uint64_t* chain1, uint64_t* chain2,
+                                   uint64_t* baby_out, uint64_t* giant_out, float* device_ms);
+
 /* Copies the resident database (datacrt layout, r * N * N / 2 words) to host. */
 int kspir_db_download(kspir_ctx* ctx, uint64_t* datacrt, size_t words);
 

@@ -25,9 +25,13 @@ constexpr uint64_t kBsModInvCrt = 51309461009346113ull;  // bsMod^-1 mod crtMod,
 constexpr uint32_t kCrtModInvBs = 3920321u;              // crtMod^-1 mod bsMod, crt.h:34
 
 constexpr uint32_t kP = 65537u;        // plaintext modulus bsgsp, params.h:94
+constexpr uint32_t kAuxMod = 268361729u;   // auxiliary modulus of the offline key derivation, crt.h:37
 
-// channels of the RNS representation (p: only for the database preprocessing)
-enum Chan : int { CH_Q1 = 0, CH_Q2 = 1, CH_BS = 2, CH_P = 3, CH_COUNT = 4 };
+// channels of the RNS representation (p: only for the database preprocessing;
+// the last three only for the offline key derivation: crtBaMod = bsMod * auxMod
+// transformed with root_of_unity_crt_bamod, crt.h:82, as its two residues, and
+// auxMod with HEXL's minimal root)
+enum Chan : int { CH_Q1 = 0, CH_Q2 = 1, CH_BS = 2, CH_P = 3, CH_BA_BS = 4, CH_BA_AUX = 5, CH_AUX = 6, CH_COUNT = 7 };
 
 // Per-channel constants, filled on the host (context.cu) and kept in
 // __constant__ memory.

@@ -29,6 +29,7 @@
 #include "k_second.cuh"
 #include "k_util.cuh"
 #include "k_answer.cuh"
+#include "k_offline.cuh"
 #include "ntt.cuh"
 #include "pipeline.cuh"
 
@@ -367,7 +368,9 @@ Batch batch_of(const kspir_ctx* c, int slot0) {
 }
 
 // the channel moduli, in Chan order
-const uint32_t kChanQ[CH_COUNT] = {kQ1, kQ2, kBsMod, kP};
+const uint32_t kChanQ[CH_COUNT] = {kQ1, kQ2, kBsMod, kP, kBsMod, kAuxMod, kAuxMod};
+const uint64_t kRootCrt = 3375402822066082ull;     // root_of_unity_crt, crt.h:81
+const uint64_t kRootCrtBa = 1486445687605966ull;   // root_of_unity_crt_bamod, crt.h:82
 
 // every per-channel constant of c_dev (also written by the allocation-free set-up)
 DevConst make_dev_const() {
@@ -395,8 +398,8 @@ int init_constants(kspir_ctx* c) {
 
     // twiddles: crt channels use root_of_unity_crt (reference crt.h:81) reduced
     // per prime; bsMod and p use HEXL's minimal primitive root
-    const uint64_t root_crt = 3375402822066082ull;
-    const uint64_t roots[CH_COUNT] = {root_crt % kQ1, root_crt % kQ2, h_min_root(kBsMod), h_min_root(kP)};
+    const uint64_t roots[CH_COUNT] = {kRootCrt % kQ1,      kRootCrt % kQ2,        h_min_root(kBsMod), h_min_root(kP),
+                                      kRootCrtBa % kBsMod, kRootCrtBa % kAuxMod, h_min_root(kAuxMod)};
     // per channel uint2 [2][N]: {psi^brv(k), Shoup} then {psi^-brv(k), Shoup}, k-major order
     std::vector<uint32_t> tw((size_t)CH_COUNT * 4 * kN);
     for (int ch = 0; ch < CH_COUNT; ch++) {
@@ -1099,6 +1102,9 @@ int kspir_ctx_create(int device, const kspir_params* params, kspir_ctx** out) {
     KS_CUDA(c.get(), cudaFuncSetAttribute(k_pack_fused<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, kPackSmem));
     KS_CUDA(c.get(), cudaFuncSetAttribute(k_pack_split_fwd<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, kPackSplitSmem));
     KS_CUDA(c.get(), cudaFuncSetAttribute(k_pack_split_inv<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, kPackSplitSmem));
+    KS_CUDA(c.get(), cudaFuncSetAttribute(k_off_keyswitch, cudaFuncAttributeMaxDynamicSharedMemorySize, kOffSmem));
+    KS_CUDA(c.get(), cudaFuncSetAttribute(k_off_intt_key, cudaFuncAttributeMaxDynamicSharedMemorySize, kNttJobSmem));
+    KS_CUDA(c.get(), cudaFuncSetAttribute(k_off_modswitch, cudaFuncAttributeMaxDynamicSharedMemorySize, kNttJobSmem));
 #define KS_ATTR(n) \
     KS_CUDA(c.get(), cudaFuncSetAttribute(k_scan<n>, cudaFuncAttributeMaxDynamicSharedMemorySize, ScanCfg<n>::SMEM));
     KS_ATTR(64) KS_ATTR(128) KS_ATTR(256)
@@ -1391,6 +1397,161 @@ int client_scratch(kspir_ctx* c, size_t bytes, uint8_t** out) {
     return KSPIR_OK;
 }
 }  // namespace
+
+// ---------------------------------------------------------------------------
+// Offline key derivation (k_offline.cuh)
+
+namespace {
+
+CrtRef make_crt_ref(uint64_t m1, uint64_t m2) {
+    CrtRef c;
+    const hu128 M = (hu128)m1 * m2;
+    const hu128 two128 = (~(hu128)0 % M + 1) % M;   // 2^128 mod M
+    c.M.lo = (uint64_t)M; c.M.hi = (uint64_t)(M >> 64);
+    c.two128.lo = (uint64_t)two128; c.two128.hi = (uint64_t)(two128 >> 64);
+    c.qi1 = m2; c.qinv1 = h_invmod(m2 % m1, m1);   // term of x1: m2 * (m2^-1 mod m1)
+    c.qi2 = m1; c.qinv2 = h_invmod(m1 % m2, m2);   // term of x2: m1 * (m1^-1 mod m2)
+    return c;
+}
+
+OffGadget make_off_gadget(int ell, int base_bits, int gbits) {
+    OffGadget g;
+    g.ell = ell; g.base_bits = base_bits; g.gbits = gbits;
+    hu128 off = 0;
+    for (int i = 0; i < ell; i++) off += (hu128)1 << (base_bits + i * gbits);
+    off <<= (gbits - 1);
+    off += base_bits ? ((hu128)1 << (base_bits - 1)) : 0;   // base / 2
+    g.offset.lo = (uint64_t)off; g.offset.hi = (uint64_t)(off >> 64);
+    return g;
+}
+
+// One chain: entries e = 1..E of keys (device words [E + 1][6][2][N]; entry 1
+// = the automorphism key as generated), links e -> e + 1 for e = 1..E-1; the
+// first link reads entry 1 in coefficient form from entry 0.
+int run_offline_chain(kspir_ctx* c, const OffChain& ch, uint64_t* keys, int E, const uint32_t* okey, uint32_t* kres,
+                      uint32_t* dig, uint32_t* bres, uint32_t* res, uint32_t p1inv) {
+    cudaStream_t st = c->stream;
+    const size_t key_words = (size_t)6 * 2 * kN;
+    k_off_key_residues<<<blocks_for(6L * 2 * kN, 256), 256, 0, st>>>(keys + key_words, kres, 6, kOffRows, ch);
+    k_off_intt_key<<<dim3(2, 2, 6), kNttThreads, kNttJobSmem, st>>>(kres, res, c->ntabs, ch);
+    k_off_compose<<<dim3(kN / 256, 2, kOffRows), 256, 0, st>>>(res, keys, ch, p1inv);
+    for (int e = 1; e < E; e++) {
+        const uint64_t* in = keys + (size_t)(e == 1 ? 0 : e) * key_words;
+        k_off_decomp<<<dim3(kN / 256, kOffRows), 256, 0, st>>>(in, dig, bres, ch);
+        k_off_keyswitch<<<dim3(2 + ch.nch2, kOffRows), kNttThreads, kOffSmem, st>>>(dig, bres, okey, res, c->ntabs, ch);
+        k_off_compose<<<dim3(kN / 256, 2, kOffRows), 256, 0, st>>>(res, keys + (size_t)(e + 1) * key_words, ch, p1inv);
+    }
+    KS_CUDA(c, cudaGetLastError());
+    return KSPIR_OK;
+}
+
+}  // namespace
+
+extern "C" int kspir_gen_autokey_from_offline(kspir_ctx* c, const uint64_t* offline1, const uint64_t* offline2,
+                                              const uint64_t* auto1, const uint64_t* auto2, uint64_t* chain1,
+                                              uint64_t* chain2, uint64_t* baby_out, uint64_t* giant_out,
+                                              float* device_ms) {
+    if (!c || !offline1 || !offline2 || !auto1 || !auto2) return KSPIR_ERR_INVALID_ARG;
+    const int N1 = c->N1, N2 = c->N2;
+    if (N2 < 2) return set_err(c, KSPIR_ERR_INVALID_ARG, "offline derivation needs N2 >= 2");
+    const uint64_t kBa = (uint64_t)kBsMod * kAuxMod;
+    const size_t P2 = (size_t)2 * kN;   // words of one RLWE
+    // inputs: crtMod rows, then rows of the second modulus
+    if (!canonical(offline1, 5 * P2, kCrtMod) || !canonical(offline1 + 5 * P2, 5 * P2, kBa) ||
+        !canonical(offline2, 5 * P2, kCrtMod) || !canonical(offline2 + 5 * P2, 5 * P2, kAuxMod) ||
+        !canonical(auto1, 3 * P2, kCrtMod) || !canonical(auto1 + 3 * P2, 3 * P2, kBa) ||
+        !canonical(auto2, 3 * P2, kCrtMod) || !canonical(auto2 + 3 * P2, 3 * P2, kAuxMod))
+        return set_err(c, KSPIR_ERR_INVALID_ARG, "key word not canonical");
+    std::lock_guard<std::mutex> lk(c->mu);
+    KS_CUDA(c, cudaSetDevice(c->device));
+    cudaStream_t st = c->stream;
+
+    OffChain baby{};
+    baby.nch2 = 2; baby.ch2[0] = CH_BA_BS; baby.ch2[1] = CH_BA_AUX; baby.m2 = kBa;
+    baby.ginv = inv_mod_2n(5);
+    baby.crt = make_crt_ref(kCrtMod, kBa);
+    baby.g = make_off_gadget(5, 18, 18);           // offlineKey1: ellnum 5, base 2^18, Bg 2^18
+    OffChain giant{};
+    giant.nch2 = 1; giant.ch2[0] = CH_AUX; giant.ch2[1] = CH_AUX; giant.m2 = kAuxMod;
+    giant.ginv = inv_mod_2n(pow5((uint32_t)N1));
+    giant.crt = make_crt_ref(kCrtMod, kAuxMod);
+    giant.g = make_off_gadget(5, 14, 14);          // offlineKey2: ellnum 5, base 2^14, Bg 2^14
+    const uint32_t p1inv = (uint32_t)h_invmod(kBsMod, kAuxMod);
+    const uint64_t aux_inv = h_invmod(kAuxMod % kCrtMod, kCrtMod);   // auxModInv
+
+    // device buffers, carved from the context's scratch allocation
+    const size_t key_words = 6 * P2;
+    const size_t n_keys1 = (size_t)N1 * key_words, n_keys2 = (size_t)N2 * key_words;
+    const size_t n_okey = (size_t)10 * 2 * 4 * kN, n_kres = (size_t)6 * 2 * 4 * kN;
+    const size_t n_dig = (size_t)kOffRows * kOffEll * 4 * kN, n_bres = (size_t)kOffRows * 4 * kN;
+    const size_t n_res = (size_t)kOffRows * 4 * 2 * kN;
+    const size_t n_ms = (size_t)(N1 - 1 + N2 - 1) * kOffRows * 2 * 2 * kN;
+    const size_t n_msw = (size_t)(N1 - 1 + N2 - 1) * kOffRows * P2;
+    const size_t bytes = (n_keys1 + n_keys2 + 2 * 10 * P2 + n_msw) * 8 +
+                         (2 * n_okey + n_kres + n_dig + n_bres + n_res + n_ms) * 4 + 64 * 256;
+    uint8_t* base = nullptr;
+    int rc = client_scratch(c, bytes, &base);
+    if (rc) return rc;
+    Carve cv;
+    cv.base = base;
+    uint64_t* keys1 = cv.take<uint64_t>(n_keys1);
+    uint64_t* keys2 = cv.take<uint64_t>(n_keys2);
+    uint64_t* off_w = cv.take<uint64_t>(2 * 10 * P2);
+    uint64_t* msw = cv.take<uint64_t>(n_msw);
+    uint32_t* okey1 = cv.take<uint32_t>(n_okey);
+    uint32_t* okey2 = cv.take<uint32_t>(n_okey);
+    uint32_t* kres = cv.take<uint32_t>(n_kres);
+    uint32_t* dig = cv.take<uint32_t>(n_dig);
+    uint32_t* bres = cv.take<uint32_t>(n_bres);
+    uint32_t* res = cv.take<uint32_t>(n_res);
+    uint32_t* ms = cv.take<uint32_t>(n_ms);
+
+    cudaEvent_t e0, e1;
+    KS_CUDA(c, cudaEventCreate(&e0));
+    KS_CUDA(c, cudaEventCreate(&e1));
+    KS_CUDA(c, cudaMemcpyAsync(keys1 + key_words, auto1, key_words * 8, cudaMemcpyHostToDevice, st));
+    KS_CUDA(c, cudaMemcpyAsync(keys2 + key_words, auto2, key_words * 8, cudaMemcpyHostToDevice, st));
+    KS_CUDA(c, cudaMemcpyAsync(off_w, offline1, 10 * P2 * 8, cudaMemcpyHostToDevice, st));
+    KS_CUDA(c, cudaMemcpyAsync(off_w + 10 * P2, offline2, 10 * P2 * 8, cudaMemcpyHostToDevice, st));
+    KS_CUDA(c, cudaEventRecord(e0, st));
+    k_off_key_residues<<<blocks_for(10L * 2 * kN, 256), 256, 0, st>>>(off_w, okey1, 10, kOffEll, baby);
+    k_off_key_residues<<<blocks_for(10L * 2 * kN, 256), 256, 0, st>>>(off_w + 10 * P2, okey2, 10, kOffEll, giant);
+    rc = run_offline_chain(c, baby, keys1, N1 - 1, okey1, kres, dig, bres, res, p1inv);
+    if (!rc) rc = run_offline_chain(c, giant, keys2, N2 - 1, okey2, kres, dig, bres, res, p1inv);
+    if (!rc) {
+        // the modulus switch of every key of both chains (entries 1..): the
+        // baby keys' words, then the giant keys' words
+        uint32_t* ms2 = ms + (size_t)(N1 - 1) * kOffRows * 2 * 2 * kN;
+        uint64_t* msw2 = msw + (size_t)(N1 - 1) * kOffRows * P2;
+        k_off_modswitch<<<(N1 - 1) * 4 * kOffRows, kNttThreads, kNttJobSmem, st>>>(keys1 + key_words, ms, aux_inv,
+                                                                                  c->ntabs);
+        k_off_modswitch<<<(N2 - 1) * 4 * kOffRows, kNttThreads, kNttJobSmem, st>>>(keys2 + key_words, ms2, aux_inv,
+                                                                                  c->ntabs);
+        k_compose_words<<<blocks_for((long)(N1 - 1 + N2 - 1) * kOffRows * 2 * kN, 256), 256, 0, st>>>(
+            ms, msw, (N1 - 1 + N2 - 1) * kOffRows * 2);
+        KS_CUDA(c, cudaEventRecord(e1, st));
+        KS_CUDA(c, cudaGetLastError());
+        std::vector<uint64_t> w((size_t)(N1 - 1) * kOffRows * P2);
+        KS_COPY(c, w.data(), msw, w.size() * 8, cudaMemcpyDeviceToHost);
+        if (baby_out)
+            for (int e = 0; e < N1 - 1; e++) {
+                uint64_t* o = baby_out + (size_t)e * key_words;
+                memcpy(o, w.data() + (size_t)e * kOffRows * P2, kOffRows * P2 * 8);
+                memset(o + kOffRows * P2, 0, kOffRows * P2 * 8);   // the bsMod rows come out zero
+            }
+        if (giant_out) KS_COPY(c, giant_out, msw2, (size_t)(N2 - 1) * kOffRows * P2 * 8, cudaMemcpyDeviceToHost);
+        if (chain1 && N1 > 2)
+            KS_COPY(c, chain1, keys1 + 2 * key_words, (size_t)(N1 - 2) * key_words * 8, cudaMemcpyDeviceToHost);
+        if (chain2 && N2 > 2)
+            KS_COPY(c, chain2, keys2 + 2 * key_words, (size_t)(N2 - 2) * key_words * 8, cudaMemcpyDeviceToHost);
+        float ms_ = 0;
+        KS_CUDA(c, cudaEventElapsedTime(&ms_, e0, e1));
+        if (device_ms) *device_ms = ms_;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return rc;
+}
 
 extern "C" {
 

@@ -81,6 +81,7 @@ SIGNATURES = {
     "kspir_client_key_bytes": (_sz, [_vp]),
     "kspir_debug_scan_fault": (_i, [_vp, ctypes.c_int64, ctypes.c_long]),
     "kspir_set_fused": (_i, [_vp, _i]),
+    "kspir_gen_autokey_from_offline": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "kspir_get_fused": (_i, [_vp]),
     "kspir_server_create": (_i, [_vp, _vp, _vp]),
     "kspir_server_destroy": (_i, [_vp]),
@@ -373,6 +374,22 @@ class Context:
 
     def sync(self):
         self._check(self.lib.kspir_sync(self._h))
+
+    def gen_autokey_from_offline(self, offline1, offline2, auto1, auto2):
+        """Reference genAutoKeyFromOffline (twosteps.cpp:1749-1864) on the
+        device: dict(chain1, chain2, baby, giant, device_ms) in the layouts of
+        kspir_gen_autokey_from_offline."""
+        ins = [_u64(a).reshape(-1) for a in (offline1, offline2, auto1, auto2)]
+        N1, N2 = self.N1, self.N2
+        out = {"chain1": np.empty(max(N1 - 2, 0) * 12 * N, np.uint64),
+               "chain2": np.empty(max(N2 - 2, 0) * 12 * N, np.uint64),
+               "baby": np.empty((N1 - 1) * 12 * N, np.uint64), "giant": np.empty((N2 - 1) * 6 * N, np.uint64)}
+        ms = ctypes.c_float()
+        self._check(self.lib.kspir_gen_autokey_from_offline(self._h, *[ptr(a) for a in ins], ptr(out["chain1"]),
+                                                            ptr(out["chain2"]), ptr(out["baby"]), ptr(out["giant"]),
+                                                            ctypes.byref(ms)))
+        out["device_ms"] = ms.value
+        return out
 
     def set_fused(self, enable: bool):
         """Single answers as the one fused kernel (kspir_set_fused)."""

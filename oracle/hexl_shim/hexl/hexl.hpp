@@ -17,8 +17,15 @@
 //     i.e. (a+b >= q ? a+b-q : a+b) and (a >= b ? a-b : a+q-b).  These keep
 //     HEXL's behaviour on the one non-canonical operand the reference feeds
 //     them (a word equal to q, from `modulus - 0`).
-//   * EltwiseMultMod / EltwiseFMAMod / EltwiseReduceMod: exact canonical
-//     modular results.
+//   * EltwiseMultMod / EltwiseFMAMod: exact canonical modular results.
+//   * EltwiseReduceMod(result, operand, n, q, input_mod_factor,
+//     output_mod_factor): HEXL documents that the operand is assumed to lie in
+//     [0, input_mod_factor * q) and reduces it to [0, output_mod_factor * q);
+//     with equal factors there is nothing to reduce and HEXL copies the
+//     operand unchanged.  The reference's offline key derivation calls it with
+//     factors (1, 1) on words that are not below q (twosteps.cpp:1776-1777,
+//     1793-1794), so this restatement copies there too; every other call
+//     reduces exactly.
 //
 // The transforms use Harvey's lazy butterflies with Shoup precomputation on
 // 64-bit words (valid for q < 2^62); every value they return is the exact
@@ -296,8 +303,12 @@ inline void EltwiseFMAMod(uint64_t* result, const uint64_t* arg1, uint64_t arg2,
 }
 
 inline void EltwiseReduceMod(uint64_t* result, const uint64_t* operand, uint64_t n,
-                             uint64_t modulus, uint64_t /*input_mod_factor*/,
-                             uint64_t /*output_mod_factor*/) {
+                             uint64_t modulus, uint64_t input_mod_factor,
+                             uint64_t output_mod_factor) {
+    if (input_mod_factor == output_mod_factor) {
+        if (result != operand) std::memcpy(result, operand, n * sizeof(uint64_t));
+        return;
+    }
     for (uint64_t i = 0; i < n; i++) result[i] = operand[i] % modulus;
 }
 

@@ -118,6 +118,7 @@ def ref():
             L.ref_pir_keep_raw.argtypes = [ctypes.c_int]
             L.ref_pir_get_raw.argtypes = [vp]
             L.ref_db_preprocess.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp]
+            L.ref_gen_autokey_from_offline.argtypes = [ctypes.c_int] + [vp] * 9
             L.ref_database_tobsgsntt.argtypes = [vp, ctypes.c_int, vp]
             L.ref_database_tocrt.argtypes = [vp, ctypes.c_int, vp]
             L.ref_pir_get_secret.argtypes = [vp]
@@ -286,3 +287,37 @@ def crt_compose(x: int, y: int) -> int:
 
 def barrett_coeff(v: int, n: int) -> int:
     return lib().ko_barrett_coeff(v, n)
+
+
+# ---------------------------------------------------------------------------
+# offline key derivation (reference genAutoKeyFromOffline, twosteps.cpp:1749-1864)
+
+AUXMOD = 268361729          # crt.h:37
+CRTBAMOD = BSMOD * AUXMOD   # crt.h:51
+
+
+def gen_offline_keys(seed: int) -> dict:
+    """Seeded input keys of the derivation (any words canonical for their
+    moduli): offline1 [10][2][N] (rows 0-4 mod crtMod, 5-9 mod crtBaMod),
+    offline2 [10][2][N] (5-9 mod auxMod), auto1 [6][2][N] (3-5 mod crtBaMod),
+    auto2 [6][2][N] (3-5 mod auxMod)."""
+    rng = np.random.default_rng(np.random.SeedSequence([seed, 0x0FF]))
+
+    def key(rows, m2):
+        k = np.empty((2 * rows, 2, N), np.uint64)
+        k[:rows] = rng.integers(0, CRTMOD, (rows, 2, N), dtype=np.uint64)
+        k[rows:] = rng.integers(0, m2, (rows, 2, N), dtype=np.uint64)
+        return k.reshape(-1)
+    return dict(offline1=key(5, CRTBAMOD), offline2=key(5, AUXMOD), auto1=key(3, CRTBAMOD), auto2=key(3, AUXMOD))
+
+
+def ref_gen_autokey_from_offline(N1: int, keys: dict) -> dict:
+    """The reference build's genAutoKeyFromOffline on these input keys."""
+    N2 = N // 2 // N1
+    out = dict(chain1=np.zeros(max(N1 - 2, 0) * 12 * N, np.uint64), chain2=np.zeros(max(N2 - 2, 0) * 12 * N, np.uint64),
+               baby=np.zeros((N1 - 1) * 12 * N, np.uint64), giant=np.zeros((N2 - 1) * 6 * N, np.uint64))
+    t = ctypes.c_double()
+    ref().ref_gen_autokey_from_offline(N1, *[_p(keys[k]) for k in ("offline1", "offline2", "auto1", "auto2")],
+                                       *[_p(out[k]) for k in ("chain1", "chain2", "baby", "giant")], ctypes.byref(t))
+    out["seconds"] = t.value
+    return out

@@ -401,4 +401,66 @@ void ref_decompose_rlwe(const uint64_t* a, const uint64_t* b, int ellnum, uint64
     for (int j = 0; j < 2 * ellnum; j++) memcpy(out + (size_t)j * kPoly, r[j].data(), kPoly * 8);
 }
 
+// ---------------------------------------------------------------------------
+// Offline key derivation (reference genAutoKeyFromOffline, twosteps.cpp:1749-1864,
+// evalAutoRNSKey :1587-1743) with the key parameters of
+// tests/test-two-steps-key.cpp:149-155.  The caller supplies the four input
+// keys (any words canonical for their moduli: the derivation is arithmetic on
+// them; the test's own key generation needs HEXL's default NTT root for the
+// composite crtBaMod, which HEXL draws at random).  Layouts (u64 words):
+//   offline1 [10][2][N]  offlineKey1.keyMap[5]: rows 0-4 mod crtMod, 5-9 mod crtBaMod, NTT form
+//   offline2 [10][2][N]  offlineKey2.keyMap[5^N1]: rows 0-4 mod crtMod, 5-9 mod auxMod
+//   auto1    [6][2][N]   autoKey1.keyMap[5]: rows 0-2 mod crtMod, 3-5 mod crtBaMod
+//   auto2    [6][2][N]   autoKey2.keyMap[5^N1]: rows 0-2 mod crtMod, 3-5 mod auxMod
+//   chain1   [N1-2][6][2][N]  autoKey1.keyMap[5^i], i = 2..N1-1, after the derivation
+//   chain2   [N2-2][6][2][N]  autoKey2.keyMap[5^(N1 i)], i = 2..N2-1
+//   baby_out [N1-1][6][2][N]  result.keyMap[5^i], i = 1..N1-1
+//   giant_out [N2-1][3][2][N] result.keyMap[5^(N1 i)], i = 1..N2-1
+
+namespace {
+
+// (params.h defines `ell` as a macro: the row count is `rows` here)
+std::vector<RlweCiphertext> flat_to_keys(const uint64_t* p, int rows, uint64_t m1, uint64_t m2) {
+    std::vector<RlweCiphertext> v(rows, RlweCiphertext(N, m1));
+    for (int j = 0; j < rows; j++) v.push_back(RlweCiphertext(N, m2));
+    for (int j = 0; j < 2 * rows; j++) load_rlwe(v[j], p + (size_t)j * 2 * kPoly, true);
+    return v;
+}
+
+void keys_to_flat(uint64_t* p, const std::vector<RlweCiphertext>& v) {
+    for (size_t j = 0; j < v.size(); j++) store_rlwe(p + j * 2 * kPoly, v[j]);
+}
+
+}  // namespace
+
+// genAutoKeyFromOffline(result, autoKey1, autoKey2, offlineKey1, offlineKey2, N1)
+// on key objects rebuilt from the flat inputs (NTT form, as keyGen leaves them).
+void ref_gen_autokey_from_offline(int N1, const uint64_t* offline1, const uint64_t* offline2, const uint64_t* auto1,
+                                  const uint64_t* auto2, uint64_t* chain1, uint64_t* chain2, uint64_t* baby_out,
+                                  uint64_t* giant_out, double* seconds) {
+    const int N2 = N / 2 / N1;
+    AutoKeyBSGSRNS offlineKey1(N, crtMod, crtBaMod, 5, 0x01 << 18, 0x01 << 18);
+    AutoKeyBSGSRNS offlineKey2(N, crtMod, auxMod, 5, 0x01 << 14, 0x01 << 14);
+    AutoKeyBSGSRNS autoKey1(N, crtMod, crtBaMod, 3, (0x01 << 20) * auxMod, 0x01 << 20);
+    AutoKeyBSGSRNS autoKey2(N, crtMod, auxMod, 3, (0x01 << 11) * auxMod, 0x01 << 15);
+    const int32_t i1 = pow_mod(5, 1, 2 * N), iN1 = pow_mod(5, N1, 2 * N);
+    offlineKey1.keyMap.insert(std::make_pair(i1, flat_to_keys(offline1, 5, crtMod, crtBaMod)));
+    offlineKey2.keyMap.insert(std::make_pair(iN1, flat_to_keys(offline2, 5, crtMod, auxMod)));
+    autoKey1.keyMap.insert(std::make_pair(i1, flat_to_keys(auto1, 3, crtMod, crtBaMod)));
+    autoKey2.keyMap.insert(std::make_pair(iN1, flat_to_keys(auto2, 3, crtMod, auxMod)));
+    AutoKeyBSGSRNS result(N, crtMod, bsMod);
+    auto t0 = std::chrono::high_resolution_clock::now();
+    genAutoKeyFromOffline(result, autoKey1, autoKey2, offlineKey1, offlineKey2, N1);
+    auto t1 = std::chrono::high_resolution_clock::now();
+    if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
+    for (int i = 2; chain1 && i <= N1 - 1; i++)
+        keys_to_flat(chain1 + (size_t)(i - 2) * 6 * 2 * kPoly, autoKey1.keyMap.at(pow_mod(5, i, 2 * N)));
+    for (int i = 2; chain2 && i <= N2 - 1; i++)
+        keys_to_flat(chain2 + (size_t)(i - 2) * 6 * 2 * kPoly, autoKey2.keyMap.at(pow_mod(5, N1 * i, 2 * N)));
+    for (int i = 1; baby_out && i <= N1 - 1; i++)
+        keys_to_flat(baby_out + (size_t)(i - 1) * 6 * 2 * kPoly, result.keyMap.at(pow_mod(5, i, 2 * N)));
+    for (int i = 1; giant_out && i <= N2 - 1; i++)
+        keys_to_flat(giant_out + (size_t)(i - 1) * 3 * 2 * kPoly, result.keyMap.at(pow_mod(5, N1 * i, 2 * N)));
+}
+
 }  // extern "C"

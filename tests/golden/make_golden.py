@@ -12,7 +12,10 @@ Runs the reference's own sources (compiled by ``make -C oracle ref`` into
   raw databases (``kspir_b200.synth.gen_raw_db``), of an edge-value pattern
   and of the database test-pir.cpp samples -- input and output digests;
 * small unit vectors of the reference helpers (crt_compose, barrett_coeff,
-  the decompositions) on edge values.
+  the decompositions) on edge values;
+* the offline key derivation (genAutoKeyFromOffline) of seeded input keys
+  (``oracle.pyoracle.gen_offline_keys``) at N1 = 64 (tests/test-two-steps-key.cpp)
+  and 128 -- digests of every output key map.
 
 Usage:  python tests/golden/make_golden.py   (needs /root/reference to build oracle/_ref)
 """
@@ -38,6 +41,7 @@ CASES = [(2, 128, 5), (1, 128, 3), (4, 64, 7), (2, 256, 11)]
 TESTPIR = (1, 16, 128)   # seed, r, N1
 PREPROCESS = [(31, 1, 128), (32, 1, 64), (33, 1, 256), (34, 2, 128)]
 PREPROCESS_TESTPIR = (3, 2, 128)
+OFFLINE = [(41, 64), (42, 128)]   # seed, N1
 
 
 def sha(a: np.ndarray) -> str:
@@ -145,6 +149,14 @@ def main():
         L.ref_ntt(po._p(y), m, 0)
         ntt[str(m)] = dict(in_sha=sha(x), out_sha=sha(y), out_head=head(y))
     out["units"]["ntt"] = ntt
+    off = []
+    for seed, N1 in OFFLINE:
+        keys = po.gen_offline_keys(seed)
+        res = po.ref_gen_autokey_from_offline(N1, keys)
+        off.append(dict(seed=seed, N1=N1, inputs_sha={k: sha(v) for k, v in keys.items()},
+                        **{k + "_sha": sha(res[k]) for k in ("chain1", "chain2", "baby", "giant")},
+                        giant_head=head(res["giant"])))
+    out["offline"] = off
     with open(os.path.join(HERE, "golden.json"), "w") as f:
         json.dump(out, f, indent=1)
     print("wrote", os.path.join(HERE, "golden.json"), file=sys.stderr)

@@ -222,6 +222,17 @@ def test_packing_leaves_rlwes_like_the_reference(r):
 
 
 @needs_ref
+@pytest.mark.parametrize("case", GOLDEN["offline"], ids=lambda c: f"N1_{c['N1']}")
+def test_offline_derivation_reference_matches_golden(case):
+    # the reference build's genAutoKeyFromOffline on the seeded input keys
+    keys = po.gen_offline_keys(case["seed"])
+    assert {k: sha(v) for k, v in keys.items()} == case["inputs_sha"]
+    res = po.ref_gen_autokey_from_offline(case["N1"], keys)
+    for k in ("chain1", "chain2", "baby", "giant"):
+        assert sha(res[k]) == case[k + "_sha"], k
+
+
+@needs_ref
 def test_testpir_replay_known_answer():
     g = GOLDEN["testpir"]
     seed, r, N1 = g["seed"], g["r"], g["N1"]
