@@ -207,7 +207,12 @@ int kspir_answer(kspir_ctx* ctx, int client, const uint64_t* query, uint64_t* re
 
 /* Same on device buffers (query [2][2][N], response [2][N]), enqueued on
  * `stream` (a cudaStream_t, or NULL for the context's stream); returns once
- * enqueued.  Call kspir_sync to wait and collect device-side errors. */
+ * enqueued.  Call kspir_sync to wait and collect device-side errors.
+ * Successive calls rotate over min(max_inflight, 4) workspace slots (each
+ * waits, on its stream, for the last answer that used its slot), so answers
+ * issued on different streams run at the same time: one answer's key
+ * switches overlap another's database scan.  With the fused answer on
+ * (kspir_set_fused) every call uses slot 0. */
 int kspir_answer_device(kspir_ctx* ctx, int client, const uint64_t* d_query, uint64_t* d_response, void* stream);
 int kspir_sync(kspir_ctx* ctx);
 

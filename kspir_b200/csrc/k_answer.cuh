@@ -149,8 +149,10 @@ __device__ __noinline__ bool fa_wait_counter(int* cnt, int idx, int target, uint
     const int* c = cnt + idx;
     if (ld_acquire_gpu(c) >= target) return true;
     const uint64_t t0 = globaltimer_ns();
-    for (;;) {
-        __nanosleep(128);
+    // exponential backoff from 64 ns to 2 us: a waiter polls L2, which the
+    // database stream is saturating
+    for (unsigned ns = 64;; ns = ns < 2048 ? 2 * ns : ns) {
+        __nanosleep(ns);
         if (ld_acquire_gpu(c) >= target) return true;
         if (*reinterpret_cast<volatile const int*>(cnt + FC_ABORT)) return false;
         if (globaltimer_ns() - t0 > limit_ns) {

@@ -170,6 +170,7 @@ GadgetBsgs make_gadget_bsgs(int ell, uint64_t base, uint64_t bg) {
 size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 constexpr int kTimingRing = 512;   // event sets of recent launches kept for kspir_timing_summary
+constexpr int kSingleSlots = 4;    // workspace slots device-buffer single answers rotate over
 constexpr int kMaxBatch = 256;     // queries per launch
 
 struct ClientList {
@@ -278,6 +279,13 @@ struct kspir_ctx {
     uint32_t* fa_acc = nullptr;
     unsigned long long* fa_times = nullptr;
     std::vector<char> ring_fused;
+    // device-buffer single answers rotate over the first single_slots
+    // workspace slots, so answers issued on different streams overlap; each
+    // slot's last answer is marked by slot_done (waited for before reuse)
+    int single_slots = 1;
+    int next_single = 0;
+    std::vector<cudaEvent_t> slot_done;
+    std::vector<char> slot_used;
     std::mutex mu;            // serialises enqueues from several host threads
 };
 
@@ -918,6 +926,24 @@ int finish(kspir_ctx* c, int slot0, int nq) {
     return KSPIR_OK;
 }
 
+// Orders `st` after every device-buffer single answer still using a workspace
+// slot (they may run on other streams).
+int wait_singles(kspir_ctx* c, cudaStream_t st) {
+    for (int i = 0; i < c->single_slots; i++)
+        if (c->slot_used[i]) KS_CUDA(c, cudaStreamWaitEvent(st, c->slot_done[i], 0));
+    return KSPIR_OK;
+}
+
+// Marks every single-answer slot as used by work just enqueued on `st`, so a
+// later device-buffer single answer (on any stream) is ordered after it.
+int mark_singles(kspir_ctx* c, cudaStream_t st) {
+    for (int i = 0; i < c->single_slots; i++) {
+        KS_CUDA(c, cudaEventRecord(c->slot_done[i], st));
+        c->slot_used[i] = 1;
+    }
+    return KSPIR_OK;
+}
+
 // the tensor-core database operand, rebuilt from the resident database
 int build_dbop(kspir_ctx* c) {
     if (!c->mma) return KSPIR_OK;
@@ -1126,6 +1152,10 @@ int kspir_ctx_create(int device, const kspir_params* params, kspir_ctx** out) {
     c->ring_nq.assign(kTimingRing, 0);
     for (auto& evs : c->ring)
         for (auto& e : evs) KS_CUDA(c.get(), cudaEventCreate(&e));
+    c->single_slots = std::min(p.max_inflight, kSingleSlots);
+    c->slot_done.assign(c->single_slots, nullptr);
+    c->slot_used.assign(c->single_slots, 0);
+    for (auto& e : c->slot_done) KS_CUDA(c.get(), cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     rc = init_key_slots(c.get());
     if (rc) return rc;
     rc = init_workspaces(c.get());
@@ -1144,6 +1174,7 @@ int kspir_ctx_destroy(kspir_ctx* c) {
     cudaStreamSynchronize(c->stream);
     for (auto& evs : c->ring)
         for (auto& e : evs) if (e) cudaEventDestroy(e);
+    for (auto& e : c->slot_done) if (e) cudaEventDestroy(e);
     for (auto& kv : c->graphs)
         for (auto& g : kv.second.g) if (g) cudaGraphExecDestroy(g);
     if (c->capture) cudaStreamDestroy(c->capture);
@@ -1185,6 +1216,7 @@ int kspir_db_upload(kspir_ctx* c, const uint64_t* datacrt, size_t words) {
     if (words != need) return set_err(c, KSPIR_ERR_INVALID_ARG, "database size must be r*N*N/2 words");
     std::lock_guard<std::mutex> lk(c->mu);
     KS_CUDA(c, cudaSetDevice(c->device));
+    if (int wrc = wait_singles(c, c->stream)) return wrc;
     if (!c->db) KS_CUDA(c, cudaMalloc(&c->db, need * 8));
     KS_COPY(c, c->db, datacrt, need * 8, cudaMemcpyHostToDevice);
     int rc = build_dbop(c);
@@ -1262,6 +1294,7 @@ int kspir_db_preprocess(kspir_ctx* c, const uint64_t* data, size_t words, float*
     if (words != need) return set_err(c, KSPIR_ERR_INVALID_ARG, "raw database must be r*N*N/2 words");
     std::lock_guard<std::mutex> lk(c->mu);
     KS_CUDA(c, cudaSetDevice(c->device));
+    if (int wrc = wait_singles(c, c->stream)) return wrc;
     uint64_t* d_raw = nullptr;
     KS_CUDA(c, cudaMalloc(&d_raw, need * 8));
     int rc = copy_sync(c, d_raw, data, need * 8, cudaMemcpyHostToDevice);
@@ -1276,6 +1309,7 @@ int kspir_db_preprocess_device(kspir_ctx* c, const uint64_t* d_data, size_t word
         return set_err(c, KSPIR_ERR_INVALID_ARG, "raw database must be r*N*N/2 words");
     std::lock_guard<std::mutex> lk(c->mu);
     KS_CUDA(c, cudaSetDevice(c->device));
+    if (int wrc = wait_singles(c, c->stream)) return wrc;
     return db_preprocess_dev(c, d_data, device_ms);
 }
 
@@ -1293,6 +1327,7 @@ int kspir_database_tobsgsntt(kspir_ctx* c, const uint64_t* data, uint64_t* resul
     if (!c || !data || !result) return KSPIR_ERR_INVALID_ARG;
     std::lock_guard<std::mutex> lk(c->mu);
     KS_CUDA(c, cudaSetDevice(c->device));
+    if (int wrc = wait_singles(c, c->stream)) return wrc;
     int rc = ensure_db_tables(c);
     if (!rc) rc = ensure_prep_buffers(c);
     if (rc) return rc;
@@ -1323,6 +1358,7 @@ int kspir_database_tocrt(kspir_ctx* c, const uint64_t* data_ntt, uint64_t* datac
     if (!c || !data_ntt || !datacrt) return KSPIR_ERR_INVALID_ARG;
     std::lock_guard<std::mutex> lk(c->mu);
     KS_CUDA(c, cudaSetDevice(c->device));
+    if (int wrc = wait_singles(c, c->stream)) return wrc;
     int rc = ensure_prep_buffers(c);
     if (rc) return rc;
     uint64_t* d_rows = c->prep_dev + kSubWords;
@@ -1464,6 +1500,7 @@ extern "C" int kspir_gen_autokey_from_offline(kspir_ctx* c, const uint64_t* offl
         return set_err(c, KSPIR_ERR_INVALID_ARG, "key word not canonical");
     std::lock_guard<std::mutex> lk(c->mu);
     KS_CUDA(c, cudaSetDevice(c->device));
+    if (int wrc = wait_singles(c, c->stream)) return wrc;
     cudaStream_t st = c->stream;
 
     OffChain baby{};
@@ -1563,6 +1600,7 @@ int kspir_client_queries(kspir_ctx* c, int n, const uint64_t* secrets, const uin
     if (!small_secret(secrets, (size_t)n * kN)) return set_err(c, KSPIR_ERR_INVALID_ARG, "secret words must be small");
     std::lock_guard<std::mutex> lk(c->mu);
     KS_CUDA(c, cudaSetDevice(c->device));
+    if (int wrc = wait_singles(c, c->stream)) return wrc;
     int rc = ensure_client_tables(c);
     if (rc) return rc;
     const size_t sw = (size_t)n * kN, qw = (size_t)n * 4 * kN, rw = (size_t)n * 6 * kN;
@@ -1593,6 +1631,7 @@ int kspir_client_decrypt(kspir_ctx* c, int n, const uint64_t* secrets, const uin
         return set_err(c, KSPIR_ERR_INVALID_ARG, "word not canonical");
     std::lock_guard<std::mutex> lk(c->mu);
     KS_CUDA(c, cudaSetDevice(c->device));
+    if (int wrc = wait_singles(c, c->stream)) return wrc;
     // QInv(r, crtMod) (utils.cpp:118-190) is r^-1 mod crtMod for every r of its
     // table; it has no entry for 128 (and returns 0 there)
     const uint64_t qinv = (uint64_t)h_invmod((uint64_t)r % kCrtMod, kCrtMod);
@@ -1623,6 +1662,7 @@ int kspir_db_download(kspir_ctx* c, uint64_t* datacrt, size_t words) {
     if (!c->db_loaded) return set_err(c, KSPIR_ERR_NOT_READY, "database not uploaded");
     std::lock_guard<std::mutex> lk(c->mu);
     KS_CUDA(c, cudaSetDevice(c->device));
+    if (int wrc = wait_singles(c, c->stream)) return wrc;
     KS_COPY(c, datacrt, c->db, need * 8, cudaMemcpyDeviceToHost);
     return KSPIR_OK;
 }
@@ -1808,6 +1848,7 @@ int kspir_db_save(kspir_ctx* c, const char* path) {
     if (!c->db_loaded) return set_err(c, KSPIR_ERR_NOT_READY, "database not uploaded");
     std::lock_guard<std::mutex> lk(c->mu);
     KS_CUDA(c, cudaSetDevice(c->device));
+    if (int wrc = wait_singles(c, c->stream)) return wrc;
     const size_t words = (size_t)c->p.r * kN * (kN / 2);
     FileHeader h{};
     memcpy(h.magic, kDbMagic, 8);
@@ -1839,6 +1880,7 @@ int kspir_db_load(kspir_ctx* c, const char* path) {
     if (!c || !path) return KSPIR_ERR_INVALID_ARG;
     std::lock_guard<std::mutex> lk(c->mu);
     KS_CUDA(c, cudaSetDevice(c->device));
+    if (int wrc = wait_singles(c, c->stream)) return wrc;
     const size_t words = (size_t)c->p.r * kN * (kN / 2);
     FILE* f = fopen(path, "rb");
     if (!f) return set_err(c, KSPIR_ERR_IO, std::string("cannot open ") + path);
@@ -1889,6 +1931,7 @@ int kspir_perms_upload(kspir_ctx* c, const int32_t* perms, size_t count) {
         if (perms[i] < 0 || perms[i] >= kN) return set_err(c, KSPIR_ERR_INVALID_ARG, "permutation entry out of range");
     std::lock_guard<std::mutex> lk(c->mu);
     KS_CUDA(c, cudaSetDevice(c->device));
+    if (int wrc = wait_singles(c, c->stream)) return wrc;
     KS_COPY(c, c->perms, perms, count * 4, cudaMemcpyHostToDevice);
     c->perms_loaded = true;
     return KSPIR_OK;
@@ -1901,6 +1944,7 @@ int kspir_client_keys_upload(kspir_ctx* c, int client, const uint64_t* baby, con
     if (c->levels > 0 && !packing) return KSPIR_ERR_INVALID_ARG;
     std::lock_guard<std::mutex> lk(c->mu);
     KS_CUDA(c, cudaSetDevice(c->device));
+    if (int wrc = wait_singles(c, c->stream)) return wrc;
     const size_t nb_poly = (size_t)c->N1h * 3 * 2;                 // crt rows and bs rows each
     const size_t ng_poly = (size_t)(c->N2 - 1) * 2 * 2;
     const size_t np_poly = (size_t)c->levels * 4 * 2;
@@ -1955,10 +1999,16 @@ int kspir_answer_device(kspir_ctx* c, int client, const uint64_t* d_query, uint6
     std::lock_guard<std::mutex> lk(c->mu);
     cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
     KS_CUDA(c, cudaSetDevice(c->device));
-    KS_CUDA(c, cudaMemcpyAsync(c->bq64, d_query, 4 * kN * 8, cudaMemcpyDeviceToDevice, st));
-    rc = enqueue_answer(c, 0, 1, &client, st, true);
+    // the fused answer has one set of counters: it always runs in slot 0
+    const int slot = c->fused ? 0 : c->next_single;
+    if (!c->fused) c->next_single = (slot + 1) % c->single_slots;
+    if (c->slot_used[slot]) KS_CUDA(c, cudaStreamWaitEvent(st, c->slot_done[slot], 0));
+    KS_CUDA(c, cudaMemcpyAsync(c->bq64 + (size_t)slot * 4 * kN, d_query, 4 * kN * 8, cudaMemcpyDeviceToDevice, st));
+    rc = enqueue_answer(c, slot, 1, &client, st, true);
     if (rc) return rc;
-    KS_CUDA(c, cudaMemcpyAsync(d_response, c->bresp, 2 * kN * 8, cudaMemcpyDeviceToDevice, st));
+    KS_CUDA(c, cudaMemcpyAsync(d_response, c->bresp + (size_t)slot * 2 * kN, 2 * kN * 8, cudaMemcpyDeviceToDevice, st));
+    KS_CUDA(c, cudaEventRecord(c->slot_done[slot], st));
+    c->slot_used[slot] = 1;
     KS_CUDA(c, cudaGetLastError());
     return KSPIR_OK;
 }
@@ -1983,6 +2033,7 @@ int kspir_answer(kspir_ctx* c, int client, const uint64_t* query, uint64_t* resp
     if (!query || !response) return KSPIR_ERR_INVALID_ARG;
     std::lock_guard<std::mutex> lk(c->mu);
     KS_CUDA(c, cudaSetDevice(c->device));
+    if (int wrc = wait_singles(c, c->stream)) return wrc;
     KS_CUDA(c, cudaMemcpyAsync(c->bq64, query, 4 * kN * 8, cudaMemcpyHostToDevice, c->stream));
     rc = enqueue_answer(c, 0, 1, &client, c->stream, true);
     if (rc) return rc;
@@ -2008,12 +2059,13 @@ int kspir_answer_batch_device(kspir_ctx* c, int n, const int32_t* clients, const
     std::lock_guard<std::mutex> lk(c->mu);
     cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
     KS_CUDA(c, cudaSetDevice(c->device));
+    if (int wrc = wait_singles(c, st)) return wrc;
     KS_CUDA(c, cudaMemcpyAsync(c->bq64, d_queries, (size_t)n * 4 * kN * 8, cudaMemcpyDeviceToDevice, st));
     rc = enqueue_answer(c, 0, n, clients, st);
     if (rc) return rc;
     KS_CUDA(c, cudaMemcpyAsync(d_responses, c->bresp, (size_t)n * 2 * kN * 8, cudaMemcpyDeviceToDevice, st));
     KS_CUDA(c, cudaGetLastError());
-    return KSPIR_OK;
+    return mark_singles(c, st);
 }
 
 int kspir_answer_batch(kspir_ctx* c, int n, const int32_t* clients, const uint64_t* queries, uint64_t* responses) {
@@ -2025,6 +2077,7 @@ int kspir_answer_batch(kspir_ctx* c, int n, const int32_t* clients, const uint64
         if ((rc = check_client(c, clients[i]))) return rc;
     std::lock_guard<std::mutex> lk(c->mu);
     KS_CUDA(c, cudaSetDevice(c->device));
+    if (int wrc = wait_singles(c, c->stream)) return wrc;
     KS_CUDA(c, cudaMemcpyAsync(c->bq64, queries, (size_t)n * 4 * kN * 8, cudaMemcpyHostToDevice, c->stream));
     rc = enqueue_answer(c, 0, n, clients, c->stream);
     if (rc) return rc;
@@ -2048,6 +2101,7 @@ int kspir_tune_batch(kspir_ctx* c, int n, int* kind_out, float* ms_out) {
     if (n < 1 || n > c->p.max_inflight || n > kMaxBatch) return set_err(c, KSPIR_ERR_INVALID_ARG, "batch size");
     std::lock_guard<std::mutex> lk(c->mu);
     KS_CUDA(c, cudaSetDevice(c->device));
+    if (int wrc = wait_singles(c, c->stream)) return wrc;
     cudaEvent_t e0, e1;
     KS_CUDA(c, cudaEventCreate(&e0));
     KS_CUDA(c, cudaEventCreate(&e1));
@@ -2185,6 +2239,7 @@ int kspir_matrix_vector_mul_bsgs_rns_crt_large(kspir_ctx* c, int client, uint64_
     const Workspace w = ws_host(c, 0);
     cudaStream_t st = c->stream;
     KS_CUDA(c, cudaSetDevice(c->device));
+    if (int wrc = wait_singles(c, c->stream)) return wrc;
     KS_CUDA(c, cudaMemcpyAsync(c->bq64, query_inout, 4 * kN * 8, cudaMemcpyHostToDevice, st));
     k_set_clients<<<1, 32, 0, st>>>(c->client_of, 0, ClientList{1, {client}});
     enqueue_baby(c, 0, 1, false, st);
@@ -2222,6 +2277,7 @@ int kspir_external_product(kspir_ctx* c, int client, uint64_t* result, uint64_t*
     const Workspace w = ws_host(c, 0);
     cudaStream_t st = c->stream;
     KS_CUDA(c, cudaSetDevice(c->device));
+    if (int wrc = wait_singles(c, c->stream)) return wrc;
     k_set_clients<<<1, 32, 0, st>>>(c->client_of, 0, ClientList{1, {client}});
     uint64_t* words = reinterpret_cast<uint64_t*>(c->stage32);     // r*2*N u64 fit in r*4*N u32
     // first_dim -> ws.result residues; the caller's accumulators (NTT domain) -> ws.sout residues
@@ -2254,6 +2310,7 @@ int kspir_packing_rlwes(kspir_ctx* c, int client, uint64_t* rlwes, uint64_t* res
     const Workspace w = ws_host(c, 0);
     cudaStream_t st = c->stream;
     KS_CUDA(c, cudaSetDevice(c->device));
+    if (int wrc = wait_singles(c, c->stream)) return wrc;
     k_set_clients<<<1, 32, 0, st>>>(c->client_of, 0, ClientList{1, {client}});
     uint64_t* words = reinterpret_cast<uint64_t*>(c->stage32);
     KS_CUDA(c, cudaMemcpyAsync(words, rlwes, n * 8, cudaMemcpyHostToDevice, st));
@@ -2294,6 +2351,7 @@ int kspir_fetch_stage_slot(kspir_ctx* c, int slot, int stage, uint64_t* out, siz
     const int R = c->p.r;
     cudaStream_t st = c->stream;
     KS_CUDA(c, cudaSetDevice(c->device));
+    if (int wrc = wait_singles(c, c->stream)) return wrc;
     KS_CUDA(c, cudaStreamSynchronize(st));
     if (stage == KSPIR_STAGE_CIPHERBUF) {
         const size_t n = (size_t)kN * c->N1 * 2;

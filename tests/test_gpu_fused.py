@@ -34,7 +34,8 @@ def test_fused_answer_matches_oracle(r):
     with make_ctx(r, db, c) as ctx:
         got = ctx.answer(0, c["query"])
         assert np.array_equal(ctx.fetch_stage(kb.STAGE_RESULT), bsgs), "first-dimension results"
-        assert np.array_equal(ctx.fetch_stage(kb.STAGE_EXT), ext), "external products"
+        if r <= 2:   # from two packing levels on, the tree reuses the external products' buffer
+            assert np.array_equal(ctx.fetch_stage(kb.STAGE_EXT), ext), "external products"
         assert np.array_equal(got, want), "response"
         tot, ph = ctx.last_timing()
         assert tot > 0 and all(p >= 0 for p in ph)
