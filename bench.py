@@ -8,11 +8,15 @@ with N = 4096, N1 = 128, N2 = 16 (reference tests/test-pir.cpp:14-29).
 Synthetic, seeded inputs of that shape (kspir_b200.synth).
 
 Reported (one JSON line on rank 0):
-  value      whole-job queries/s of the plain single-query answer, inputs
-             resident in HBM, device-timed with CUDA events on the launching
-             stream (max over ranks)
-  e2e        queries/s through the public C ABI (kspir_answer) with the
-             query in pinned host memory and the response read back, per step
+  value      whole-job queries/s of single-query answers, inputs resident in
+             HBM, issued round-robin on --streams streams so one answer's key
+             switches overlap another's database scan; device-timed with CUDA
+             events on the launching stream (max over ranks).  latency_ms is
+             one answer at a time on one stream, with its phases
+  e2e        queries/s through the public C ABI (kspir_answer, blocking) from
+             --streams host threads, each query in pinned host memory and its
+             response read back, per step; one_caller_queries_per_s from one
+             thread
   roofline   the dominant kernel (the database scan): algorithmic bytes per
              launch (r * N * N/2 * 8 = 1 GiB) / its mean CUDA-event duration
   batched    the batched answer (kspir_answer_batch) at B = 1, 8, 32, 64, 128
@@ -60,6 +64,8 @@ def parse():
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--streams", type=int, default=3,
+                    help="streams (and host threads, end to end) the single answers are issued on")
     ap.add_argument("--batches", default="1,8,32,64,128", help="batch sizes of the batched sweep ('' = none)")
     ap.add_argument("--clients", type=int, default=128, help="distinct client key sets of the batched sweep")
     ap.add_argument("--no-extras", dest="extras", action="store_false",
@@ -318,8 +324,13 @@ def run_gpu(args, rank, world, local_rank):
     stream = torch.cuda.Stream()
     host_ref = ctx.answer(0, cl["query"])   # host path, for a consistency check of the device path
 
-    def step():
-        ctx.answer_device(0, dq.data_ptr(), dr.data_ptr(), stream.cuda_stream)
+    S = max(1, args.streams)
+    streams = [stream] + [torch.cuda.Stream() for _ in range(S - 1)]
+    drs = [dr] + [torch.empty(2 * N, dtype=torch.int64, device="cuda") for _ in range(S - 1)]
+
+    def step(i=0):
+        k = i % S
+        ctx.answer_device(0, dq.data_ptr(), drs[k].data_ptr(), streams[k].cuda_stream)
 
     with torch.cuda.stream(stream):
         for _ in range(max(args.warmup, 3)):
@@ -328,44 +339,77 @@ def run_gpu(args, rank, world, local_rank):
     if not np.array_equal(dr.cpu().numpy().view(np.uint64), host_ref):
         raise RuntimeError("device-path response differs from the host-path response")
 
-    ctx.timing_reset()
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(local_rank) as clocks:
-        ev0.record(stream)
-        for _ in range(args.steps):
-            step()
-        ev1.record(stream)
+    def timed(nstreams):
+        """Device time of args.steps answers issued round-robin on `nstreams`
+        streams, bracketed by events on the main stream."""
+        main = torch.cuda.current_stream()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        if dist:
+            dist.barrier()
         torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    ms = ev0.elapsed_time(ev1)
-    answers, launches, tot_ms, phases = ctx.timing_summary()
+        ev0.record(main)
+        for st in streams[:nstreams]:
+            st.wait_event(ev0)
+        for i in range(args.steps):
+            step(i % nstreams)
+        for st in streams[:nstreams]:
+            main.wait_stream(st)
+        ev1.record(main)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        return ev0.elapsed_time(ev1)
+
+    # one answer at a time: the latency and its phases
+    ctx.timing_reset()
+    ms_serial = timed(1)
+    answers, _, tot_ms, phases = ctx.timing_summary()
+    # answers on S streams at once: one's key switches overlap another's scan
+    for i in range(3 * S):
+        step(i)
+    torch.cuda.synchronize()
+    ctx.timing_reset()
+    with ClockSampler(local_rank) as clocks:
+        ms = timed(S)
+    _, launches, _, _ = ctx.timing_summary()
     ctx.sync()
+    for k in range(S):
+        if not np.array_equal(drs[k].cpu().numpy().view(np.uint64), host_ref):
+            raise RuntimeError(f"stream {k}: overlapped response differs from the host-path response")
 
-    # end to end through the C ABI: pinned host query in, response out, every step
-    qh = torch.from_numpy(cl["query"].view(np.int64).copy()).pin_memory()
-    rh = torch.empty(2 * N, dtype=torch.int64).pin_memory()
-    qh_np = qh.numpy().view(np.uint64)
-    rh_np = rh.numpy().view(np.uint64)
-    for _ in range(3):
-        ctx.answer(0, qh_np, out=rh_np)
+    # end to end through the C ABI: pinned host query in, response out, every
+    # step; S host threads each call kspir_answer (blocking) on its own buffers
+    qhs = [torch.from_numpy(cl["query"].view(np.int64).copy()).pin_memory() for _ in range(S)]
+    rhs = [torch.empty(2 * N, dtype=torch.int64).pin_memory() for _ in range(S)]
+    qh_np = [q.numpy().view(np.uint64) for q in qhs]
+    rh_np = [r_.numpy().view(np.uint64) for r_ in rhs]
+
+    def e2e_run(nthreads, steps):
+        def worker(t):
+            for _ in range(t, steps, nthreads):
+                ctx.answer(0, qh_np[t], out=rh_np[t])
+        ths = [threading.Thread(target=worker, args=(t,)) for t in range(nthreads)]
+        t0 = time.perf_counter()
+        for th in ths:
+            th.start()
+        for th in ths:
+            th.join()
+        return time.perf_counter() - t0
+
+    e2e_run(S, 3 * S)
     if dist:
         dist.barrier()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        ctx.answer(0, qh_np, out=rh_np)
-    e2e_s = time.perf_counter() - t0
-    if not np.array_equal(rh_np, host_ref):
-        raise RuntimeError("e2e response differs")
+    e2e_s = e2e_run(S, args.steps)
+    e2e_serial_s = e2e_run(1, max(args.steps // 4, 10))
+    for t in range(S):
+        if not np.array_equal(rh_np[t], host_ref):
+            raise RuntimeError("e2e response differs")
 
     if dist:
-        t = torch.tensor([ms, e2e_s], dtype=torch.float64, device="cuda")
+        t = torch.tensor([ms, e2e_s, ms_serial], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, e2e_s = float(t[0]), float(t[1])
+        ms, e2e_s, ms_serial = float(t[0]), float(t[1]), float(t[2])
 
     clients16 = [cl]
     batched = run_batched(args, ctx, batches, nclients, rank, dist, torch, clients16) if batches else None
@@ -399,6 +443,8 @@ def run_gpu(args, rank, world, local_rank):
             "dtype": "u64",
             "data": "synthetic (seeded uniform canonical words; reference shapes)",
             "config": workload_config(args),
+            "streams": S,
+            "latency_ms": ms_serial / args.steps,
             "phases_ms_per_step": {"baby_steps": phases[0] / answers, "db_scan": scan_ms,
                                    "giant_steps": phases[2] / answers, "external_products": phases[3] / answers,
                                    "packing": phases[4] / answers},
@@ -406,11 +452,12 @@ def run_gpu(args, rank, world, local_rank):
                          "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_src,
                          "algorithmic_bytes_per_launch": db_bytes, "traffic": read_traffic(r)},
             "e2e": {"value": world * args.steps / e2e_s, "unit": "queries/s",
-                    "h2d_bytes_per_step": 4 * N * 8, "d2h_bytes_per_step": 2 * N * 8},
+                    "h2d_bytes_per_step": 4 * N * 8, "d2h_bytes_per_step": 2 * N * 8,
+                    "host_threads": S, "one_caller_queries_per_s": world * max(args.steps // 4, 10) / e2e_serial_s},
             # the whole answer against the bytes it must touch: the database,
             # one client's keys and the 8 MiB rotated-query buffer
             "answer_gbs": (db_bytes + ctx.lib.kspir_client_key_bytes(ctx.handle) + N * N1 * 2 * 8)
-                          / (ms / args.steps * 1e-3) / 1e9,
+                          / (ms_serial / args.steps * 1e-3) / 1e9,
             "gpu_launches": int(launches) * world,
             "clocks": clocks.summary(),
         }

@@ -61,7 +61,7 @@ typedef struct kspir_params {
 /* Context bound to one CUDA device.  Allocates the per-query workspaces. */
 int kspir_ctx_create(int device, const kspir_params* params, kspir_ctx** out);
 int kspir_ctx_destroy(kspir_ctx* ctx);
-const char* kspir_last_error(const kspir_ctx* ctx);   /* NULL: the calling thread's last error */
+const char* kspir_last_error(const kspir_ctx* ctx);   /* the calling thread's last error text (any ctx, or NULL) */
 const char* kspir_strerror(int code);
 
 /* Replaces the datacrt argument of matrix_vector_mul_bsgs_rns_crt_large
@@ -202,17 +202,22 @@ int kspir_client_keys_upload(kspir_ctx* ctx, int client, const uint64_t* baby, c
 
 /* The server's online answer, reference tests/test-pir.cpp:110-116
  * (matrix_vector_mul_bsgs_rns_crt_large -> externalProduct x r -> packingRLWEs),
- * host buffers in and out.  The caller's query is not modified. */
+ * host buffers in and out.  The caller's query is not modified.  Blocks until
+ * the response is in `response`.  Safe to call from several host threads at
+ * once: each call owns one of min(max_inflight, 4) workspace slots and its
+ * stream while it runs, and waits for its answer without holding the context,
+ * so up to four concurrent callers' answers overlap on the device (one
+ * answer's key switches with another's database scan).  Pinned host buffers
+ * let the copies run asynchronously. */
 int kspir_answer(kspir_ctx* ctx, int client, const uint64_t* query, uint64_t* response);
 
 /* Same on device buffers (query [2][2][N], response [2][N]), enqueued on
  * `stream` (a cudaStream_t, or NULL for the context's stream); returns once
  * enqueued.  Call kspir_sync to wait and collect device-side errors.
- * Successive calls rotate over min(max_inflight, 4) workspace slots (each
+ * Successive calls rotate over the same workspace slots as kspir_answer (each
  * waits, on its stream, for the last answer that used its slot), so answers
- * issued on different streams run at the same time: one answer's key
- * switches overlap another's database scan.  With the fused answer on
- * (kspir_set_fused) every call uses slot 0. */
+ * issued on different streams run at the same time.  With the fused answer on
+ * (kspir_set_fused) every single answer uses slot 0. */
 int kspir_answer_device(kspir_ctx* ctx, int client, const uint64_t* d_query, uint64_t* d_response, void* stream);
 int kspir_sync(kspir_ctx* ctx);
 

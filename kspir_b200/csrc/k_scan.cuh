@@ -39,6 +39,17 @@ constexpr uint64_t kWaitLimitNs = 2000000000ull;     // 2 s per bounded wait
 // that warp never waits more than one phase ahead of the barrier (an mbarrier
 // parity wait cannot tell phase u-1 from u+1).
 
+// Ring shape of the single-query scan (measured on B200 with a 1 GiB
+// database: 4 consumer warps over 8 stages of 18 KiB streamed at 6.9 TB/s,
+// 6 over 12 at 6.1 TB/s, and the 148 KiB of shared memory leave room for a
+// key-switch CTA of a concurrent answer on the same SM).
+#ifndef KSPIR_SCAN_CONS
+#define KSPIR_SCAN_CONS 4
+#endif
+#ifndef KSPIR_SCAN_NST
+#define KSPIR_SCAN_NST 8
+#endif
+
 template <int N1>
 struct ScanCfg {
     static constexpr int N2 = kN / 2 / N1;
@@ -48,8 +59,8 @@ struct ScanCfg {
     static constexpr int SLAB = kN / 2 * 8;             // DB bytes per item
     static constexpr int QSLAB = 2 * N1 * 8;            // cipherbuf bytes per item
     static constexpr int STAGE = SLAB + QSLAB;
-    static constexpr int CONS = N1 <= 128 ? 6 : 4;      // consumer warps
-    static constexpr int NST = N1 <= 128 ? 12 : 8;      // ring stages, a multiple of CONS
+    static constexpr int CONS = N1 <= 128 ? KSPIR_SCAN_CONS : 4;   // consumer warps
+    static constexpr int NST = N1 <= 128 ? KSPIR_SCAN_NST : 8;     // ring stages, a multiple of CONS
     static constexpr int THREADS = 32 * (CONS + 1);
     static constexpr int SMEM = NST * STAGE + 2 * NST * 8;
     static_assert(NST % CONS == 0, "stages must be owned by one consumer warp each");

@@ -8,6 +8,7 @@
 #include <array>
 #include <cstdio>
 #include <cstdlib>
+#include <condition_variable>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -203,7 +204,6 @@ struct kspir_ctx {
     kspir_params p{};
     int N1 = 0, N2 = 0, N1h = 0, levels = 0;
     cudaStream_t stream = nullptr;
-    std::string err;
     uint64_t* db = nullptr;
     bool db_loaded = false;
     bool mma = false;                 // batched tensor-core scan enabled (N1 = 128, several slots)
@@ -232,6 +232,7 @@ struct kspir_ctx {
     NttTables ntabs{};
     PathGadgets gad{};
     int nsm = 148;
+    int scan_ctas = 148;      // CTAs of the single-query scan (KSPIR_SCAN_CTAS, default every SM)
     // workspaces: slot s is slot 0's layout shifted by s * ws_bytes
     void* ws_mem = nullptr;
     size_t ws_bytes = 0;
@@ -279,22 +280,32 @@ struct kspir_ctx {
     uint32_t* fa_acc = nullptr;
     unsigned long long* fa_times = nullptr;
     std::vector<char> ring_fused;
-    // device-buffer single answers rotate over the first single_slots
-    // workspace slots, so answers issued on different streams overlap; each
-    // slot's last answer is marked by slot_done (waited for before reuse)
+    // single answers rotate over the first single_slots workspace slots, so
+    // answers issued on different streams (or by different host threads)
+    // overlap; each slot's last answer is marked by slot_done (waited for
+    // before reuse).  A host-buffer answer owns its slot (slot_busy) from its
+    // enqueue until it has read its response, runs on the slot's stream and
+    // waits for host_done outside the mutex; its error word lands in
+    // single_errs[slot] (pinned).
     int single_slots = 1;
     int next_single = 0;
     std::vector<cudaEvent_t> slot_done;
+    std::vector<cudaEvent_t> host_done;
+    std::vector<cudaStream_t> slot_stream;
     std::vector<char> slot_used;
+    std::vector<char> slot_busy;
+    int* single_errs = nullptr;
+    std::condition_variable slot_cv;
     std::mutex mu;            // serialises enqueues from several host threads
 };
 
 namespace {
 
-thread_local std::string g_thread_err;   // errors without a context (creation)
+thread_local std::string g_thread_err;   // the calling thread's last error text
 
-int set_err(kspir_ctx* c, int code, const std::string& msg) {
-    if (c) c->err = msg;
+// Error text is kept per host thread (like errno): several threads may call
+// into one context at once.
+int set_err(kspir_ctx*, int code, const std::string& msg) {
     g_thread_err = msg;
     return code;
 }
@@ -656,7 +667,7 @@ void enqueue_scan(kspir_ctx* c, int slot0, int nq, int kind, cudaStream_t st) {
             switch (c->N1) {
 #define KS_SCAN(n)                                                                                           \
     case n:                                                                                                  \
-        k_scan<n><<<c->nsm, ScanCfg<n>::THREADS, ScanCfg<n>::SMEM, st>>>(c->db, w.cipherbuf, w.sout, R, w.err, \
+        k_scan<n><<<c->scan_ctas, ScanCfg<n>::THREADS, ScanCfg<n>::SMEM, st>>>(c->db, w.cipherbuf, w.sout, R, w.err, \
                                                                          c->wait_limit_ns, c->scan_skip);        \
         break;
                 KS_SCAN(64) KS_SCAN(128) KS_SCAN(256)
@@ -906,8 +917,6 @@ int check_ready(kspir_ctx* c, int client) {
     return rc ? rc : check_client(c, client);
 }
 
-// Waits for the context stream and reports (then clears) the error words of
-// slots [slot0, slot0 + nq).
 // Waits for the work enqueued on the context stream and collects the error
 // words of slots [slot0, slot0 + nq) with it (one synchronisation).
 int finish(kspir_ctx* c, int slot0, int nq) {
@@ -943,6 +952,41 @@ int mark_singles(kspir_ctx* c, cudaStream_t st) {
     }
     return KSPIR_OK;
 }
+
+// Chooses the workspace slot of a single answer; `lk` holds c->mu.  The fused
+// answer has one set of counters and always runs in slot 0.  A host-buffer
+// answer (`host`) waits until a slot no other host call owns is free; a
+// device-buffer answer prefers such a slot but takes the next one otherwise
+// (the slot events order it after the owner on the device).
+int pick_slot(kspir_ctx* c, std::unique_lock<std::mutex>& lk, bool host) {
+    for (;;) {
+        const int n = c->fused ? 1 : c->single_slots;
+        for (int k = 0; k < n; k++) {
+            const int s = (c->next_single + k) % n;
+            if (!c->slot_busy[s]) {
+                c->next_single = (s + 1) % c->single_slots;
+                return s;
+            }
+        }
+        if (!host) {
+            const int s = c->fused ? 0 : c->next_single;
+            c->next_single = (s + 1) % c->single_slots;
+            return s;
+        }
+        c->slot_cv.wait(lk);
+    }
+}
+
+// A host call's ownership of a single-answer slot; released (and the waiting
+// host calls woken) when it goes out of scope with c->mu held.
+struct SlotHold {
+    kspir_ctx* c;
+    int slot;
+    ~SlotHold() {
+        c->slot_busy[slot] = 0;
+        c->slot_cv.notify_all();
+    }
+};
 
 // the tensor-core database operand, rebuilt from the resident database
 int build_dbop(kspir_ctx* c) {
@@ -1091,7 +1135,7 @@ const char* kspir_strerror(int code) {
     }
 }
 
-const char* kspir_last_error(const kspir_ctx* ctx) { return ctx ? ctx->err.c_str() : g_thread_err.c_str(); }
+const char* kspir_last_error(const kspir_ctx*) { return g_thread_err.c_str(); }
 
 int kspir_ctx_create(int device, const kspir_params* params, kspir_ctx** out) {
     if (!params || !out) return KSPIR_ERR_INVALID_ARG;
@@ -1115,6 +1159,8 @@ int kspir_ctx_create(int device, const kspir_params* params, kspir_ctx** out) {
     if (const char* e = getenv("KSPIR_NO_GRAPHS")) c->use_graphs = !(e[0] == '1');
     if (const char* e = getenv("KSPIR_NO_PDL")) c->use_pdl = !(e[0] == '1');
     KS_CUDA(c.get(), cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device));
+    c->scan_ctas = c->nsm;
+    if (const char* e = getenv("KSPIR_SCAN_CTAS")) c->scan_ctas = std::max(1, std::min(c->nsm, atoi(e)));
     KS_CUDA(c.get(), cudaFuncSetAttribute(k_baby_rot<3, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBabySmem));
     KS_CUDA(c.get(), cudaFuncSetAttribute(k_baby_pair<3, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBabyPairSmem));
     KS_CUDA(c.get(), cudaFuncSetAttribute(k_client_query, cudaFuncAttributeMaxDynamicSharedMemorySize, kClientSmem));
@@ -1154,8 +1200,16 @@ int kspir_ctx_create(int device, const kspir_params* params, kspir_ctx** out) {
         for (auto& e : evs) KS_CUDA(c.get(), cudaEventCreate(&e));
     c->single_slots = std::min(p.max_inflight, kSingleSlots);
     c->slot_done.assign(c->single_slots, nullptr);
+    c->host_done.assign(c->single_slots, nullptr);
+    c->slot_stream.assign(c->single_slots, nullptr);
     c->slot_used.assign(c->single_slots, 0);
-    for (auto& e : c->slot_done) KS_CUDA(c.get(), cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    c->slot_busy.assign(c->single_slots, 0);
+    for (int i = 0; i < c->single_slots; i++) {
+        KS_CUDA(c.get(), cudaEventCreateWithFlags(&c->slot_done[i], cudaEventDisableTiming));
+        KS_CUDA(c.get(), cudaEventCreateWithFlags(&c->host_done[i], cudaEventDisableTiming));
+        KS_CUDA(c.get(), cudaStreamCreateWithFlags(&c->slot_stream[i], cudaStreamNonBlocking));
+    }
+    KS_CUDA(c.get(), cudaHostAlloc(&c->single_errs, (size_t)c->single_slots * 4, cudaHostAllocDefault));
     rc = init_key_slots(c.get());
     if (rc) return rc;
     rc = init_workspaces(c.get());
@@ -1171,10 +1225,13 @@ int kspir_ctx_create(int device, const kspir_params* params, kspir_ctx** out) {
 int kspir_ctx_destroy(kspir_ctx* c) {
     if (!c) return KSPIR_ERR_INVALID_ARG;
     cudaSetDevice(c->device);
-    cudaStreamSynchronize(c->stream);
+    cudaDeviceSynchronize();
     for (auto& evs : c->ring)
         for (auto& e : evs) if (e) cudaEventDestroy(e);
     for (auto& e : c->slot_done) if (e) cudaEventDestroy(e);
+    for (auto& e : c->host_done) if (e) cudaEventDestroy(e);
+    for (auto& st : c->slot_stream) if (st) cudaStreamDestroy(st);
+    if (c->single_errs) cudaFreeHost(c->single_errs);
     for (auto& kv : c->graphs)
         for (auto& g : kv.second.g) if (g) cudaGraphExecDestroy(g);
     if (c->capture) cudaStreamDestroy(c->capture);
@@ -1996,12 +2053,10 @@ int kspir_answer_device(kspir_ctx* c, int client, const uint64_t* d_query, uint6
     int rc = check_ready(c, client);
     if (rc) return rc;
     if (!d_query || !d_response) return KSPIR_ERR_INVALID_ARG;
-    std::lock_guard<std::mutex> lk(c->mu);
+    std::unique_lock<std::mutex> lk(c->mu);
     cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
     KS_CUDA(c, cudaSetDevice(c->device));
-    // the fused answer has one set of counters: it always runs in slot 0
-    const int slot = c->fused ? 0 : c->next_single;
-    if (!c->fused) c->next_single = (slot + 1) % c->single_slots;
+    const int slot = pick_slot(c, lk, false);
     if (c->slot_used[slot]) KS_CUDA(c, cudaStreamWaitEvent(st, c->slot_done[slot], 0));
     KS_CUDA(c, cudaMemcpyAsync(c->bq64 + (size_t)slot * 4 * kN, d_query, 4 * kN * 8, cudaMemcpyDeviceToDevice, st));
     rc = enqueue_answer(c, slot, 1, &client, st, true);
@@ -2031,21 +2086,40 @@ int kspir_answer(kspir_ctx* c, int client, const uint64_t* query, uint64_t* resp
     int rc = check_ready(c, client);
     if (rc) return rc;
     if (!query || !response) return KSPIR_ERR_INVALID_ARG;
-    std::lock_guard<std::mutex> lk(c->mu);
+    std::unique_lock<std::mutex> lk(c->mu);
     KS_CUDA(c, cudaSetDevice(c->device));
-    if (int wrc = wait_singles(c, c->stream)) return wrc;
-    KS_CUDA(c, cudaMemcpyAsync(c->bq64, query, 4 * kN * 8, cudaMemcpyHostToDevice, c->stream));
-    rc = enqueue_answer(c, 0, 1, &client, c->stream, true);
+    const int slot = pick_slot(c, lk, true);
+    c->slot_busy[slot] = 1;
+    SlotHold hold{c, slot};
+    cudaStream_t st = c->slot_stream[slot];
+    if (c->slot_used[slot]) KS_CUDA(c, cudaStreamWaitEvent(st, c->slot_done[slot], 0));
+    KS_CUDA(c, cudaMemcpyAsync(c->bq64 + (size_t)slot * 4 * kN, query, 4 * kN * 8, cudaMemcpyHostToDevice, st));
+    rc = enqueue_answer(c, slot, 1, &client, st, true);
     if (rc) return rc;
     KS_CUDA(c, cudaGetLastError());
     // the query is validated while the device answers it; a non-canonical one
     // is reported before anything reaches the caller's response buffer
-    if (!canonical(query, 2 * kN, kCrtMod) || !canonical(query + 2 * kN, 2 * kN, kBsMod)) {
-        KS_CUDA(c, cudaStreamSynchronize(c->stream));
-        return set_err(c, KSPIR_ERR_INVALID_ARG, "query word not canonical");
+    const bool ok = canonical(query, 2 * kN, kCrtMod) && canonical(query + 2 * kN, 2 * kN, kBsMod);
+    if (ok) {
+        KS_CUDA(c, cudaMemcpyAsync(response, c->bresp + (size_t)slot * 2 * kN, 2 * kN * 8, cudaMemcpyDeviceToHost, st));
+        KS_CUDA(c, cudaMemcpyAsync(c->single_errs + slot, c->errs + (size_t)slot * kErrStride, 4,
+                                   cudaMemcpyDeviceToHost, st));
     }
-    KS_CUDA(c, cudaMemcpyAsync(response, c->bresp, 2 * kN * 8, cudaMemcpyDeviceToHost, c->stream));
-    return finish(c, 0, 1);
+    KS_CUDA(c, cudaEventRecord(c->slot_done[slot], st));
+    KS_CUDA(c, cudaEventRecord(c->host_done[slot], st));
+    c->slot_used[slot] = 1;
+    // other host calls enqueue while this one waits for its answer
+    lk.unlock();
+    const cudaError_t e = cudaEventSynchronize(c->host_done[slot]);
+    lk.lock();
+    if (e != cudaSuccess) return set_err(c, KSPIR_ERR_CUDA, cudaGetErrorString(e));
+    if (!ok) return set_err(c, KSPIR_ERR_INVALID_ARG, "query word not canonical");
+    if (const int herr = c->single_errs[slot]) {
+        KS_CUDA(c, cudaMemsetAsync(c->errs + (size_t)slot * kErrStride, 0, kErrStride * 4, st));
+        KS_CUDA(c, cudaStreamSynchronize(st));
+        return set_err(c, KSPIR_ERR_TIMEOUT, "a bounded device wait gave up (code " + std::to_string(herr) + ")");
+    }
+    return KSPIR_OK;
 }
 
 int kspir_answer_batch_device(kspir_ctx* c, int n, const int32_t* clients, const uint64_t* d_queries,

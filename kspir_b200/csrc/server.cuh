@@ -201,10 +201,15 @@ void srv_launch(Srv& s, Srv::Lane& L) {
         if (!rc && cudaMemcpyAsync(c->bq64 + (size_t)L.slot0 * 4 * kN, L.hq, (size_t)n * 4 * kN * 8,
                                    cudaMemcpyHostToDevice, L.st) != cudaSuccess)
             rc = KSPIR_ERR_CUDA;
+        // a lane whose slots include the single-answer slots is ordered
+        // against direct kspir_answer / kspir_answer_device calls
+        const bool shares = L.slot0 < c->single_slots;
+        if (!rc && shares) rc = wait_singles(c, L.st);
         if (!rc) rc = enqueue_answer(c, L.slot0, n, slots.data(), L.st);
         if (!rc && cudaMemcpyAsync(L.hr, c->bresp + (size_t)L.slot0 * 2 * kN, (size_t)n * 2 * kN * 8,
                                    cudaMemcpyDeviceToHost, L.st) != cudaSuccess)
             rc = KSPIR_ERR_CUDA;
+        if (!rc && shares) rc = mark_singles(c, L.st);
         if (!rc && cudaEventRecord(L.done, L.st) != cudaSuccess) rc = KSPIR_ERR_CUDA;
     }
     if (rc) {
