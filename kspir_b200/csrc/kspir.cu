@@ -171,7 +171,12 @@ GadgetBsgs make_gadget_bsgs(int ell, uint64_t base, uint64_t bg) {
 size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 constexpr int kTimingRing = 512;   // event sets of recent launches kept for kspir_timing_summary
-constexpr int kSingleSlots = 4;    // workspace slots device-buffer single answers rotate over
+// workspace slots (and streams) single answers rotate over: answers in
+// different slots overlap on the device
+#ifndef KSPIR_SINGLE_SLOTS
+#define KSPIR_SINGLE_SLOTS 4
+#endif
+constexpr int kSingleSlots = KSPIR_SINGLE_SLOTS;
 constexpr int kMaxBatch = 256;     // queries per launch
 
 struct ClientList {
