@@ -56,7 +56,7 @@ CRTMOD = 268369921 * 249561089
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="kspir", choices=["kspir", "reference"])
     ap.add_argument("--r", type=int, default=16)
@@ -64,7 +64,7 @@ def parse():
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--streams", type=int, default=4,
+    ap.add_argument("--streams", type=int, default=8,
                     help="streams (and host threads, end to end) the single answers are issued on")
     ap.add_argument("--batches", default="1,8,32,64,128", help="batch sizes of the batched sweep ('' = none)")
     ap.add_argument("--clients", type=int, default=128, help="distinct client key sets of the batched sweep")
@@ -87,7 +87,7 @@ def workload_config(args):
 # clocks during the timed region (NVML reads only)
 
 class ClockSampler:
-    def __init__(self, index: int, period: float = 0.005):
+    def __init__(self, index: int, period: float = 0.001):
         self.samples = []
         self.max_mhz = None
         self.reasons = set()

@@ -204,9 +204,9 @@ int kspir_client_keys_upload(kspir_ctx* ctx, int client, const uint64_t* baby, c
  * (matrix_vector_mul_bsgs_rns_crt_large -> externalProduct x r -> packingRLWEs),
  * host buffers in and out.  The caller's query is not modified.  Blocks until
  * the response is in `response`.  Safe to call from several host threads at
- * once: each call owns one of min(max_inflight, 4) workspace slots and its
+ * once: each call owns one of min(max_inflight, 8) workspace slots and its
  * stream while it runs, and waits for its answer without holding the context,
- * so up to four concurrent callers' answers overlap on the device (one
+ * so up to eight concurrent callers' answers overlap on the device (one
  * answer's key switches with another's database scan).  Pinned host buffers
  * let the copies run asynchronously. */
 int kspir_answer(kspir_ctx* ctx, int client, const uint64_t* query, uint64_t* response);

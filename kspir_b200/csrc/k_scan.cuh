@@ -39,18 +39,15 @@ constexpr uint64_t kWaitLimitNs = 2000000000ull;     // 2 s per bounded wait
 // that warp never waits more than one phase ahead of the barrier (an mbarrier
 // parity wait cannot tell phase u-1 from u+1).
 
-// Ring shape of the single-query scan (measured on B200 with a 1 GiB
-// database: 4 consumer warps over 8 stages of 18 KiB streamed at 6.9 TB/s,
-// 6 over 12 at 6.1 TB/s, and the 148 KiB of shared memory leave room for a
-// key-switch CTA of a concurrent answer on the same SM).
-#ifndef KSPIR_SCAN_CONS
-#define KSPIR_SCAN_CONS 4
-#endif
-#ifndef KSPIR_SCAN_NST
-#define KSPIR_SCAN_NST 8
-#endif
-
-template <int N1>
+// Ring shapes of the single-query scan, measured on B200 with a 1 GiB
+// database (consumer warps x stages of 18 KiB, 148 CTAs): 4 x 8 0.156 ms
+// (6.9 TB/s), 6 x 6 0.176 ms, 6 x 12 0.176 ms, 4 x 4 0.214 ms.  The default
+// (streaming) shape is 4 x 8: 148 KiB of shared memory, which leaves room on
+// the SM for a baby-step or transform CTA of a concurrent answer.  The sharing
+// shape (ScanShare) is 6 x 6: 110 KiB, slower alone but leaving room for a
+// giant-step or external-product CTA (107 KiB) beside it, which pays when
+// several answers are in flight.
+template <int N1, int CONS_ = 4, int NST_ = 8>
 struct ScanCfg {
     static constexpr int N2 = kN / 2 / N1;
     static constexpr int CHUNKS = N1 / 2;               // 16-byte chunks per row
@@ -59,8 +56,8 @@ struct ScanCfg {
     static constexpr int SLAB = kN / 2 * 8;             // DB bytes per item
     static constexpr int QSLAB = 2 * N1 * 8;            // cipherbuf bytes per item
     static constexpr int STAGE = SLAB + QSLAB;
-    static constexpr int CONS = N1 <= 128 ? KSPIR_SCAN_CONS : 4;   // consumer warps
-    static constexpr int NST = N1 <= 128 ? KSPIR_SCAN_NST : 8;     // ring stages, a multiple of CONS
+    static constexpr int CONS = CONS_;                  // consumer warps
+    static constexpr int NST = NST_;                    // ring stages, a multiple of CONS
     static constexpr int THREADS = 32 * (CONS + 1);
     static constexpr int SMEM = NST * STAGE + 2 * NST * 8;
     static_assert(NST % CONS == 0, "stages must be owned by one consumer warp each");
@@ -68,6 +65,13 @@ struct ScanCfg {
     static constexpr int NV = 4 * RPL;                  // partial sums per lane
     static constexpr int NOUT = NV / 8;                 // finished outputs per lane
     static_assert(RPL >= 2 && CPL >= 1, "N1 must be in [64, 256]");
+};
+
+template <int N1>
+struct ScanShare {   // 6 x 6 where a 107 KiB CTA still fits beside it (N1 <= 128)
+    static constexpr int CONS = N1 <= 128 ? 6 : 4;
+    static constexpr int NST = N1 <= 128 ? 6 : 8;
+    using Cfg = ScanCfg<N1, CONS, NST>;
 };
 
 // The multiply-accumulate of one work item by one warp: the slab DB[r][z]
@@ -139,11 +143,11 @@ __device__ __forceinline__ void scan_item_store(uint64_t* v, int lane, int r, in
 // stage waits for bytes that never come, gives up after limit_ns, records the
 // error and stops; the producer then gives up waiting for the stage to be
 // released, and drains the copies it did issue before the CTA exits.
-template <int N1>
-__global__ void __launch_bounds__(ScanCfg<N1>::THREADS, 1)
+template <int N1, int CONS = 4, int NST = 8>
+__global__ void __launch_bounds__(ScanCfg<N1, CONS, NST>::THREADS, 1)
     k_scan(const uint64_t* __restrict__ db, const uint64_t* __restrict__ cbuf, uint32_t* __restrict__ sout,
            int R, int* __restrict__ err, uint64_t limit_ns, long skip) {
-    using C = ScanCfg<N1>;
+    using C = ScanCfg<N1, CONS, NST>;
     extern __shared__ __align__(128) uint8_t smem[];
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + C::NST * C::STAGE);
     uint64_t* empty = full + C::NST;

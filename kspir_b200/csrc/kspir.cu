@@ -174,7 +174,7 @@ constexpr int kTimingRing = 512;   // event sets of recent launches kept for ksp
 // workspace slots (and streams) single answers rotate over: answers in
 // different slots overlap on the device
 #ifndef KSPIR_SINGLE_SLOTS
-#define KSPIR_SINGLE_SLOTS 4
+#define KSPIR_SINGLE_SLOTS 8
 #endif
 constexpr int kSingleSlots = KSPIR_SINGLE_SLOTS;
 constexpr int kMaxBatch = 256;     // queries per launch
@@ -299,6 +299,7 @@ struct kspir_ctx {
     std::vector<cudaStream_t> slot_stream;
     std::vector<char> slot_used;
     std::vector<char> slot_busy;
+    std::vector<cudaStream_t> slot_last_stream;   // stream of each slot's last answer
     int* single_errs = nullptr;
     std::condition_variable slot_cv;
     std::mutex mu;            // serialises enqueues from several host threads
@@ -664,7 +665,9 @@ void launch_scan_mma(kspir_ctx* c, int slot0, int nq, cudaStream_t st) {
     k_scan_mma<BT><<<std::min(c->nsm, units), C::THREADS, C::SMEM, st>>>(a);
 }
 
-void enqueue_scan(kspir_ctx* c, int slot0, int nq, int kind, cudaStream_t st) {
+// `share`: another single answer runs beside this one, so the CUDA-core scan
+// takes the ring shape that leaves room for that answer's key-switch CTAs.
+void enqueue_scan(kspir_ctx* c, int slot0, int nq, int kind, cudaStream_t st, bool share = false) {
     const int R = c->p.r;
     if (kind == SCAN_CUDA) {
         for (int q = 0; q < nq; q++) {
@@ -672,8 +675,14 @@ void enqueue_scan(kspir_ctx* c, int slot0, int nq, int kind, cudaStream_t st) {
             switch (c->N1) {
 #define KS_SCAN(n)                                                                                           \
     case n:                                                                                                  \
-        k_scan<n><<<c->scan_ctas, ScanCfg<n>::THREADS, ScanCfg<n>::SMEM, st>>>(c->db, w.cipherbuf, w.sout, R, w.err, \
-                                                                         c->wait_limit_ns, c->scan_skip);        \
+        if (share) {                                                                                         \
+            using SC = typename ScanShare<n>::Cfg;                                                           \
+            k_scan<n, SC::CONS, SC::NST><<<c->scan_ctas, SC::THREADS, SC::SMEM, st>>>(                        \
+                c->db, w.cipherbuf, w.sout, R, w.err, c->wait_limit_ns, c->scan_skip);                        \
+        } else {                                                                                             \
+            k_scan<n><<<c->scan_ctas, ScanCfg<n>::THREADS, ScanCfg<n>::SMEM, st>>>(                          \
+                c->db, w.cipherbuf, w.sout, R, w.err, c->wait_limit_ns, c->scan_skip);                        \
+        }                                                                                                    \
         break;
                 KS_SCAN(64) KS_SCAN(128) KS_SCAN(256)
 #undef KS_SCAN
@@ -838,7 +847,8 @@ int enqueue_fused(kspir_ctx* c, int client, cudaStream_t st, int ring_slot) {
 
 // allow_fused: a single answer of slot 0 through the public single-answer
 // calls may run as the fused kernel (batches and serving lanes never do)
-int enqueue_answer(kspir_ctx* c, int slot0, int nq, const int* clients, cudaStream_t st, bool allow_fused = false) {
+int enqueue_answer(kspir_ctx* c, int slot0, int nq, const int* clients, cudaStream_t st, bool allow_fused = false,
+                   bool share = false) {
     const int slot = (int)(c->enqueues % kTimingRing);
     auto& ev = c->ring[slot];
     if (allow_fused && c->fused && nq == 1 && slot0 == 0) {
@@ -869,7 +879,7 @@ int enqueue_answer(kspir_ctx* c, int slot0, int nq, const int* clients, cudaStre
         cudaEventRecord(ev[0], st);
         KS_CUDA(c, cudaGraphLaunch(pg->g[0], st));
         cudaEventRecord(ev[1], st);
-        enqueue_scan(c, slot0, nq, kind, st);
+        enqueue_scan(c, slot0, nq, kind, st, share);
         cudaEventRecord(ev[2], st);
         KS_CUDA(c, cudaGraphLaunch(pg->g[1], st));
         cudaEventRecord(ev[3], st);
@@ -881,7 +891,7 @@ int enqueue_answer(kspir_ctx* c, int slot0, int nq, const int* clients, cudaStre
         cudaEventRecord(ev[0], st);
         enqueue_baby(c, slot0, nq, kind != SCAN_CUDA, st);
         cudaEventRecord(ev[1], st);
-        enqueue_scan(c, slot0, nq, kind, st);
+        enqueue_scan(c, slot0, nq, kind, st, share);
         cudaEventRecord(ev[2], st);
         enqueue_giant(c, slot0, nq, st);
         cudaEventRecord(ev[3], st);
@@ -954,6 +964,7 @@ int mark_singles(kspir_ctx* c, cudaStream_t st) {
     for (int i = 0; i < c->single_slots; i++) {
         KS_CUDA(c, cudaEventRecord(c->slot_done[i], st));
         c->slot_used[i] = 1;
+        c->slot_last_stream[i] = st;
     }
     return KSPIR_OK;
 }
@@ -992,6 +1003,18 @@ struct SlotHold {
         c->slot_cv.notify_all();
     }
 };
+
+// Whether a single answer in another slot, on another stream, may still be
+// running when this one (slot `self`, stream `st`) starts: then the scan takes
+// the sharing ring shape.  Answers on the same stream run one after another
+// and keep the streaming shape.
+bool singles_beside(kspir_ctx* c, int self, cudaStream_t st) {
+    for (int i = 0; i < c->single_slots; i++) {
+        if (i == self || !c->slot_used[i] || c->slot_last_stream[i] == st) continue;
+        if (c->slot_busy[i] || cudaEventQuery(c->slot_done[i]) == cudaErrorNotReady) return true;
+    }
+    return false;
+}
 
 // the tensor-core database operand, rebuilt from the resident database
 int build_dbop(kspir_ctx* c) {
@@ -1182,8 +1205,10 @@ int kspir_ctx_create(int device, const kspir_params* params, kspir_ctx** out) {
     KS_CUDA(c.get(), cudaFuncSetAttribute(k_off_keyswitch, cudaFuncAttributeMaxDynamicSharedMemorySize, kOffSmem));
     KS_CUDA(c.get(), cudaFuncSetAttribute(k_off_intt_key, cudaFuncAttributeMaxDynamicSharedMemorySize, kNttJobSmem));
     KS_CUDA(c.get(), cudaFuncSetAttribute(k_off_modswitch, cudaFuncAttributeMaxDynamicSharedMemorySize, kNttJobSmem));
-#define KS_ATTR(n) \
-    KS_CUDA(c.get(), cudaFuncSetAttribute(k_scan<n>, cudaFuncAttributeMaxDynamicSharedMemorySize, ScanCfg<n>::SMEM));
+#define KS_ATTR(n)                                                                                         \
+    KS_CUDA(c.get(), cudaFuncSetAttribute(k_scan<n>, cudaFuncAttributeMaxDynamicSharedMemorySize, ScanCfg<n>::SMEM)); \
+    KS_CUDA(c.get(), cudaFuncSetAttribute(k_scan<n, ScanShare<n>::CONS, ScanShare<n>::NST>,                     \
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, ScanShare<n>::Cfg::SMEM));
     KS_ATTR(64) KS_ATTR(128) KS_ATTR(256)
 #undef KS_ATTR
     int rc = KSPIR_OK;
@@ -1209,6 +1234,7 @@ int kspir_ctx_create(int device, const kspir_params* params, kspir_ctx** out) {
     c->slot_stream.assign(c->single_slots, nullptr);
     c->slot_used.assign(c->single_slots, 0);
     c->slot_busy.assign(c->single_slots, 0);
+    c->slot_last_stream.assign(c->single_slots, nullptr);
     for (int i = 0; i < c->single_slots; i++) {
         KS_CUDA(c.get(), cudaEventCreateWithFlags(&c->slot_done[i], cudaEventDisableTiming));
         KS_CUDA(c.get(), cudaEventCreateWithFlags(&c->host_done[i], cudaEventDisableTiming));
@@ -2062,13 +2088,15 @@ int kspir_answer_device(kspir_ctx* c, int client, const uint64_t* d_query, uint6
     cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
     KS_CUDA(c, cudaSetDevice(c->device));
     const int slot = pick_slot(c, lk, false);
+    const bool share = singles_beside(c, slot, st);
     if (c->slot_used[slot]) KS_CUDA(c, cudaStreamWaitEvent(st, c->slot_done[slot], 0));
     KS_CUDA(c, cudaMemcpyAsync(c->bq64 + (size_t)slot * 4 * kN, d_query, 4 * kN * 8, cudaMemcpyDeviceToDevice, st));
-    rc = enqueue_answer(c, slot, 1, &client, st, true);
+    rc = enqueue_answer(c, slot, 1, &client, st, true, share);
     if (rc) return rc;
     KS_CUDA(c, cudaMemcpyAsync(d_response, c->bresp + (size_t)slot * 2 * kN, 2 * kN * 8, cudaMemcpyDeviceToDevice, st));
     KS_CUDA(c, cudaEventRecord(c->slot_done[slot], st));
     c->slot_used[slot] = 1;
+    c->slot_last_stream[slot] = st;
     KS_CUDA(c, cudaGetLastError());
     return KSPIR_OK;
 }
@@ -2097,9 +2125,10 @@ int kspir_answer(kspir_ctx* c, int client, const uint64_t* query, uint64_t* resp
     c->slot_busy[slot] = 1;
     SlotHold hold{c, slot};
     cudaStream_t st = c->slot_stream[slot];
+    const bool share = singles_beside(c, slot, st);
     if (c->slot_used[slot]) KS_CUDA(c, cudaStreamWaitEvent(st, c->slot_done[slot], 0));
     KS_CUDA(c, cudaMemcpyAsync(c->bq64 + (size_t)slot * 4 * kN, query, 4 * kN * 8, cudaMemcpyHostToDevice, st));
-    rc = enqueue_answer(c, slot, 1, &client, st, true);
+    rc = enqueue_answer(c, slot, 1, &client, st, true, share);
     if (rc) return rc;
     KS_CUDA(c, cudaGetLastError());
     // the query is validated while the device answers it; a non-canonical one
@@ -2113,6 +2142,7 @@ int kspir_answer(kspir_ctx* c, int client, const uint64_t* query, uint64_t* resp
     KS_CUDA(c, cudaEventRecord(c->slot_done[slot], st));
     KS_CUDA(c, cudaEventRecord(c->host_done[slot], st));
     c->slot_used[slot] = 1;
+    c->slot_last_stream[slot] = st;
     // other host calls enqueue while this one waits for its answer
     lk.unlock();
     const cudaError_t e = cudaEventSynchronize(c->host_done[slot]);

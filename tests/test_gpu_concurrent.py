@@ -1,7 +1,7 @@
 """Single answers that overlap on the device: word-for-word parity.
 
 kspir_answer may be called from several host threads at once (each call owns
-one of four workspace slots and its stream while it runs) and
+one of eight workspace slots and its stream while it runs) and
 kspir_answer_device rotates over the same slots on the caller's streams.
 Every response must equal the one the same query gets alone, and the oracle's
 (oracle/kspir_oracle.c); other entry points issued between them must be
