@@ -9,7 +9,7 @@
 // exact 64-bit sums (products < 2^56, N1 <= 512 terms; any wrap mod 2^64 is
 // the reference's too), and the reference composes out = crt_compose(a_lo,
 // a_hi), which is the canonical crtMod value with residues (a_lo mod q1,
-// a_hi mod q2).  The kernel stores those residues in the z-blocked layout of
+// a_hi mod q2).  The kernel stores those residues in the blocked layout of
 // sout_idx (row r * N2 + i, cv = comp * 2 + ch).
 //
 // Data movement: one 16 KiB slab DB[r][z] (N2 x N1 words) plus the 16*N1-byte

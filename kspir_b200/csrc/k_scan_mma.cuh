@@ -29,8 +29,9 @@
 // Work: a unit is (ZB consecutive NTT slots, prime, query tile); its ZB query
 // tiles stay resident while the database tiles stream through a ring in the
 // order (row group g, slot).  The epilogue keeps the ZB results of one
-// (row, component, query) in registers and writes them as one 16- or 32-byte
-// piece of the z-blocked scan output (sout_idx), so stores fill whole sectors.
+// (row, component, query) in registers and writes them as 16-byte pieces of
+// the blocked scan output (sout_idx), where the eight row lanes of a query
+// cover two 128-byte lines.
 //
 // Warp roles: warp 0 producer (one lane), warp 1 TMEM allocation and MMA issue
 // (one lane), warps 2.. epilogue (warp w reads TMEM lanes 32 (w % 4) .. and a
@@ -317,11 +318,12 @@ __global__ void __launch_bounds__(MmaCfg<BT>::THREADS, 1) k_scan_mma(ScanMmaArgs
                         if (bq < a.nq) {
                             uint32_t* so = reinterpret_cast<uint32_t*>(reinterpret_cast<char*>(a.sout0) +
                                                                        (size_t)(a.slot0 + bq) * a.ws_bytes);
-                            uint4* dst = reinterpret_cast<uint4*>(so + sout_idx(row, comp * 2 + ch, z0, a.rows));
-                            dst[0] = make_uint4(ob[0][c], ob[1][c], ob[2][c], ob[3][c]);
-                            if (C::ZB == 8)
-                                dst[1] = make_uint4(ob[4 % C::ZB][c], ob[5 % C::ZB][c], ob[6 % C::ZB][c],
-                                                    ob[7 % C::ZB][c]);
+                            // four consecutive slots per 16-byte store; the eight
+                            // row lanes of this query cover two 128-byte lines
+#pragma unroll
+                            for (int z4 = 0; z4 < C::ZB; z4 += 4)
+                                *reinterpret_cast<uint4*>(so + sout_idx(row, comp * 2 + ch, z0 + z4, a.rows)) =
+                                    make_uint4(ob[z4][c], ob[z4 + 1][c], ob[z4 + 2][c], ob[z4 + 3][c]);
                         }
                     }
                 }
@@ -368,7 +370,7 @@ __global__ void __launch_bounds__(kSplitThreads) k_qop_split_rm(const uint32_t* 
         const uint32_t* cb = reinterpret_cast<const uint32_t*>(reinterpret_cast<const char*>(cb0) +
                                                               (size_t)(slot0 + bq) * ws_bytes);
         constexpr int W = kSplitThreads / 32;
-#pragma unroll 8
+#pragma unroll 32
         for (int row = warp; row < kMmaK * 4; row += W)
             V[row * kSplitZ + (lane ^ (4 * ((row >> 6) & 7)))] = __ldg(cb + (size_t)row * kN + z0 + lane);
         __syncthreads();

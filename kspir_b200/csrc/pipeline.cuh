@@ -26,12 +26,16 @@ struct ClientKeysDev {
     const uint32_t* rgsw;
 };
 
-// Database-scan output layout: z-blocked so that eight consecutive NTT slots of
-// one polynomial share a 32-byte sector (the batched scan writes whole sectors):
-//   sout[z / 8][row = r * N2 + i][comp * 2 + ch][z % 8]
+// Database-scan output layout: a 128-byte line holds 8 consecutive NTT slots
+// of 4 consecutive rows (one 32-byte sector per row):
+//   sout[z / 8][row / 4][comp * 2 + ch][row % 4][z % 8],  row = r * N2 + i
+// A giant step reads and rewrites its own row in whole sectors, and the
+// batched scan's epilogue (four slots per thread, eight row lanes per query)
+// writes two lines per query and store instead of eight (rows = r * N2 is a
+// multiple of 4).
 constexpr int kZBlock = 8;
 __host__ __device__ __forceinline__ size_t sout_idx(int row, int cv, int z, int rows) {
-    return (((size_t)(z >> 3) * rows + row) * 4 + cv) * kZBlock + (z & 7);
+    return ((((size_t)(z >> 3) * (rows >> 2) + (row >> 2)) * 4 + cv) * 4 + (row & 3)) * kZBlock + (z & 7);
 }
 
 struct Workspace {
