@@ -143,12 +143,10 @@ __device__ __forceinline__ void scan_item_store(uint64_t* v, int lane, int r, in
 // stage waits for bytes that never come, gives up after limit_ns, records the
 // error and stops; the producer then gives up waiting for the stage to be
 // released, and drains the copies it did issue before the CTA exits.
-// Sub-databases [r0, r0 + R) of Rtot (a single answer scans its two halves
-// in two launches, so that the giant steps of the first overlap the second).
 template <int N1, int CONS = 4, int NST = 8>
 __global__ void __launch_bounds__(ScanCfg<N1, CONS, NST>::THREADS, 1)
     k_scan(const uint64_t* __restrict__ db, const uint64_t* __restrict__ cbuf, uint32_t* __restrict__ sout,
-           int R, int* __restrict__ err, uint64_t limit_ns, long skip, int r0, int Rtot) {
+           int R, int* __restrict__ err, uint64_t limit_ns, long skip) {
     using C = ScanCfg<N1, CONS, NST>;
     extern __shared__ __align__(128) uint8_t smem[];
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + C::NST * C::STAGE);
@@ -185,7 +183,7 @@ __global__ void __launch_bounds__(ScanCfg<N1, CONS, NST>::THREADS, 1)
                 issued = j + 1;
                 if (j == skip_j) continue;   // injected failure: nothing arrives on full[s]
                 const long it = blockIdx.x + j * gridDim.x;
-                const long r = r0 + it / kN, z = it % kN;
+                const long r = it / kN, z = it % kN;
                 uint8_t* st = smem + (size_t)s * C::STAGE;
                 mbar_arrive_expect_tx(&full[s], C::STAGE);
                 // the database streams through L2 once (evict first); the 8 MiB
@@ -214,7 +212,7 @@ __global__ void __launch_bounds__(ScanCfg<N1, CONS, NST>::THREADS, 1)
         __syncwarp();
         if (lane == 0) mbar_arrive(&empty[s]);
         const long it = blockIdx.x + j * gridDim.x;
-        scan_item_store<N1>(v, lane, r0 + (int)(it / kN), (int)(it % kN), Rtot, sout);
+        scan_item_store<N1>(v, lane, (int)(it / kN), (int)(it % kN), R, sout);
     }
 }
 

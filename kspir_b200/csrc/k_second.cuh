@@ -98,7 +98,7 @@ constexpr int kGiantSmem = kN * 8 + kGiantPolys * kPadN * 4;
 template <int ELL>
 __global__ void __launch_bounds__(kNttThreads) k_giant_fused(uint32_t* sout, const uint32_t* __restrict__ gkeys,
                                                              const uint16_t* __restrict__ gsigma, int N1,
-                                                             NttTables tabs, GadgetB g, int R, Batch bt, int r0) {
+                                                             NttTables tabs, GadgetB g, int R, Batch bt) {
     static_assert(2 * ELL <= kGiantPolys, "shared-memory polynomials");
     extern __shared__ __align__(16) uint8_t smem_raw[];
     uint2* tws = reinterpret_cast<uint2*>(smem_raw);
@@ -106,7 +106,7 @@ __global__ void __launch_bounds__(kNttThreads) k_giant_fused(uint32_t* sout, con
     const int N2 = kN / 2 / N1;
     const int rows = R * N2;
     const int rc = blockIdx.x;
-    const int r = r0 + rc / (N2 - 1), c = rc % (N2 - 1) + 1;   // sub-databases from r0 (grid: their steps)
+    const int r = rc / (N2 - 1), c = rc % (N2 - 1) + 1;
     const int row = r * N2 + c;
     const int tid = threadIdx.x;
     sout = shifted(sout, ws_off(bt));
@@ -183,13 +183,12 @@ __global__ void __launch_bounds__(kNttThreads) k_giant_fused(uint32_t* sout, con
 
 // result[r][comp][ch][k] = (output[0] + the N2 - 1 giant-step contributions)
 // mod q: the sum of the N2 rows of sub-database r after k_giant_fused.
-// Sub-databases [r0, r0 + count) of R.
 __global__ void k_giant_finish(const uint32_t* __restrict__ sout, uint32_t* __restrict__ result, int R, int N2,
-                               Batch bt, int r0, int count) {
+                               Batch bt) {
     pdl_launch_dependents();
     pdl_wait();
-    const long idx = (long)r0 * 4 * kN + (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= (long)(r0 + count) * 4 * kN) return;
+    const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long)R * 4 * kN) return;
     sout = shifted(sout, ws_off(bt));
     result = shifted(result, ws_off(bt));
     const int k = (int)(idx % kN);
@@ -524,7 +523,7 @@ __global__ void __launch_bounds__(kNttThreads) k_ext_fused(const uint32_t* __res
                                                            const uint32_t* __restrict__ init,
                                                            uint32_t* __restrict__ ext,
                                                            uint32_t* __restrict__ coef_out, NttTables tabs,
-                                                           GadgetS g, Batch bt, int r0) {
+                                                           GadgetS g, Batch bt) {
     static_assert(2 * ELL <= kExtPolys, "shared-memory polynomials");
     extern __shared__ __align__(16) uint8_t smem_raw[];
     first_dim = shifted(first_dim, ws_off(bt));
@@ -534,7 +533,7 @@ __global__ void __launch_bounds__(kNttThreads) k_ext_fused(const uint32_t* __res
     rgsw = shifted(rgsw, key_off(bt));
     uint2* tws = reinterpret_cast<uint2*>(smem_raw);
     uint32_t* P = reinterpret_cast<uint32_t*>(smem_raw + kN * 8);   // [4][N]
-    const int r = r0 + (blockIdx.x >> 1), ch = blockIdx.x & 1;   // sub-databases from r0
+    const int r = blockIdx.x >> 1, ch = blockIdx.x & 1;
     const uint32_t* fd = first_dim + (size_t)r * 4 * kN;          // [comp][prime][N]
     pdl_launch_dependents();
     // first_dim to coefficient form, all four polynomials (P[comp * 2 + prime])

@@ -256,11 +256,7 @@ struct kspir_ctx {
     ClientKeysDev keys0{};
     std::vector<char> key_loaded;
     // CUDA graphs of the four non-scan phases per (slot0, queries)
-    // baby steps, giant steps, external products, packing; for single
-    // answers also the split tail: giant steps + external products of the
-    // first half of the sub-databases, giant steps and external products of
-    // the second half
-    struct PhaseGraphs { cudaGraphExec_t g[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr}; };
+    struct PhaseGraphs { cudaGraphExec_t g[4] = {nullptr, nullptr, nullptr, nullptr}; };
     std::map<std::pair<int, int>, PhaseGraphs> graphs;
     cudaStream_t capture = nullptr;
     bool use_graphs = true;
@@ -304,12 +300,6 @@ struct kspir_ctx {
     std::vector<char> slot_used;
     std::vector<char> slot_busy;
     std::vector<cudaStream_t> slot_last_stream;   // stream of each slot's last answer
-    // a single answer alone runs the giant steps and external products of its
-    // first half of sub-databases on the slot's aux stream, beside the scan
-    // of the second half (split_ev: first scan done, first tail done)
-    bool split = true;
-    std::vector<cudaStream_t> slot_aux;
-    std::vector<std::array<cudaEvent_t, 2>> split_ev;
     int* single_errs = nullptr;
     std::condition_variable slot_cv;
     std::mutex mu;            // serialises enqueues from several host threads
@@ -677,11 +667,8 @@ void launch_scan_mma(kspir_ctx* c, int slot0, int nq, cudaStream_t st) {
 
 // `share`: another single answer runs beside this one, so the CUDA-core scan
 // takes the ring shape that leaves room for that answer's key-switch CTAs.
-// The CUDA-core scan covers sub-databases [r0, r0 + count) (count 0: all).
-void enqueue_scan(kspir_ctx* c, int slot0, int nq, int kind, cudaStream_t st, bool share = false, int r0 = 0,
-                  int count = 0) {
+void enqueue_scan(kspir_ctx* c, int slot0, int nq, int kind, cudaStream_t st, bool share = false) {
     const int R = c->p.r;
-    const int Rl = count > 0 ? count : R;
     if (kind == SCAN_CUDA) {
         for (int q = 0; q < nq; q++) {
             const Workspace w = ws_host(c, slot0 + q);
@@ -691,10 +678,10 @@ void enqueue_scan(kspir_ctx* c, int slot0, int nq, int kind, cudaStream_t st, bo
         if (share) {                                                                                         \
             using SC = typename ScanShare<n>::Cfg;                                                           \
             k_scan<n, SC::CONS, SC::NST><<<c->scan_ctas, SC::THREADS, SC::SMEM, st>>>(                        \
-                c->db, w.cipherbuf, w.sout, Rl, w.err, c->wait_limit_ns, c->scan_skip, r0, R);                \
+                c->db, w.cipherbuf, w.sout, R, w.err, c->wait_limit_ns, c->scan_skip);                        \
         } else {                                                                                             \
             k_scan<n><<<c->scan_ctas, ScanCfg<n>::THREADS, ScanCfg<n>::SMEM, st>>>(                          \
-                c->db, w.cipherbuf, w.sout, Rl, w.err, c->wait_limit_ns, c->scan_skip, r0, R);                \
+                c->db, w.cipherbuf, w.sout, R, w.err, c->wait_limit_ns, c->scan_skip);                        \
         }                                                                                                    \
         break;
                 KS_SCAN(64) KS_SCAN(128) KS_SCAN(256)
@@ -712,18 +699,15 @@ void enqueue_scan(kspir_ctx* c, int slot0, int nq, int kind, cudaStream_t st, bo
     }
 }
 
-// giant steps and row sums of sub-databases [r0, r0 + count) (count 0: all)
-void enqueue_giant(kspir_ctx* c, int slot0, int nq, cudaStream_t st, int r0 = 0, int count = 0) {
+void enqueue_giant(kspir_ctx* c, int slot0, int nq, cudaStream_t st) {
     const Workspace& w = c->ws0;
     const Batch bt = batch_of(c, slot0);
     const int R = c->p.r;
-    const int Rl = count > 0 ? count : R;
     if (c->N2 > 1)
-        launch(c, false, k_giant_fused<2>, dim3(Rl * (c->N2 - 1), nq), kNttThreads, kGiantSmem, st, w.sout,
-               (const uint32_t*)c->keys0.giant, (const uint16_t*)c->sigma_giant, c->N1, c->ntabs, c->gad.giant, R, bt,
-               r0);
-    launch(c, false, k_giant_finish, dim3(blocks_for((long)Rl * 4 * kN, 256), nq), 256, 0, st, (const uint32_t*)w.sout,
-           w.result, R, c->N2, bt, r0, Rl);
+        launch(c, false, k_giant_fused<2>, dim3(R * (c->N2 - 1), nq), kNttThreads, kGiantSmem, st, w.sout,
+               (const uint32_t*)c->keys0.giant, (const uint16_t*)c->sigma_giant, c->N1, c->ntabs, c->gad.giant, R, bt);
+    launch(c, false, k_giant_finish, dim3(blocks_for((long)R * 4 * kN, 256), nq), 256, 0, st, (const uint32_t*)w.sout,
+           w.result, R, c->N2, bt);
 }
 
 // external products of `count` first-dimension results (result -> ext);
@@ -731,10 +715,10 @@ void enqueue_giant(kspir_ctx* c, int slot0, int nq, cudaStream_t st, int r0 = 0,
 // address) or is null for zero; coef_out (or null) receives the
 // first-dimension results in coefficient form
 void enqueue_ext(kspir_ctx* c, int slot0, int nq, int count, const uint32_t* init, uint32_t* coef_out,
-                 cudaStream_t st, int r0 = 0) {
+                 cudaStream_t st) {
     const Workspace& w = c->ws0;
     launch(c, false, k_ext_fused<2>, dim3(count * 2, nq), kNttThreads, kExtSmem, st, (const uint32_t*)w.result,
-           (const uint32_t*)c->keys0.rgsw, init, w.ext, coef_out, c->ntabs, c->gad.ext, batch_of(c, slot0), r0);
+           (const uint32_t*)c->keys0.rgsw, init, w.ext, coef_out, c->ntabs, c->gad.ext, batch_of(c, slot0));
 }
 
 // c2out (or null; split kernels only): receives each merge's X^I c + r, the
@@ -781,20 +765,13 @@ int build_graphs(kspir_ctx* c, int slot0, int nq, bool rm, kspir_ctx::PhaseGraph
     if (it != c->graphs.end()) { *out = &it->second; return KSPIR_OK; }
     kspir_ctx::PhaseGraphs pg;
     cudaStream_t cs = c->capture;
-    const int R = c->p.r, h = R / 2;
-    const int nph = (nq == 1 && R >= 2) ? 7 : 4;
-    for (int ph = 0; ph < nph; ph++) {
+    for (int ph = 0; ph < 4; ph++) {
         cudaGraph_t g = nullptr;
         KS_CUDA(c, cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
         if (ph == 0) enqueue_baby(c, slot0, nq, rm, cs);
         else if (ph == 1) enqueue_giant(c, slot0, nq, cs);
-        else if (ph == 2) enqueue_ext(c, slot0, nq, R, nullptr, nullptr, cs);
-        else if (ph == 3) enqueue_packing(c, slot0, nq, cs);
-        else if (ph == 4) {
-            enqueue_giant(c, slot0, nq, cs, 0, h);
-            enqueue_ext(c, slot0, nq, h, nullptr, nullptr, cs, 0);
-        } else if (ph == 5) enqueue_giant(c, slot0, nq, cs, h, R - h);
-        else enqueue_ext(c, slot0, nq, R - h, nullptr, nullptr, cs, h);
+        else if (ph == 2) enqueue_ext(c, slot0, nq, c->p.r, nullptr, nullptr, cs);
+        else enqueue_packing(c, slot0, nq, cs);
         KS_CUDA(c, cudaStreamEndCapture(cs, &g));
         cudaError_t e = cudaGraphInstantiate(&pg.g[ph], g, 0);
         cudaGraphDestroy(g);
@@ -895,42 +872,6 @@ int enqueue_answer(kspir_ctx* c, int slot0, int nq, const int* clients, cudaStre
     k_set_clients<<<1, kMaxBatch, 0, st>>>(c->client_of, slot0, cl);
     const int kind = scan_kind_for(c, nq);
     c->last_kind = kind;
-    const bool split = allow_fused && nq == 1 && !share && c->split && c->p.r >= 2 && kind == SCAN_CUDA &&
-                       c->use_graphs && slot0 < c->single_slots;
-    if (split) {
-        // one answer alone: the giant steps and external products of the first
-        // half of the sub-databases run on the slot's aux stream beside the
-        // scan of the second half (sharing ring shape, room for their CTAs)
-        kspir_ctx::PhaseGraphs* pg = nullptr;
-        int rc = build_graphs(c, slot0, nq, false, &pg);
-        if (rc) return rc;
-        const int R = c->p.r, h = R / 2;
-        cudaStream_t aux = c->slot_aux[slot0];
-        auto& se = c->split_ev[slot0];
-        cudaEventRecord(ev[0], st);
-        KS_CUDA(c, cudaGraphLaunch(pg->g[0], st));
-        cudaEventRecord(ev[1], st);
-        enqueue_scan(c, slot0, nq, kind, st, false, 0, h);
-        KS_CUDA(c, cudaEventRecord(se[0], st));
-        enqueue_scan(c, slot0, nq, kind, st, true, h, R - h);
-        cudaEventRecord(ev[2], st);
-        KS_CUDA(c, cudaStreamWaitEvent(aux, se[0], 0));
-        KS_CUDA(c, cudaGraphLaunch(pg->g[4], aux));
-        KS_CUDA(c, cudaEventRecord(se[1], aux));
-        KS_CUDA(c, cudaGraphLaunch(pg->g[5], st));
-        cudaEventRecord(ev[3], st);
-        KS_CUDA(c, cudaGraphLaunch(pg->g[6], st));
-        KS_CUDA(c, cudaStreamWaitEvent(st, se[1], 0));
-        cudaEventRecord(ev[4], st);
-        KS_CUDA(c, cudaGraphLaunch(pg->g[3], st));
-        cudaEventRecord(ev[5], st);
-        c->ring_nq[slot] = nq;
-        c->enqueues++;
-        c->answers += nq;
-        c->launches += answer_launches(c, kind, nq) + 1;   // the scan in two launches
-        c->last_slot = slot;
-        return KSPIR_OK;
-    }
     if (c->use_graphs) {
         kspir_ctx::PhaseGraphs* pg = nullptr;
         int rc = build_graphs(c, slot0, nq, kind != SCAN_CUDA, &pg);
@@ -1300,13 +1241,6 @@ int kspir_ctx_create(int device, const kspir_params* params, kspir_ctx** out) {
         KS_CUDA(c.get(), cudaStreamCreateWithFlags(&c->slot_stream[i], cudaStreamNonBlocking));
     }
     KS_CUDA(c.get(), cudaHostAlloc(&c->single_errs, (size_t)c->single_slots * 4, cudaHostAllocDefault));
-    c->slot_aux.assign(c->single_slots, nullptr);
-    c->split_ev.assign(c->single_slots, {nullptr, nullptr});
-    for (int i = 0; i < c->single_slots; i++) {
-        KS_CUDA(c.get(), cudaStreamCreateWithFlags(&c->slot_aux[i], cudaStreamNonBlocking));
-        for (auto& e : c->split_ev[i]) KS_CUDA(c.get(), cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-    }
-    if (const char* e = getenv("KSPIR_NO_SPLIT")) c->split = !(e[0] == '1');
     rc = init_key_slots(c.get());
     if (rc) return rc;
     rc = init_workspaces(c.get());
@@ -1328,9 +1262,6 @@ int kspir_ctx_destroy(kspir_ctx* c) {
     for (auto& e : c->slot_done) if (e) cudaEventDestroy(e);
     for (auto& e : c->host_done) if (e) cudaEventDestroy(e);
     for (auto& st : c->slot_stream) if (st) cudaStreamDestroy(st);
-    for (auto& st : c->slot_aux) if (st) cudaStreamDestroy(st);
-    for (auto& evs : c->split_ev)
-        for (auto& e : evs) if (e) cudaEventDestroy(e);
     if (c->single_errs) cudaFreeHost(c->single_errs);
     for (auto& kv : c->graphs)
         for (auto& g : kv.second.g) if (g) cudaGraphExecDestroy(g);
