@@ -450,7 +450,9 @@ def run_gpu(args, rank, world, local_rank):
                                    "packing": phases[4] / answers},
             "roofline": {"bound": "hbm", "kernel": "k_scan", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_src,
-                         "algorithmic_bytes_per_launch": db_bytes, "traffic": read_traffic(r)},
+                         "algorithmic_bytes_per_launch": db_bytes, "traffic": read_traffic(r),
+                         "timed_in": "the latency run (one answer at a time): mean CUDA-event duration "
+                                     "of the scan launch on the answer's stream"},
             "e2e": {"value": world * args.steps / e2e_s, "unit": "queries/s",
                     "h2d_bytes_per_step": 4 * N * 8, "d2h_bytes_per_step": 2 * N * 8,
                     "host_threads": S, "one_caller_queries_per_s": world * max(args.steps // 4, 10) / e2e_serial_s},
