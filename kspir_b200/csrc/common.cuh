@@ -62,17 +62,21 @@ __device__ __forceinline__ uint32_t shoup_lazy(uint32_t x, uint32_t w, uint32_t 
     return x * w - t * q;
 }
 
+// Conditional subtractions as an unsigned minimum: for x < 2m, x - m wraps
+// above x exactly when x < m.
 __device__ __forceinline__ uint32_t shoup_mul(uint32_t x, uint32_t w, uint32_t wp, uint32_t q) {
-    uint32_t r = shoup_lazy(x, w, wp, q);
-    return r >= q ? r - q : r;
+    const uint32_t r = shoup_lazy(x, w, wp, q);
+    return umin(r, r - q);
 }
 
-// Exact reduction of a product or a short sum of products (< 2^62) by Barrett.
+// Exact reduction of any 64-bit p by Barrett with barrett = floor(2^64 / q):
+// qh = floor(p * barrett / 2^64) is floor(p / q) or one less (p * barrett
+// falls short of p * 2^64 / q by less than p < 2^64), so p - qh q is in
+// [0, 2q) and is computed in 32 bits.
 __device__ __forceinline__ uint32_t reduce64(uint64_t p, uint32_t q, uint64_t barrett) {
-    uint64_t qh = __umul64hi(p, barrett);
-    uint64_t r = p - qh * q;
-    while (r >= q) r -= q;   // at most twice for p < 2^62
-    return (uint32_t)r;
+    const uint32_t qh = (uint32_t)__umul64hi(p, barrett);
+    const uint32_t r = (uint32_t)p - qh * q;
+    return umin(r, r - q);
 }
 
 __device__ __forceinline__ uint32_t mulmod(uint32_t a, uint32_t b, int ch) {
@@ -80,12 +84,13 @@ __device__ __forceinline__ uint32_t mulmod(uint32_t a, uint32_t b, int ch) {
 }
 
 __device__ __forceinline__ uint32_t addmod(uint32_t a, uint32_t b, uint32_t q) {
-    uint32_t s = a + b;
-    return s >= q ? s - q : s;
+    const uint32_t s = a + b;
+    return umin(s, s - q);
 }
 
 __device__ __forceinline__ uint32_t submod(uint32_t a, uint32_t b, uint32_t q) {
-    return a >= b ? a - b : a + q - b;
+    const uint32_t d = a - b;   // wraps when a < b, and d + q is then the residue
+    return umin(d, d + q);
 }
 
 // A signed small integer (|v| < q) as a canonical residue.
@@ -106,15 +111,18 @@ __device__ __forceinline__ uint64_t crt_compose_res(uint32_t r1, uint32_t r2) {
 
 // x mod q, exact for every 64-bit x, q a prime in (2^27, 2^28); mu1 = 2^59 / q,
 // c32 = 2^32 mod q, mu2 = 2^57 / q.  Two Barrett steps with 32x32 products.
+__host__ __device__ __forceinline__ uint32_t min_u32(uint32_t a, uint32_t b) { return a < b ? a : b; }
+
 __host__ __device__ __forceinline__ uint32_t mod28(uint64_t x, uint32_t q, uint32_t mu1, uint32_t c32, uint32_t mu2) {
     const uint32_t xh = (uint32_t)(x >> 32), xl = (uint32_t)x;
+    // conditional subtractions as minima (x - m wraps above x when x < m)
     uint32_t r = xh - (uint32_t)(((uint64_t)xh * mu1) >> 59) * q;   // in [0, 2q)
-    r = r >= q ? r - q : r;
+    r = min_u32(r, r - q);
     const uint64_t y = (uint64_t)r * c32 + xl;                       // < 2^57, same residue
     const uint32_t qh = (uint32_t)(((y >> 26) * mu2) >> 31);
     uint32_t t = (uint32_t)y - qh * q;                                // in [0, 3q)
-    t = t >= q ? t - q : t;
-    return t >= q ? t - q : t;
+    t = min_u32(t, t - 2 * q);                                        // in [0, 2q)
+    return min_u32(t, t - q);
 }
 
 // x mod q_ch for the crt primes (ch 0: q1, 1: q2), any 64-bit x.  (mod28 measured

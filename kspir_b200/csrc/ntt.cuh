@@ -105,16 +105,19 @@ __device__ __forceinline__ void unit_store(uint32_t* s, int b, const uint32_t* x
     }
 }
 
+// x - m if x >= m else x, for x < 2m < 2^32: one subtraction and an unsigned
+// minimum (x - m wraps above x when x < m)
+__device__ __forceinline__ uint32_t sub_if_ge(uint32_t x, uint32_t m) { return umin(x, x - m); }
+
 __device__ __forceinline__ void fwd_bfly(uint32_t& X, uint32_t& Y, uint2 w, uint32_t q, uint32_t q2) {
-    uint32_t x = X >= q2 ? X - q2 : X;
+    uint32_t x = sub_if_ge(X, q2);
     uint32_t t = shoup_lazy(Y, w.x, w.y, q);
     X = x + t;
     Y = x - t + q2;
 }
 
 __device__ __forceinline__ void inv_bfly(uint32_t& X, uint32_t& Y, uint2 w, uint32_t q, uint32_t q2) {
-    uint32_t s = X + Y;
-    s = s >= q2 ? s - q2 : s;
+    uint32_t s = sub_if_ge(X + Y, q2);
     uint32_t d = shoup_lazy(X - Y + q2, w.x, w.y, q);
     X = s;
     Y = d;
@@ -148,8 +151,7 @@ __device__ __forceinline__ void fwd_pass(uint32_t* s, int stride, const uint2* t
         if (P == 3) {
 #pragma unroll
             for (int t = 0; t < 8; t++) {
-                uint32_t v = x[m][t] >= q2 ? x[m][t] - q2 : x[m][t];
-                x[m][t] = v >= q ? v - q : v;
+                x[m][t] = sub_if_ge(sub_if_ge(x[m][t], q2), q);
             }
         }
     }
