@@ -95,7 +95,8 @@ __device__ __forceinline__ uint32_t submod(uint32_t a, uint32_t b, uint32_t q) {
 
 // A signed small integer (|v| < q) as a canonical residue.
 __device__ __forceinline__ uint32_t signed_to_res(int64_t v, uint32_t q) {
-    return v < 0 ? (uint32_t)(v + (int64_t)q) : (uint32_t)v;
+    const uint32_t u = (uint32_t)v;   // above 2^32 - q exactly when v < 0, and u + q then wraps to v + q
+    return umin(u, u + q);
 }
 
 // ---------------------------------------------------------------------------
@@ -103,8 +104,8 @@ __device__ __forceinline__ uint32_t signed_to_res(int64_t v, uint32_t q) {
 
 // canonical value mod crtMod from its residues (Garner)
 __device__ __forceinline__ uint64_t crt_compose_res(uint32_t r1, uint32_t r2) {
-    uint32_t r1m = r1 >= kQ2 ? r1 - kQ2 : r1;           // r1 mod q2 (q1 < 2 q2)
-    uint32_t d = r2 >= r1m ? r2 - r1m : r2 + kQ2 - r1m;  // (r2 - r1) mod q2
+    const uint32_t r1m = umin(r1, r1 - kQ2);             // r1 mod q2 (q1 < 2 q2)
+    const uint32_t d = submod(r2, r1m, kQ2);             // (r2 - r1) mod q2
     uint32_t t = shoup_mul(d, c_dev.q1inv_mod_q2, c_dev.q1inv_mod_q2_p, kQ2);
     return (uint64_t)r1 + (uint64_t)kQ1 * t;
 }
@@ -173,7 +174,8 @@ __device__ __forceinline__ int auto_src(int k, uint32_t ginv, bool* neg) {
     return (int)(i0 & (kN - 1));
 }
 
-__device__ __forceinline__ uint32_t negmod(uint32_t x, uint32_t q) { return x ? q - x : 0; }
+// q - x, and 0 for x = 0 (0 - x wraps above q - x for every other x)
+__device__ __forceinline__ uint32_t negmod(uint32_t x, uint32_t q) { return umin(q - x, 0u - x); }
 
 // acc += a * b with a 32x32->64-bit product, as one fused wide multiply-add
 __device__ __forceinline__ void mad_wide(uint64_t& acc, uint32_t a, uint32_t b) {
