@@ -182,22 +182,28 @@ __global__ void __launch_bounds__(kNttThreads) k_giant_fused(uint32_t* sout, con
 }
 
 // result[r][comp][ch][k] = (output[0] + the N2 - 1 giant-step contributions)
-// mod q: the sum of the N2 rows of sub-database r after k_giant_fused.
+// mod q: the sum of the N2 rows of sub-database r after k_giant_fused.  One
+// thread per four consecutive slots (16-byte loads from each row's sectors).
 __global__ void k_giant_finish(const uint32_t* __restrict__ sout, uint32_t* __restrict__ result, int R, int N2,
                                Batch bt) {
     pdl_launch_dependents();
     pdl_wait();
     const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= (long)R * 4 * kN) return;
+    if (idx >= (long)R * 4 * (kN / 4)) return;
     sout = shifted(sout, ws_off(bt));
     result = shifted(result, ws_off(bt));
-    const int k = (int)(idx % kN);
-    const int cc_ = (int)((idx / kN) % 4);      // comp * 2 + ch
-    const int r = (int)(idx / (4 * kN));
+    const int z = (int)(idx % (kN / 4)) * 4;
+    const int cc_ = (int)((idx / (kN / 4)) % 4);      // comp * 2 + ch
+    const int r = (int)(idx / (4 * (kN / 4)));
     const ChanConst q = c_dev.ch[cc_ & 1];
-    uint64_t v = 0;
-    for (int c = 0; c < N2; c++) v += __ldcg(sout + sout_idx(r * N2 + c, cc_, k, R * N2));
-    result[idx] = reduce64(v, q.q, q.barrett);
+    uint64_t v0 = 0, v1 = 0, v2 = 0, v3 = 0;
+    for (int c = 0; c < N2; c++) {
+        const uint4 w = __ldcg(reinterpret_cast<const uint4*>(sout + sout_idx(r * N2 + c, cc_, z, R * N2)));
+        v0 += w.x; v1 += w.y; v2 += w.z; v3 += w.w;
+    }
+    *reinterpret_cast<uint4*>(result + ((size_t)r * 4 + cc_) * kN + z) =
+        make_uint4(reduce64(v0, q.q, q.barrett), reduce64(v1, q.q, q.barrett), reduce64(v2, q.q, q.barrett),
+                   reduce64(v3, q.q, q.barrett));
 }
 
 }  // namespace kspir

@@ -706,7 +706,7 @@ void enqueue_giant(kspir_ctx* c, int slot0, int nq, cudaStream_t st) {
     if (c->N2 > 1)
         launch(c, false, k_giant_fused<2>, dim3(R * (c->N2 - 1), nq), kNttThreads, kGiantSmem, st, w.sout,
                (const uint32_t*)c->keys0.giant, (const uint16_t*)c->sigma_giant, c->N1, c->ntabs, c->gad.giant, R, bt);
-    launch(c, false, k_giant_finish, dim3(blocks_for((long)R * 4 * kN, 256), nq), 256, 0, st, (const uint32_t*)w.sout,
+    launch(c, false, k_giant_finish, dim3(blocks_for((long)R * 4 * (kN / 4), 256), nq), 256, 0, st, (const uint32_t*)w.sout,
            w.result, R, c->N2, bt);
 }
 
