@@ -62,7 +62,6 @@ __device__ __forceinline__ uint32_t pow5_mod2n(uint32_t e) {
     return r;
 }
 
-constexpr int kBabySmem = kN * 8 + kPadN * 4;       // twiddles + one padded polynomial
 constexpr int kBabyPairSmem = kN * 8 + 2 * kPadN * 4;   // twiddles + two padded polynomials
 constexpr int kPerThread = kN / kNttThreads; // 8 coefficients per thread
 
@@ -196,32 +195,12 @@ __device__ __forceinline__ void baby_crt_part(const BabyRot& R, const BabyArgs& 
     }
 }
 
-// One CTA per (rotation, component, crt prime): blockIdx.x = 4*ki + 2*comp + ch;
-// blockIdx.y = query of the batch.  Each CTA recomputes the bsMod part of its
-// component (one inverse transform) so the four CTAs of a rotation run in
-// parallel: the shape for one query, whose 252 CTAs then fit one wave.
-// MINB CTAs per SM: 2 (at most 64 registers).
-template <int ELL, int MINB>
-__global__ void __launch_bounds__(kNttThreads, MINB) k_baby_rot(BabyArgs a, ClientKeysDev keys, NttTables tabs, Batch bt) {
-    extern __shared__ __align__(16) uint8_t smem_raw[];
-    uint2* tws = reinterpret_cast<uint2*>(smem_raw);
-    uint32_t* S = reinterpret_cast<uint32_t*>(smem_raw + kN * 8);
-    const int ch = blockIdx.x & 1;
-    BabyRot R;
-    pdl_launch_dependents();
-    stage_twiddles(tws, tabs, CH_BS, NTT_INV);
-    baby_setup<ELL>(R, a, keys, bt, blockIdx.x >> 2, (blockIdx.x >> 1) & 1);
-    pdl_wait();   // the digits come from the previous kernel
-    baby_bs_part<ELL>(R, a, S, tws, ch == 0);
-    baby_crt_part<ELL>(R, a, S, tws, tabs, ch);
-}
-
-// One CTA per (rotation, component): blockIdx.x = 2*ki + comp.  The bsMod part
-// runs once for both primes (six transforms per rotation instead of eight):
-// the shape for batches, which have CTAs enough to fill the GPU without the
-// duplicated work.  MINB 2: at 3 CTAs per SM (42 registers) it spills, and
-// measured no faster (batch of 64: baby steps 1.68 ms at 3, 1.66 ms at 2,
-// 1.74 ms for the four-CTA shape).
+// One CTA per (rotation, component): blockIdx.x = 2*ki + comp, blockIdx.y =
+// query of the batch.  The bsMod part runs once for both primes (six
+// transforms per rotation; a shape with one CTA per prime as well, which
+// recomputes it, ran eight and measured slower for single queries too once
+// the reductions were minimum-form).  MINB 2: at 3 CTAs per SM (40-42 registers) it spills, and
+// measured slower (batch of 64: baby steps 1.55 ms at 3, 1.32 ms at 2).
 template <int ELL, int MINB>
 __global__ void __launch_bounds__(kNttThreads, MINB) k_baby_pair(BabyArgs a, ClientKeysDev keys, NttTables tabs, Batch bt) {
     extern __shared__ __align__(16) uint8_t smem_raw[];

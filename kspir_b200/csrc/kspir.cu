@@ -607,13 +607,14 @@ void enqueue_baby(kspir_ctx* c, int slot0, int nq, bool rm, cudaStream_t st) {
     a1.dig = w.dig0; a1.srcB = w.qbn; a1.srcBbs = w.qbbs; a1.perms = c->perms; a1.sigma = c->sigma_baby;
     a1.cipherbuf = w.cipherbuf; a1.interA = w.interA; a1.interB = w.interB; a1.inter_bs = w.inter_bs;
     a1.N1 = c->N1; a1.col_base = 1; a1.inter_idx = c->N1h - 2;
+    // one CTA per (rotation, component), also for a single query: with the
+    // minimum-form reductions its six transforms per rotation beat the
+    // four-CTA shape (eight transforms) on one answer (0.399 against
+    // 0.403 ms) and on overlapped answers (0.229 against 0.235 ms)
     auto rot = [&](const BabyArgs& args, int nrot) {
         if (nrot <= 0) return;
-        if (nq == 1)
-            launch(c, false, k_baby_rot<3, 2>, dim3(nrot * 4, nq), kNttThreads, kBabySmem, st, args, c->keys0, c->ntabs, bt);
-        else
-            launch(c, false, k_baby_pair<3, 2>, dim3(nrot * 2, nq), kNttThreads, kBabyPairSmem, st, args, c->keys0, c->ntabs,
-                   bt);
+        launch(c, false, k_baby_pair<3, 2>, dim3(nrot * 2, nq), kNttThreads, kBabyPairSmem, st, args, c->keys0, c->ntabs,
+               bt);
     };
     rot(a1, c->N1h - 1);
     launch(c, false, k_ntt_jobs<true>, dim3(2, nq), kNttThreads, kNttJobSmem, st, (const NttJob*)(c->jobs + c->seg_inter),
@@ -1189,7 +1190,6 @@ int kspir_ctx_create(int device, const kspir_params* params, kspir_ctx** out) {
     KS_CUDA(c.get(), cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device));
     c->scan_ctas = c->nsm;
     if (const char* e = getenv("KSPIR_SCAN_CTAS")) c->scan_ctas = std::max(1, std::min(c->nsm, atoi(e)));
-    KS_CUDA(c.get(), cudaFuncSetAttribute(k_baby_rot<3, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBabySmem));
     KS_CUDA(c.get(), cudaFuncSetAttribute(k_baby_pair<3, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBabyPairSmem));
     KS_CUDA(c.get(), cudaFuncSetAttribute(k_client_query, cudaFuncAttributeMaxDynamicSharedMemorySize, kClientSmem));
     KS_CUDA(c.get(), cudaFuncSetAttribute(k_client_decrypt, cudaFuncAttributeMaxDynamicSharedMemorySize, kClientSmem));
