@@ -205,7 +205,11 @@ void srv_launch(Srv& s, Srv::Lane& L) {
         // against direct kspir_answer / kspir_answer_device calls
         const bool shares = L.slot0 < c->single_slots;
         if (!rc && shares) rc = wait_singles(c, L.st);
-        if (!rc) rc = enqueue_answer(c, L.slot0, n, slots.data(), L.st);
+        // a single query beside another lane's batch takes the scan ring
+        // shape that leaves room for that batch's key-switch CTAs
+        bool others = false;
+        for (const auto& O : s.lanes) others = others || (&O != &L && O.busy);
+        if (!rc) rc = enqueue_answer(c, L.slot0, n, slots.data(), L.st, false, others);
         if (!rc && cudaMemcpyAsync(L.hr, c->bresp + (size_t)L.slot0 * 2 * kN, (size_t)n * 2 * kN * 8,
                                    cudaMemcpyDeviceToHost, L.st) != cudaSuccess)
             rc = KSPIR_ERR_CUDA;
