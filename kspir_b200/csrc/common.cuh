@@ -40,6 +40,7 @@ struct ChanConst {
     uint32_t two_q;
     uint64_t barrett;      // floor(2^64 / q)
     uint32_t ninv, ninv_p; // N^-1 mod q and its Shoup companion
+    uint32_t ninv_w, ninv_w_p;   // N^-1 times the last inverse layer's twiddle (psi^-N/2), Shoup
     uint32_t bsinv, bsinv_p;  // bsMod^-1 mod crtMod, reduced mod q (crt channels only)
 };
 

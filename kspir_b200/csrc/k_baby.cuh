@@ -165,7 +165,7 @@ __device__ __forceinline__ void baby_crt_part(const BabyRot& R, const BabyArgs& 
     uint32_t* inter_out = shifted(comp == 0 ? a.interA : a.interB, R.wo);
     Sync::sync();   // x2 complete and the previous twiddles no longer read
     stage_twiddles(tws, tabs, ch, NTT_FWD);
-    cta_ntt_forward<Sync>(S, tws, ch);   // NTT_ch(x2), x2 < bsMod < q
+    cta_ntt_forward<Sync, true>(S, tws, ch);   // NTT_ch(x2), x2 < bsMod < q; outputs in [0, 4q)
 
     const ChanConst cc = c_dev.ch[ch];
     int pk[kPerThread];
@@ -187,7 +187,9 @@ __device__ __forceinline__ void baby_crt_part(const BabyRot& R, const BabyArgs& 
         uint32_t A = negmod(mod_crt(acc[it], ch), cc.q);
         if (comp == 1) A = addmod(A, __ldcg(shifted(a.srcB, R.wo) + ch * kN + sig[k]), cc.q);
         if (R.inter) inter_out[ch * kN + k] = A;
-        const uint32_t r = shoup_mul(submod(A, S[pidx(tid) + it * kPadStep], cc.q), cc.bsinv, cc.bsinv_p, cc.q);
+        // (A - S) bsMod^-1 with S in [0, 4q): A + 4q - S is in (0, 5q), and the
+        // Shoup product reduces any 32-bit input to a canonical residue
+        const uint32_t r = shoup_mul(A + 2 * cc.two_q - S[pidx(tid) + it * kPadStep], cc.bsinv, cc.bsinv_p, cc.q);
         if (a.cb_rm)
             cb32[cipherbuf_rm_idx(R.col, comp, ch, k)] = r;
         else

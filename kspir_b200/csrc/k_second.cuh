@@ -158,7 +158,9 @@ __global__ void __launch_bounds__(kNttThreads) k_giant_fused(uint32_t* sout, con
     for (int ch = 0; ch < 2; ch++) {
         __syncthreads();
         stage_twiddles(tws, tabs, ch, NTT_FWD);
-        cta_ntt_forward_m<ELL>(P + ch * kPadN, 2 * kPadN, tws, ch);   // digits j of this prime: P[j*2+ch]
+        // digits j of this prime: P[j*2+ch], left in [0, 4q) (they only feed the
+        // exact multiply-accumulate below)
+        cta_ntt_forward_m<ELL, CtaSync, true>(P + ch * kPadN, 2 * kPadN, tws, ch);
         const ChanConst cc = c_dev.ch[ch];
         uint32_t cbv[kPerThreadG];
 #pragma unroll
@@ -272,7 +274,7 @@ __global__ void __launch_bounds__(kNttThreads) k_pack_fused(const uint32_t* __re
         const uint32_t vb = submod(__ldcg(r0 + (1 * 2 + ch) * kN + src), cshift(1, ch, src), q);
         P[ELL * kPadN + pk] = neg ? negmod(vb, q) : vb;
     }
-    cta_ntt_forward_m<ELL + 1>(P, kPadN, tws, ch);
+    cta_ntt_forward_m<ELL + 1, CtaSync, true>(P, kPadN, tws, ch);   // outputs in [0, 4q)
 #pragma unroll
     for (int it = 0; it < kPerThreadG; it++) {
         const int k = tid + it * kNttThreads;
@@ -285,7 +287,7 @@ __global__ void __launch_bounds__(kNttThreads) k_pack_fused(const uint32_t* __re
         }
         const uint32_t a2 = negmod(mod_crt(sa, ch), q);
         const int pk = pidx(tid) + it * kPadStep;
-        const uint32_t b2 = submod(P[ELL * kPadN + pk], mod_crt(sb, ch), q);
+        const uint32_t b2 = submod(canon4q(P[ELL * kPadN + pk], q), mod_crt(sb, ch), q);
         P[pk] = a2;            // only this thread reads index k of these rows
         P[kPadN + pk] = b2;
     }
@@ -370,7 +372,7 @@ __device__ __forceinline__ void pack_split_fwd_body(const uint32_t* __restrict__
         }
         S[pidx(tid) + it * kPadStep] = v;
     }
-    cta_ntt_forward<Sync>(S, tws, ch);
+    cta_ntt_forward<Sync, true>(S, tws, ch);   // outputs in [0, 4q)
     uint32_t* pa = part + (((size_t)j * 2 + ch) * (ELL + 1) + d) * 2 * kN;
 #pragma unroll
     for (int it = 0; it < kPerThreadG; it++) {
@@ -380,7 +382,7 @@ __device__ __forceinline__ void pack_split_fwd_body(const uint32_t* __restrict__
             pa[k] = mod_crt((uint64_t)dv * ka[it], ch);
             pa[kN + k] = mod_crt((uint64_t)dv * kb[it], ch);
         } else {
-            pa[k] = dv;   // NTT(temp.b)
+            pa[k] = canon4q(dv, q);   // NTT(temp.b)
         }
     }
 }
@@ -482,7 +484,7 @@ __device__ __forceinline__ void ext_tail(uint32_t* P, uint2* tws, const uint32_t
 #pragma unroll
         for (int row = 0; row < 2 * ELL; row++) P[row * kPadN + pidx(tid) + it * kPadStep] = dres[it][row];
     stage_twiddles(tws, tabs, ch, NTT_FWD);
-    cta_ntt_forward_m<2 * ELL, Sync>(P, kPadN, tws, ch);
+    cta_ntt_forward_m<2 * ELL, Sync, true>(P, kPadN, tws, ch);   // digits in [0, 4q), for the exact sum below
     const ChanConst cq = c_dev.ch[ch];
     uint32_t outv[kPerThreadG][2];
 #pragma unroll

@@ -397,6 +397,19 @@ const uint32_t kChanQ[CH_COUNT] = {kQ1, kQ2, kBsMod, kP, kBsMod, kAuxMod, kAuxMo
 const uint64_t kRootCrt = 3375402822066082ull;     // root_of_unity_crt, crt.h:81
 const uint64_t kRootCrtBa = 1486445687605966ull;   // root_of_unity_crt_bamod, crt.h:82
 
+// the transform root psi of each channel: crt channels use root_of_unity_crt
+// (reference crt.h:81) reduced per prime; bsMod and p use HEXL's minimal
+// primitive root
+uint64_t chan_root(int ch) {
+    switch (ch) {
+        case CH_Q1: return kRootCrt % kQ1;
+        case CH_Q2: return kRootCrt % kQ2;
+        case CH_BA_BS: return kRootCrtBa % kBsMod;
+        case CH_BA_AUX: return kRootCrtBa % kAuxMod;
+        default: return h_min_root(kChanQ[ch]);
+    }
+}
+
 // every per-channel constant of c_dev (also written by the allocation-free set-up)
 DevConst make_dev_const() {
     DevConst dc{};
@@ -408,6 +421,12 @@ DevConst make_dev_const() {
         cc.barrett = ~0ull / q;
         cc.ninv = (uint32_t)h_invmod(kN, q);
         cc.ninv_p = shoup32(cc.ninv, q);
+        // the last inverse layer's single twiddle is entry 1 of the inverse
+        // table: psi^-brv(1) = psi^-(N/2); folding N^-1 into it saves one
+        // multiplication per butterfly of that layer
+        const uint64_t iw1 = h_powmod(h_invmod(chan_root(ch), q), h_bitrev12(1), q);
+        cc.ninv_w = (uint32_t)(iw1 * cc.ninv % q);
+        cc.ninv_w_p = shoup32(cc.ninv_w, q);
         cc.bsinv = ch < 2 ? (uint32_t)(kBsModInvCrt % q) : 0;
         cc.bsinv_p = shoup32(cc.bsinv, q);
     }
@@ -423,8 +442,8 @@ int init_constants(kspir_ctx* c) {
 
     // twiddles: crt channels use root_of_unity_crt (reference crt.h:81) reduced
     // per prime; bsMod and p use HEXL's minimal primitive root
-    const uint64_t roots[CH_COUNT] = {kRootCrt % kQ1,      kRootCrt % kQ2,        h_min_root(kBsMod), h_min_root(kP),
-                                      kRootCrtBa % kBsMod, kRootCrtBa % kAuxMod, h_min_root(kAuxMod)};
+    uint64_t roots[CH_COUNT];
+    for (int ch = 0; ch < CH_COUNT; ch++) roots[ch] = chan_root(ch);
     // per channel uint2 [2][N]: {psi^brv(k), Shoup} then {psi^-brv(k), Shoup}, k-major order
     std::vector<uint32_t> tw((size_t)CH_COUNT * 4 * kN);
     for (int ch = 0; ch < CH_COUNT; ch++) {

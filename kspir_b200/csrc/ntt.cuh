@@ -125,7 +125,8 @@ __device__ __forceinline__ void inv_bfly(uint32_t& X, uint32_t& Y, uint2 w, uint
 
 // One forward pass over M polynomials (s + m * stride): thread u's radix-8 unit
 // of each, three butterfly layers, no barrier inside (units are disjoint).
-template <int P, int M>
+// LAZY: the last pass leaves its outputs in [0, 4q) instead of canonical.
+template <int P, int M, bool LAZY = false>
 __device__ __forceinline__ void fwd_pass(uint32_t* s, int stride, const uint2* tws, uint32_t q, uint32_t q2, int u) {
     constexpr int lq = 9 - 3 * P, q8 = 1 << lq, m0 = 1 << (3 * P);
     const int i0 = u >> lq, j = u & (q8 - 1);
@@ -148,7 +149,7 @@ __device__ __forceinline__ void fwd_pass(uint32_t* s, int stride, const uint2* t
         fwd_bfly(x[m][2], x[m][3], wc1, q, q2);
         fwd_bfly(x[m][4], x[m][5], wc2, q, q2);
         fwd_bfly(x[m][6], x[m][7], wc3, q, q2);
-        if (P == 3) {
+        if (P == 3 && !LAZY) {
 #pragma unroll
             for (int t = 0; t < 8; t++) {
                 x[m][t] = sub_if_ge(sub_if_ge(x[m][t], q2), q);
@@ -161,7 +162,7 @@ __device__ __forceinline__ void fwd_pass(uint32_t* s, int stride, const uint2* t
 
 template <int P, int M>
 __device__ __forceinline__ void inv_pass(uint32_t* s, int stride, const uint2* tws, uint32_t q, uint32_t q2,
-                                         uint32_t ni, uint32_t nip, int u) {
+                                         uint32_t ni, uint32_t nip, int u, int ch) {
     constexpr int lq = 9 - 3 * P, q8 = 1 << lq, m0 = 1 << (3 * P);
     const int i0 = u >> lq, j = u & (q8 - 1);
     const int b = pidx(i0 * 8 * q8 + j);
@@ -181,11 +182,20 @@ __device__ __forceinline__ void inv_pass(uint32_t* s, int stride, const uint2* t
         inv_bfly(x[m][1], x[m][3], wb0, q, q2);
         inv_bfly(x[m][4], x[m][6], wb1, q, q2);
         inv_bfly(x[m][5], x[m][7], wb1, q, q2);
-#pragma unroll
-        for (int t = 0; t < 4; t++) inv_bfly(x[m][t], x[m][t + 4], wa, q, q2);
         if (P == 0) {
+            // the last layer with N^-1 folded in (its one twiddle wa times
+            // N^-1 is a per-channel constant): X + Y and X - Y each take one
+            // product and come out canonical
+            const ChanConst& cc = c_dev.ch[ch];
 #pragma unroll
-            for (int t = 0; t < 8; t++) x[m][t] = shoup_mul(x[m][t], ni, nip, q);
+            for (int t = 0; t < 4; t++) {
+                const uint32_t X = x[m][t], Y = x[m][t + 4];
+                x[m][t] = shoup_mul(X + Y, ni, nip, q);
+                x[m][t + 4] = shoup_mul(X - Y + q2, cc.ninv_w, cc.ninv_w_p, q);
+            }
+        } else {
+#pragma unroll
+            for (int t = 0; t < 4; t++) inv_bfly(x[m][t], x[m][t + 4], wa, q, q2);
         }
     }
 #pragma unroll
@@ -194,9 +204,11 @@ __device__ __forceinline__ void inv_pass(uint32_t* s, int stride, const uint2* t
 
 // Forward transforms of M padded polynomials s + m * stride of channel ch in
 // lockstep (one barrier per pass for all of them); input in [0, 4q)
-// (canonical inputs are fine), output canonical.  tws holds the forward
-// twiddles of ch.
-template <int M, class Sync = CtaSync>
+// (canonical inputs are fine), output canonical -- or, with LAZY, in [0, 4q)
+// for consumers that only multiply-accumulate and reduce exactly (the
+// canonical pass costs two minima per coefficient, 6 % of a transform).
+// tws holds the forward twiddles of ch.
+template <int M, class Sync = CtaSync, bool LAZY = false>
 __device__ __forceinline__ void cta_ntt_forward_m(uint32_t* s, int stride, const uint2* tws, int ch) {
     const uint32_t q = c_dev.ch[ch].q, q2 = c_dev.ch[ch].two_q;
     const int u = threadIdx.x;
@@ -207,9 +219,12 @@ __device__ __forceinline__ void cta_ntt_forward_m(uint32_t* s, int stride, const
     Sync::sync();
     fwd_pass<2, M>(s, stride, tws, q, q2, u);
     Sync::sync();
-    fwd_pass<3, M>(s, stride, tws, q, q2, u);
+    fwd_pass<3, M, LAZY>(s, stride, tws, q, q2, u);
     Sync::sync();
 }
+
+// x in [0, 4q) to canonical
+__device__ __forceinline__ uint32_t canon4q(uint32_t x, uint32_t q) { return sub_if_ge(sub_if_ge(x, 2 * q), q); }
 
 // Inverse transforms (include N^-1); input in [0, 2q) (canonical inputs are
 // fine), output canonical.  tws holds the inverse twiddles of ch.
@@ -219,19 +234,19 @@ __device__ __forceinline__ void cta_ntt_inverse_m(uint32_t* s, int stride, const
     const uint32_t ni = c_dev.ch[ch].ninv, nip = c_dev.ch[ch].ninv_p;
     const int u = threadIdx.x;
     Sync::sync();
-    inv_pass<3, M>(s, stride, tws, q, q2, ni, nip, u);
+    inv_pass<3, M>(s, stride, tws, q, q2, ni, nip, u, ch);
     Sync::sync();
-    inv_pass<2, M>(s, stride, tws, q, q2, ni, nip, u);
+    inv_pass<2, M>(s, stride, tws, q, q2, ni, nip, u, ch);
     Sync::sync();
-    inv_pass<1, M>(s, stride, tws, q, q2, ni, nip, u);
+    inv_pass<1, M>(s, stride, tws, q, q2, ni, nip, u, ch);
     Sync::sync();
-    inv_pass<0, M>(s, stride, tws, q, q2, ni, nip, u);
+    inv_pass<0, M>(s, stride, tws, q, q2, ni, nip, u, ch);
     Sync::sync();
 }
 
-template <class Sync = CtaSync>
+template <class Sync = CtaSync, bool LAZY = false>
 __device__ __forceinline__ void cta_ntt_forward(uint32_t* s, const uint2* tws, int ch) {
-    cta_ntt_forward_m<1, Sync>(s, kPadN, tws, ch);
+    cta_ntt_forward_m<1, Sync, LAZY>(s, kPadN, tws, ch);
 }
 template <class Sync = CtaSync>
 __device__ __forceinline__ void cta_ntt_inverse(uint32_t* s, const uint2* tws, int ch) {
