@@ -139,8 +139,19 @@ __device__ __forceinline__ void fwd_pass(uint32_t* s, int stride, const uint2* t
     for (int m = 0; m < M; m++) unit_load<P>(s + m * stride, b, x[m]);
 #pragma unroll
     for (int m = 0; m < M; m++) {
+        if (P == 0) {
+            // the first layer: inputs are below 2q, so X needs no reduction
+            // (X + t < 4q and X - t + 2q is in (0, 4q))
 #pragma unroll
-        for (int t = 0; t < 4; t++) fwd_bfly(x[m][t], x[m][t + 4], wa, q, q2);
+            for (int t = 0; t < 4; t++) {
+                const uint32_t tw = shoup_lazy(x[m][t + 4], wa.x, wa.y, q);
+                x[m][t + 4] = x[m][t] - tw + q2;
+                x[m][t] = x[m][t] + tw;
+            }
+        } else {
+#pragma unroll
+            for (int t = 0; t < 4; t++) fwd_bfly(x[m][t], x[m][t + 4], wa, q, q2);
+        }
         fwd_bfly(x[m][0], x[m][2], wb0, q, q2);
         fwd_bfly(x[m][1], x[m][3], wb0, q, q2);
         fwd_bfly(x[m][4], x[m][6], wb1, q, q2);
@@ -203,7 +214,7 @@ __device__ __forceinline__ void inv_pass(uint32_t* s, int stride, const uint2* t
 }
 
 // Forward transforms of M padded polynomials s + m * stride of channel ch in
-// lockstep (one barrier per pass for all of them); input in [0, 4q)
+// lockstep (one barrier per pass for all of them); input in [0, 2q)
 // (canonical inputs are fine), output canonical -- or, with LAZY, in [0, 4q)
 // for consumers that only multiply-accumulate and reduce exactly (the
 // canonical pass costs two minima per coefficient, 6 % of a transform).
