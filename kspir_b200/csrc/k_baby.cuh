@@ -20,6 +20,8 @@
 // integer < bsMod); the crt channels stay in the NTT domain throughout.
 #pragma once
 
+#include <type_traits>
+
 #include "ntt.cuh"
 #include "pipeline.cuh"
 #include "ptx.cuh"
@@ -75,6 +77,16 @@ struct BabyRot {
     const int32_t* perm;    // caller permutation of rotation ki
 };
 
+// Loads of the query-side inputs (digits, b): written by earlier kernels, so a
+// stand-alone launch (CtaSync) reads them through L1 (their gathers reuse
+// lines across the rotations on an SM); inside the fused answer kernel other
+// CTAs write them during the launch, so those loads bypass L1.
+template <class Sync>
+__device__ __forceinline__ uint32_t ld_query(const uint32_t* p) {
+    if constexpr (std::is_same<Sync, CtaSync>::value) return __ldg(p);
+    else return __ldcg(p);
+}
+
 // perm[k] of this thread's coefficients (reloaded by each multiply-accumulate
 // rather than held in registers across the transforms)
 __device__ __forceinline__ void baby_perm(const BabyRot& R, int* pk) {
@@ -121,7 +133,7 @@ __device__ __forceinline__ void baby_bs_part(const BabyRot& R, const BabyArgs& a
             const uint32_t* kk = R.kbs + (size_t)(j * 2 + R.comp) * kN;
 #pragma unroll
             for (int it = 0; it < kPerThread; it++)
-                acc[it] += (uint64_t)__ldcg(d + pk[it]) * __ldg(kk + tid + it * kNttThreads);
+                acc[it] += (uint64_t)ld_query<Sync>(d + pk[it]) * __ldg(kk + tid + it * kNttThreads);
         }
 #pragma unroll
         for (int it = 0; it < kPerThread; it++)
@@ -139,7 +151,7 @@ __device__ __forceinline__ void baby_bs_part(const BabyRot& R, const BabyArgs& a
             const int pk2 = pidx(tid) + it * kPadStep;
             bool neg;
             const int src = auto_src(k, ginv, &neg);
-            uint32_t v = __ldcg(shifted(a.srcBbs, R.wo) + src);
+            uint32_t v = ld_query<Sync>(shifted(a.srcBbs, R.wo) + src);
             if (neg) v = negmod(v, qb);
             S[pk2] = addmod(S[pk2], v, qb);
         }
@@ -179,13 +191,13 @@ __device__ __forceinline__ void baby_crt_part(const BabyRot& R, const BabyArgs& 
         const uint32_t* kk = R.kcrt + (size_t)((j * 2 + comp) * 2 + ch) * kN;
 #pragma unroll
         for (int it = 0; it < kPerThread; it++)
-            acc[it] += (uint64_t)__ldcg(d + pk[it]) * __ldg(kk + tid + it * kNttThreads);
+            acc[it] += (uint64_t)ld_query<Sync>(d + pk[it]) * __ldg(kk + tid + it * kNttThreads);
     }
 #pragma unroll
     for (int it = 0; it < kPerThread; it++) {
         const int k = tid + it * kNttThreads;
         uint32_t A = negmod(mod_crt(acc[it], ch), cc.q);
-        if (comp == 1) A = addmod(A, __ldcg(shifted(a.srcB, R.wo) + ch * kN + sig[k]), cc.q);
+        if (comp == 1) A = addmod(A, ld_query<Sync>(shifted(a.srcB, R.wo) + ch * kN + sig[k]), cc.q);
         if (R.inter) inter_out[ch * kN + k] = A;
         // (A - S) bsMod^-1 with S in [0, 4q): A + 4q - S is in (0, 5q), and the
         // Shoup product reduces any 32-bit input to a canonical residue
