@@ -244,11 +244,13 @@ __global__ void __launch_bounds__(kNttThreads) k_pack_fused(const uint32_t* __re
     pdl_launch_dependents();
     stage_twiddles(tws, tabs, ch, NTT_FWD);
     pdl_wait();   // the level input comes from the previous kernel
+    // launched after that kernel completes (no early launch), and no CTA writes
+    // the level input: its gathers below read through L1
     // X^I c at position p of polynomial (comp, prime)
     auto cshift = [&](int comp, int pch, int p) -> uint32_t {
         const int s = p - I;
         const uint32_t qq = pch ? kQ2 : kQ1;
-        return s >= 0 ? __ldcg(cc + (comp * 2 + pch) * kN + s) : negmod(__ldcg(cc + (comp * 2 + pch) * kN + s + kN), qq);
+        return s >= 0 ? __ldg(cc + (comp * 2 + pch) * kN + s) : negmod(__ldg(cc + (comp * 2 + pch) * kN + s + kN), qq);
     };
     uint32_t c2v[kPerThreadG][2];
 #pragma unroll
@@ -256,14 +258,14 @@ __global__ void __launch_bounds__(kNttThreads) k_pack_fused(const uint32_t* __re
         const int k = tid + it * kNttThreads;
 #pragma unroll
         for (int comp = 0; comp < 2; comp++)
-            c2v[it][comp] = addmod(cshift(comp, ch, k), __ldcg(r0 + (comp * 2 + ch) * kN + k), q);
+            c2v[it][comp] = addmod(cshift(comp, ch, k), __ldg(r0 + (comp * 2 + ch) * kN + k), q);
         bool neg;
         const int src = auto_src(k, ginv, &neg);
         uint32_t ra[2];
 #pragma unroll
         for (int pch = 0; pch < 2; pch++) {
             const uint32_t qq = pch ? kQ2 : kQ1;
-            const uint32_t v = submod(__ldcg(r0 + (0 * 2 + pch) * kN + src), cshift(0, pch, src), qq);
+            const uint32_t v = submod(__ldg(r0 + (0 * 2 + pch) * kN + src), cshift(0, pch, src), qq);
             ra[pch] = neg ? negmod(v, qq) : v;
         }
         int32_t dig[kMaxEll];
@@ -271,7 +273,7 @@ __global__ void __launch_bounds__(kNttThreads) k_pack_fused(const uint32_t* __re
         const int pk = pidx(tid) + it * kPadStep;
 #pragma unroll
         for (int d = 0; d < ELL; d++) P[d * kPadN + pk] = signed_to_res(dig[d], q);
-        const uint32_t vb = submod(__ldcg(r0 + (1 * 2 + ch) * kN + src), cshift(1, ch, src), q);
+        const uint32_t vb = submod(__ldg(r0 + (1 * 2 + ch) * kN + src), cshift(1, ch, src), q);
         P[ELL * kPadN + pk] = neg ? negmod(vb, q) : vb;
     }
     cta_ntt_forward_m<ELL + 1, CtaSync, true>(P, kPadN, tws, ch);   // outputs in [0, 4q)
