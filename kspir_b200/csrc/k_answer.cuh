@@ -245,8 +245,8 @@ __device__ __forceinline__ void fa_rotation(const FaArgs& A, const BabyArgs& a, 
 }
 
 // giant step (r, c): the key switch of evalAutoRNSCRT for output row c of
-// sub-database r (twosteps.cpp:612-672), as k_giant_fused computes it, with
-// the terms added into acc[r] instead of written over the row.
+// sub-database r (twosteps.cpp:612-672), as k_giant_fused computes it: the
+// terms are added into acc[r].
 template <int ELL>
 __device__ __forceinline__ void fa_giant(const FaArgs& A, int r, int c, uint8_t* smem) {
     uint2* tws = reinterpret_cast<uint2*>(smem);

@@ -37,12 +37,20 @@ __device__ __forceinline__ void query_prep_one(const Workspace& ws, const Gadget
     ws.col0[3 * kN + k] = shoup_mul(submod(bq2, b_bs, kQ2), c2.bsinv, c2.bsinv_p, kQ2);
 }
 
-__global__ void k_query_prep(Workspace ws, GadgetBsgs g, Batch bt) {
+// Also zeroes the query's giant-step accumulators (acc_words u32 words of
+// ws.result, and of ws.ecoef when two_acc): the giant steps of this answer
+// add into them.
+__global__ void k_query_prep(Workspace ws, GadgetBsgs g, Batch bt, int acc_words, int two_acc) {
     pdl_launch_dependents();
     pdl_wait();
     ws = ws_at(ws, bt);
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k < kN) query_prep_one(ws, g, k);
+    const uint4 z = make_uint4(0, 0, 0, 0);
+    for (int i = 4 * k; i < acc_words; i += 4 * kN) {
+        *reinterpret_cast<uint4*>(ws.result + i) = z;
+        if (two_acc) *reinterpret_cast<uint4*>(ws.ecoef + i) = z;
+    }
 }
 
 // Digits of the intermediate rotation (evalAutoSRNSSecond, twosteps.cpp:1109-1120):

@@ -85,18 +85,21 @@ namespace kspir {
 // evalAutoRNSCRT for output[c] (twosteps.cpp:612-672) in shared memory:
 //   INTT(a) per prime -> compose -> X -> X^g -> decompose (ell digits)
 //   -> digit transforms -> -sum_j d_j * key[j]  and  b[sigma_g] - sum_j d_j * key[j]
-// and writes both, canonical, over its own input row (r, c) of the scan
-// output: the a part once the inverse transforms have read it, the b part
-// after a barrier that ends every gather of it.  k_giant_finish then sums the
-// N2 rows of each sub-database (no atomics: the 15 giant steps of one
-// sub-database would all hit the same words at the same time).
+// and adds both, canonical, into the sub-database's accumulator (u32 words
+// in L2; the scan output is only read).  k_giant_finish then adds output[0]
+// and reduces.  A u32 word holds at most kGiantTermsPerAcc terms below
+// q1 (16 (q1 - 1) < 2^32); with more giant steps per sub-database (N1 = 64:
+// 31) rows c odd go to acc0 and rows c even to acc1.
+constexpr int kGiantTermsPerAcc = 16;
+static_assert((uint64_t)kGiantTermsPerAcc * (kQ1 - 1) < (1ull << 32) && kQ2 < kQ1, "giant accumulator width");
 
 constexpr int kGiantPolys = 4;   // two primes x two digits (ell = 2)
 constexpr int kPerThreadG = kN / kNttThreads;
 constexpr int kGiantSmem = kN * 8 + kGiantPolys * kPadN * 4;
 
 template <int ELL>
-__global__ void __launch_bounds__(kNttThreads) k_giant_fused(uint32_t* sout, const uint32_t* __restrict__ gkeys,
+__global__ void __launch_bounds__(kNttThreads) k_giant_fused(const uint32_t* __restrict__ sout, uint32_t* acc0,
+                                                             uint32_t* acc1, const uint32_t* __restrict__ gkeys,
                                                              const uint16_t* __restrict__ gsigma, int N1,
                                                              NttTables tabs, GadgetB g, int R, Batch bt) {
     static_assert(2 * ELL <= kGiantPolys, "shared-memory polynomials");
@@ -111,6 +114,7 @@ __global__ void __launch_bounds__(kNttThreads) k_giant_fused(uint32_t* sout, con
     const int tid = threadIdx.x;
     sout = shifted(sout, ws_off(bt));
     gkeys = shifted(gkeys, key_off(bt));
+    uint32_t* acc = shifted((acc1 && !(c & 1)) ? acc1 : acc0, ws_off(bt)) + (size_t)r * 4 * kN;
     pdl_launch_dependents();
 
     // a of output[c], both primes, to coefficient form
@@ -162,7 +166,6 @@ __global__ void __launch_bounds__(kNttThreads) k_giant_fused(uint32_t* sout, con
         // exact multiply-accumulate below)
         cta_ntt_forward_m<ELL, CtaSync, true>(P + ch * kPadN, 2 * kPadN, tws, ch);
         const ChanConst cc = c_dev.ch[ch];
-        uint32_t cbv[kPerThreadG];
 #pragma unroll
         for (int it = 0; it < kPerThreadG; it++) {
             const int k = tid + it * kNttThreads;
@@ -174,20 +177,16 @@ __global__ void __launch_bounds__(kNttThreads) k_giant_fused(uint32_t* sout, con
                 mad_wide(sb, d, __ldg(key + ((j * 2 + 1) * 2 + ch) * kN + k));
             }
             const uint32_t bv = __ldcg(sout + sout_idx(row, 1 * 2 + ch, sig[k], rows));
-            cbv[it] = addmod(bv, negmod(mod_crt(sb, ch), cc.q), cc.q);
-            sout[sout_idx(row, 0 * 2 + ch, k, rows)] = negmod(mod_crt(sa, ch), cc.q);
+            atomicAdd(acc + (size_t)(0 * 2 + ch) * kN + k, negmod(mod_crt(sa, ch), cc.q));
+            atomicAdd(acc + (size_t)(1 * 2 + ch) * kN + k, addmod(bv, negmod(mod_crt(sb, ch), cc.q), cc.q));
         }
-        __syncthreads();   // every gather of this prime's b part is done
-#pragma unroll
-        for (int it = 0; it < kPerThreadG; it++) sout[sout_idx(row, 1 * 2 + ch, tid + it * kNttThreads, rows)] = cbv[it];
     }
 }
 
-// result[r][comp][ch][k] = (output[0] + the N2 - 1 giant-step contributions)
-// mod q: the sum of the N2 rows of sub-database r after k_giant_fused.  One
-// thread per four consecutive slots (16-byte loads from each row's sectors).
-__global__ void k_giant_finish(const uint32_t* __restrict__ sout, uint32_t* __restrict__ result, int R, int N2,
-                               Batch bt) {
+// result[r][comp][ch][k] = (output[0] + the giant-step accumulators) mod q,
+// in place over acc0 (= result).  One thread per four consecutive slots.
+__global__ void k_giant_finish(const uint32_t* __restrict__ sout, uint32_t* result, const uint32_t* acc1, int R,
+                               int N2, Batch bt) {
     pdl_launch_dependents();
     pdl_wait();
     const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -198,14 +197,16 @@ __global__ void k_giant_finish(const uint32_t* __restrict__ sout, uint32_t* __re
     const int cc_ = (int)((idx / (kN / 4)) % 4);      // comp * 2 + ch
     const int r = (int)(idx / (4 * (kN / 4)));
     const ChanConst q = c_dev.ch[cc_ & 1];
-    uint64_t v0 = 0, v1 = 0, v2 = 0, v3 = 0;
-    for (int c = 0; c < N2; c++) {
-        const uint4 w = __ldcg(reinterpret_cast<const uint4*>(sout + sout_idx(r * N2 + c, cc_, z, R * N2)));
-        v0 += w.x; v1 += w.y; v2 += w.z; v3 += w.w;
+    uint4* res = reinterpret_cast<uint4*>(result + ((size_t)r * 4 + cc_) * kN + z);
+    const uint4 a = __ldcg(res);
+    const uint4 w = __ldcg(reinterpret_cast<const uint4*>(sout + sout_idx(r * N2, cc_, z, R * N2)));
+    uint64_t v0 = (uint64_t)a.x + w.x, v1 = (uint64_t)a.y + w.y, v2 = (uint64_t)a.z + w.z, v3 = (uint64_t)a.w + w.w;
+    if (acc1) {
+        const uint4 b = __ldcg(reinterpret_cast<const uint4*>(shifted(acc1, ws_off(bt)) + ((size_t)r * 4 + cc_) * kN + z));
+        v0 += b.x; v1 += b.y; v2 += b.z; v3 += b.w;
     }
-    *reinterpret_cast<uint4*>(result + ((size_t)r * 4 + cc_) * kN + z) =
-        make_uint4(reduce64(v0, q.q, q.barrett), reduce64(v1, q.q, q.barrett), reduce64(v2, q.q, q.barrett),
-                   reduce64(v3, q.q, q.barrett));
+    *res = make_uint4(reduce64(v0, q.q, q.barrett), reduce64(v1, q.q, q.barrett), reduce64(v2, q.q, q.barrett),
+                      reduce64(v3, q.q, q.barrett));
 }
 
 }  // namespace kspir

@@ -614,11 +614,15 @@ void launch(const kspir_ctx* c, bool pdl, void (*kern)(KArgs...), dim3 grid, dim
     cudaLaunchKernelEx(&cfg, kern, args...);
 }
 
+// the giant steps of a sub-database need a second u32 accumulator
+bool giant_two_acc(const kspir_ctx* c) { return c->N2 - 1 > kGiantTermsPerAcc; }
+
 // rm: write the cipherbuf rotation-major (the tensor-core scans read that one)
 void enqueue_baby(kspir_ctx* c, int slot0, int nq, bool rm, cudaStream_t st) {
     const Workspace& w = c->ws0;
     const Batch bt = batch_of(c, slot0);
-    launch(c, false, k_query_prep, dim3(kN / 256, nq), 256, 0, st, w, c->gad.baby, bt);
+    launch(c, false, k_query_prep, dim3(kN / 256, nq), 256, 0, st, w, c->gad.baby, bt, c->p.r * 4 * kN,
+           giant_two_acc(c) ? 1 : 0);
     launch(c, false, k_ntt_jobs<false>, dim3(c->n_q, nq), kNttThreads, kNttJobSmem, st,
            (const NttJob*)(c->jobs + (rm ? c->seg_q_rm : c->seg_q)), c->ntabs, bt);
     BabyArgs a1{};
@@ -719,15 +723,20 @@ void enqueue_scan(kspir_ctx* c, int slot0, int nq, int kind, cudaStream_t st, bo
     }
 }
 
+// The giant steps add into result (and, past kGiantTermsPerAcc steps per
+// sub-database, ecoef as the second accumulator), which the answer's
+// k_query_prep (enqueue_baby) has zeroed.
 void enqueue_giant(kspir_ctx* c, int slot0, int nq, cudaStream_t st) {
     const Workspace& w = c->ws0;
     const Batch bt = batch_of(c, slot0);
     const int R = c->p.r;
+    uint32_t* acc1 = giant_two_acc(c) ? w.ecoef : nullptr;
     if (c->N2 > 1)
-        launch(c, false, k_giant_fused<2>, dim3(R * (c->N2 - 1), nq), kNttThreads, kGiantSmem, st, w.sout,
-               (const uint32_t*)c->keys0.giant, (const uint16_t*)c->sigma_giant, c->N1, c->ntabs, c->gad.giant, R, bt);
+        launch(c, false, k_giant_fused<2>, dim3(R * (c->N2 - 1), nq), kNttThreads, kGiantSmem, st,
+               (const uint32_t*)w.sout, w.result, acc1, (const uint32_t*)c->keys0.giant,
+               (const uint16_t*)c->sigma_giant, c->N1, c->ntabs, c->gad.giant, R, bt);
     launch(c, false, k_giant_finish, dim3(blocks_for((long)R * 4 * (kN / 4), 256), nq), 256, 0, st, (const uint32_t*)w.sout,
-           w.result, R, c->N2, bt);
+           w.result, (const uint32_t*)acc1, R, c->N2, bt);
 }
 
 // external products of `count` first-dimension results (result -> ext);
@@ -2506,14 +2515,6 @@ int kspir_fetch_stage_slot(kspir_ctx* c, int slot, int stage, uint64_t* out, siz
     if (words != polys * kN) return set_err(c, KSPIR_ERR_INVALID_ARG, "size mismatch");
     uint64_t* tmp = nullptr;
     uint32_t* flat = nullptr;
-    if (stage == KSPIR_STAGE_SCAN) {
-        // the giant steps overwrite rows c >= 1 of the scan output: scan the
-        // slot's rotations again, with the variant the last launch used
-        enqueue_scan(c, slot, 1, c->last_kind, st);
-        KS_CUDA(c, cudaGetLastError());
-        int rc = finish(c, slot, 1);
-        if (rc) return rc;
-    }
     KS_CUDA(c, cudaMalloc(&tmp, words * 8));
     cudaError_t e = cudaSuccess;
     if (stage == KSPIR_STAGE_SCAN) {

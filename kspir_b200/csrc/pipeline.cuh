@@ -50,9 +50,9 @@ struct Workspace {
     uint32_t* inter_acoef;  // [2 ch][N] interA, coefficient form
     uint32_t* dig1;         // [3][3 ch][N] digits of the intermediate -> NTT form
     uint64_t* cipherbuf;    // [N][N1][2] reference reorientCipher layout (twosteps.cpp:1386)
-    uint32_t* sout;         // DB-scan outputs, NTT form, layout of sout_idx (r * N2 rows);
-                            // rows c >= 1 are then overwritten by their giant-step terms
-    uint32_t* result;       // [r][2 comp][2 ch][N] first-dimension results, NTT form
+    uint32_t* sout;         // DB-scan outputs, NTT form, layout of sout_idx (r * N2 rows)
+    uint32_t* result;       // [r][2 comp][2 ch][N] first-dimension results, NTT form (the
+                            // giant steps' accumulator until k_giant_finish)
     uint32_t* ecoef;        // [r][2 comp][2 ch][N] result, coefficient form
     uint32_t* ext;          // [r][2 comp][2 ch][N] external products, coefficient form
     uint32_t* ext2;         // [r/2][2 comp][2 ch][N] packing levels ping-pong with ext
