@@ -75,11 +75,15 @@ def parse():
 
 
 def workload_config(args):
-    return {"workload": f"single-query online answer, 256 MB DB (32768 x 8 KB records), "
+    records = args.r * N // 2                 # 8 KB records: N / 2 per sub-database
+    pre = args.r * N * N // 2 * 8             # preprocessed bytes (u64 per NTT slot)
+    l2 = (f"inputs larger than L2: the {pre / 2**30:g} GiB preprocessed database is streamed every step"
+          if pre > 126 * 10**6 else f"the {pre / 2**20:g} MiB preprocessed database fits in L2 (no flush)")
+    return {"workload": f"single-query online answer, {records * 8 // 1024} MB DB ({records} x 8 KB records), "
                         f"r={args.r} N1={args.N1} N2={N // 2 // args.N1} N={N}",
             "r": args.r, "N1": args.N1, "N2": N // 2 // args.N1,
-            "db_bytes_preprocessed": args.r * N * N // 2 * 8,
-            "l2": "inputs larger than L2: the 1 GiB preprocessed database is streamed every step",
+            "db_bytes_preprocessed": pre,
+            "l2": l2,
             "parallelism": "replicas"}
 
 
