@@ -111,10 +111,11 @@ __device__ __forceinline__ uint64_t crt_compose_res(uint32_t r1, uint32_t r2) {
     return (uint64_t)r1 + (uint64_t)kQ1 * t;
 }
 
-// x mod q, exact for every 64-bit x, q a prime in (2^27, 2^28); mu1 = 2^59 / q,
-// c32 = 2^32 mod q, mu2 = 2^57 / q.  Two Barrett steps with 32x32 products.
+// unsigned minimum for code compiled for the host as well
 __host__ __device__ __forceinline__ uint32_t min_u32(uint32_t a, uint32_t b) { return a < b ? a : b; }
 
+// x mod q, exact for every 64-bit x, q a prime in (2^27, 2^28); mu1 = 2^59 / q,
+// c32 = 2^32 mod q, mu2 = 2^57 / q.  Two Barrett steps with 32x32 products.
 __host__ __device__ __forceinline__ uint32_t mod28(uint64_t x, uint32_t q, uint32_t mu1, uint32_t c32, uint32_t mu2) {
     const uint32_t xh = (uint32_t)(x >> 32), xl = (uint32_t)x;
     // conditional subtractions as minima (x - m wraps above x when x < m)
