@@ -95,17 +95,19 @@ static_assert((uint64_t)kGiantTermsPerAcc * (kQ1 - 1) < (1ull << 32) && kQ2 < kQ
 
 constexpr int kGiantPolys = 4;   // two primes x two digits (ell = 2)
 constexpr int kPerThreadG = kN / kNttThreads;
-constexpr int kGiantSmem = kN * 8 + kGiantPolys * kPadN * 4;
+// The transforms read the device twiddle tables through L1 rather than a
+// staged shared-memory copy: 72 KiB of shared memory and 40 registers give 3
+// CTAs per SM (a staged copy made it 104 KiB and 2 CTAs per SM, 8 % slower).
+constexpr int kGiantSmem = kGiantPolys * kPadN * 4;
 
 template <int ELL>
-__global__ void __launch_bounds__(kNttThreads) k_giant_fused(const uint32_t* __restrict__ sout, uint32_t* acc0,
-                                                             uint32_t* acc1, const uint32_t* __restrict__ gkeys,
-                                                             const uint16_t* __restrict__ gsigma, int N1,
-                                                             NttTables tabs, GadgetB g, int R, Batch bt) {
+__global__ void __launch_bounds__(kNttThreads, 3)
+    k_giant_fused(const uint32_t* __restrict__ sout, uint32_t* acc0, uint32_t* acc1,
+                  const uint32_t* __restrict__ gkeys, const uint16_t* __restrict__ gsigma, int N1, NttTables tabs,
+                  GadgetB g, int R, Batch bt) {
     static_assert(2 * ELL <= kGiantPolys, "shared-memory polynomials");
     extern __shared__ __align__(16) uint8_t smem_raw[];
-    uint2* tws = reinterpret_cast<uint2*>(smem_raw);
-    uint32_t* P = reinterpret_cast<uint32_t*>(smem_raw + kN * 8);   // [kGiantPolys][N]
+    uint32_t* P = reinterpret_cast<uint32_t*>(smem_raw);   // [kGiantPolys][N]
     const int N2 = kN / 2 / N1;
     const int rows = R * N2;
     const int rc = blockIdx.x;
@@ -120,13 +122,12 @@ __global__ void __launch_bounds__(kNttThreads) k_giant_fused(const uint32_t* __r
     // a of output[c], both primes, to coefficient form
 #pragma unroll
     for (int ch = 0; ch < 2; ch++) {
-        stage_twiddles(tws, tabs, ch, NTT_INV);
         pdl_wait();   // the scan output comes from the previous kernel
 #pragma unroll
         for (int k = tid; k < kN / 4; k += kNttThreads)
             *reinterpret_cast<uint4*>(P + ch * kPadN + pidx(4 * k)) =
                 __ldcg(reinterpret_cast<const uint4*>(sout + sout_idx(row, 0 * 2 + ch, 4 * k, rows)));
-        cta_ntt_inverse(P + ch * kPadN, tws, ch);
+        cta_ntt_inverse(P + ch * kPadN, twiddle_table(tabs, ch, NTT_INV), ch);
     }
     // X -> X^g, g = 5^(N1 c), then the digits (registers first: P is overwritten)
     const uint32_t e = (uint32_t)(N1 * c) & 2047u;
@@ -161,10 +162,9 @@ __global__ void __launch_bounds__(kNttThreads) k_giant_fused(const uint32_t* __r
 #pragma unroll 1
     for (int ch = 0; ch < 2; ch++) {
         __syncthreads();
-        stage_twiddles(tws, tabs, ch, NTT_FWD);
         // digits j of this prime: P[j*2+ch], left in [0, 4q) (they only feed the
         // exact multiply-accumulate below)
-        cta_ntt_forward_m<ELL, CtaSync, true>(P + ch * kPadN, 2 * kPadN, tws, ch);
+        cta_ntt_forward_m<ELL, CtaSync, true>(P + ch * kPadN, 2 * kPadN, twiddle_table(tabs, ch, NTT_FWD), ch);
         const ChanConst cc = c_dev.ch[ch];
 #pragma unroll
         for (int it = 0; it < kPerThreadG; it++) {

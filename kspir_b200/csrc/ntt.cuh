@@ -65,12 +65,18 @@ enum NttDir : int { NTT_FWD = 0, NTT_INV = 1 };
 
 // Copies the twiddles of (channel, direction) into shared memory.  The caller
 // synchronises (the transforms start with __syncthreads).
-__device__ __forceinline__ void stage_twiddles(uint2* tws, const NttTables& tabs, int ch, int dir) {
+// The device table of (ch, dir); its layout is the staged one, so a kernel
+// may also run its transforms on it directly (reads through L1).
+__device__ __forceinline__ const uint2* twiddle_table(const NttTables& tabs, int ch, int dir) {
     // a select chain, not tabs.tw[ch]: a run-time index into a kernel
     // parameter array makes the compiler copy the array to local memory
     const uint2* t = ch == 0 ? tabs.tw[0] : ch == 1 ? tabs.tw[1] : ch == 2 ? tabs.tw[2] : ch == 3 ? tabs.tw[3]
                    : ch == 4 ? tabs.tw[4] : ch == 5 ? tabs.tw[5] : tabs.tw[6];
-    const uint4* g = reinterpret_cast<const uint4*>(t + (size_t)dir * kN);
+    return t + (size_t)dir * kN;
+}
+
+__device__ __forceinline__ void stage_twiddles(uint2* tws, const NttTables& tabs, int ch, int dir) {
+    const uint4* g = reinterpret_cast<const uint4*>(twiddle_table(tabs, ch, dir));
     uint4* s = reinterpret_cast<uint4*>(tws);
 #pragma unroll
     for (int k = threadIdx.x; k < kN / 2; k += kNttThreads) s[k] = __ldg(g + k);
